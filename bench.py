@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SPID-Join equi-join: join tuples/s (|R|+|S|) and the
+fraction of the HBM roofline, on the seeded synthetic relations.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2] [--impl ours|reference]
+
+One step = one plain join (partition, build, probe, compaction) of the workload
+with R and S resident in HBM. Rank 0 prints one JSON line. Under torchrun with
+N > 1 every rank joins its own relations (replicas, weak scaling; the
+multi-GPU hash exchange is not built yet) and the time is the max over ranks.
+`--impl reference` times the reference's algorithm restated on the host cores
+(the oracle's pipeline restatement; the UPMEM original cannot run here).
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "spid-join_b200"))
+
+WORKLOADS = {
+    # name: |R|, |S|, zipf, (ranks, rank sets, bank set), description
+    "c1": (1 << 20, 1 << 21, 0.0, (1, 1, 1), "plain equi-join |R|=2^20 |S|=2^21 uniform (-s 1048576 -t 2 -z 0 -r 1)"),
+    "c2": (1 << 27, 1 << 29, 1.0, (4, 4, 1),
+           "plain equi-join |R|=2^27 |S|=2^29 Zipf 1.0, replication groups of 4 (-r 4 -R 4 -B 1)"),
+    "c3": (1 << 26, 1 << 29, 1.5, (4, 4, 1), "plain equi-join |R|=2^26 |S|=2^29 Zipf 1.5, groups of 4"),
+    "c2u": (1 << 27, 1 << 29, 0.0, (4, 4, 1), "plain equi-join |R|=2^27 |S|=2^29 uniform, groups of 4"),
+}
+SEED = 0x5EED5EED
+METRIC = "join tuples/s (|R|+|S|)"
+CPU_SAMPLE_DIV = 32   # the CPU legs run |R|/32, |S|/32 of the same workload
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return ws, int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def emit(obj):
+    print(json.dumps(obj), flush=True)
+
+
+# ------------------------------------------------------------ CPU baseline --
+def cpu_reference_run(wl, steps, warmup):
+    """The reference's pipeline restated in C on all host cores, on a sample of
+    the workload: returns (tuples/s per step list, description, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import spidjoin
+    n_r, n_s, zipf, (ranks, rsets, bset), _ = WORKLOADS[wl]
+    sr, ss = max(n_r // CPU_SAMPLE_DIV, 1), max(n_s // CPU_SAMPLE_DIV, 1)
+    R, S, expect = spidjoin.generate_host(sr, ss, zipf, seed=SEED)
+    cores = os.cpu_count() or 1
+    rates = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        out = oracle.refpipe_join(R, S, ranks=ranks, rank_sets=rsets, bank_set=bset, alg=0, nthreads=cores)
+        dt = time.perf_counter() - t0
+        if i == 0:
+            assert out.shape[0] == ss and oracle.checksum(out) == expect, "CPU restatement disagrees"
+        if i >= warmup:
+            rates.append((sr + ss) / dt)
+    sample = (f"|R|=2^{sr.bit_length() - 1} |S|=2^{ss.bit_length() - 1} (1/{CPU_SAMPLE_DIV} of the workload, "
+              f"same Zipf and layout), reference pipeline restated in C, {cores} threads")
+    return rates, sample, cores
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    rates, sample, cores = cpu_reference_run(args.workload, args.steps, args.warmup)
+    v = statistics.median(rates)
+    n_r, n_s = WORKLOADS[args.workload][:2]
+    emit({"impl": "reference", "metric": METRIC, "value": v, "unit": "tuples/s", "n_gpus": args.gpus,
+          "steps": args.steps, "warmup": args.warmup, "ms_per_step": (n_r + n_s) / v * 1e3,
+          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+          "config": {"workload": WORKLOADS[args.workload][4], "sample": sample},
+          "cpu_baseline": {"value": v, "unit": "tuples/s", "cores": cores, "kind": "port", "sample": sample},
+          "e2e": {"value": v, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    return 0
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid=None):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        cmd = ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "100"]
+        if uuid:
+            cmd.append("--id=" + uuid)
+        try:
+            self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [ln.strip().split(", ") for ln in self.f if ln.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for name, val in zip(names, r[5:9]):
+                    if val.strip().lower() == "active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- our arm --
+def traffic_from_profiles(kernel, units):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled
+    to `units` tuples when the capture used a smaller case."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            t = json.load(f)
+        k = t["kernels"][kernel]
+        return k["dram_bytes"] * units / k["units"]
+    except Exception:
+        return None
+
+
+def run_ours(args):
+    import torch
+    import spidjoin as spj
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    n_r, n_s, zipf, (ranks, rsets, bset), desc = WORKLOADS[args.workload]
+    design = spj.make_design(rank_num=ranks, rank_set=rsets, bank_set=bset, join_alg=args.alg,
+                             skew_mode=args.skew, input_size=n_r, rs_ratio=max(n_s // n_r, 1),
+                             zipf_factor=int(round(zipf * 100)))
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    lib = spj.lib()
+
+    # inputs resident in HBM (seeded, generated on the device)
+    dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
+    dS = torch.empty((n_s, 2), dtype=torch.int32, device="cuda")
+    expect = torch.zeros(1, dtype=torch.int64, device="cuda")
+    spj.check(lib.spj_generate_device(SEED + rank, n_r, n_s, zipf, dR.data_ptr(), dS.data_ptr(),
+                                      expect.data_ptr(), sp))
+    plan = spj.Plan(n_r, n_s, design)
+    out = torch.empty((plan.output_capacity, 2), dtype=torch.int32, device="cuda")
+    n_out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    csum = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    def step():
+        plan.execute(dR.data_ptr(), dS.data_ptr(), out.data_ptr(), n_out.data_ptr(), sp)
+
+    for _ in range(args.warmup):
+        step()
+    spj.check(lib.spj_checksum_device(out.data_ptr(), n_out.data_ptr(), csum.data_ptr(), sp))
+    torch.cuda.synchronize()
+    st = plan.stats()
+    ok = int(n_out.item()) == n_s and int(csum.item()) == int(expect.item())
+    if not ok:
+        raise SystemExit(f"join result check failed: {int(n_out.item())} pairs, checksum mismatch")
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid) if rank == 0 else None
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = ws * (n_r + n_s) / (ms_step / 1e3)
+
+    # per-kernel device times over the timed steps (CUDA events between launches)
+    kts = [plan.kernel_times(b) for b in range(min(args.steps, 128))]
+    kmean = {k: statistics.mean(x[k] for x in kts) for k in kts[0]}
+    n_pairs = int(n_out.item())
+    alg_bytes = {  # algorithmic bytes per launch
+        "k_hist": 8 * (n_r + n_s),
+        "k_scatter": 16 * (n_r + n_s),
+        "k_join_phj": 8 * (n_r + n_s) + 8 * n_pairs,
+    }
+    times = {"k_hist": kmean["hist_ms"], "k_scatter": kmean["scatter_ms"], "k_join_phj": kmean["join_ms"]}
+    dom = max(times, key=times.get)
+    peak, peak_kind = peaks()
+    achieved = alg_bytes[dom] / (times[dom] / 1e3) / 1e9
+    traffic = traffic_from_profiles(dom, n_r + n_s)
+    pipe_bytes = 24 * (n_r + n_s) + 8 * n_pairs
+    pipe_gbs = pipe_bytes / (ms_step / 1e3) / 1e9
+    del out
+    plan.close()
+    torch.cuda.empty_cache()
+
+    # end to end through the JoinInstance API with pinned host columns
+    e2e = None
+    if not args.no_e2e:
+        hR = torch.empty((n_r, 2), dtype=torch.int32, pin_memory=True)
+        hS = torch.empty((n_s, 2), dtype=torch.int32, pin_memory=True)
+        hR.copy_(dR)
+        hS.copy_(dS)
+        del dR, dS
+        torch.cuda.empty_cache()
+        inst = spj.JoinInstance(ranks, rsets, ranks // rsets)
+        inst.LoadColumn((hR.data_ptr(), n_r), n_r, "left")
+        inst.LoadColumn((hS.data_ptr(), n_s), n_s, "right")
+        inst.PrepareJoin(design)
+        ke = max(2, min(args.steps, 5))
+        for _ in range(1):
+            inst.StartJoin(design)
+            inst.FinishJoin(copy=False)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        got = 0
+        for _ in range(ke):
+            inst.StartJoin(design)
+            res = inst.FinishJoin(copy=False)
+            got = sum(res.byte_sizes) // 8
+        el = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([el], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        inst.close()
+        e2e = {"value": ws * (n_r + n_s) * ke / el, "unit": "tuples/s", "steps": ke,
+               "h2d_bytes_per_step": 8 * (n_r + n_s), "d2h_bytes_per_step": 8 * got + 8,
+               "ms_per_step": el / ke * 1e3}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        rates, sample, cores = cpu_reference_run(args.workload, 1, 0)
+        cpu = {"value": rates[0], "unit": "tuples/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        emit({
+            "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": desc, "n_r": n_r, "n_s": n_s, "zipf": zipf, "rank_num": ranks,
+                       "rank_set": rsets, "bank_set": bset, "join_alg": args.alg,
+                       "skew_mode": "adaptive" if args.skew == 0 else "fixed",
+                       "radix_bits": st["radix_bits"], "table_slots": st["table_slots"],
+                       "l2": "inputs (8*(|R|+|S|) bytes) larger than the 126 MB L2; no flush",
+                       "seed": SEED, "parallelism": f"replicas x{ws}"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg_bytes[dom], "traffic": traffic},
+            "pipeline_roofline": {"achieved": pipe_gbs, "peak": peak, "unit": "GB/s", "frac": pipe_gbs / peak,
+                                  "algorithmic_bytes": pipe_bytes, "formula": "24*(|R|+|S|) + 8*|out|"},
+            "kernels_ms": kmean,
+            "e2e": e2e, "cpu_baseline": cpu,
+            "gpu_launches": 8 * args.steps,
+            "clocks": clocks,
+            "check": {"n_pairs": n_pairs, "checksum_ok": ok, "max_s_partition": st["max_s_partition"],
+                      "units": st["units"]},
+        })
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--alg", type=int, default=0)
+    ap.add_argument("--skew", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

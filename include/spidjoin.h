@@ -1,0 +1,205 @@
+/*
+ * spidjoin.h -- C ABI of the B200-native SPID-Join equi-join (libspidjoin.so).
+ *
+ * The join computes, for relations R (build side) and S (probe side) of 8-byte
+ * tuples {u32 key, u32 payload}, the pairs (R.payload, S.payload) of equal keys.
+ * Key 0 marks padding and never joins. Every entry point returns SPJ_OK (0) or a
+ * negative SPJ_E_* code; spj_last_error() gives the message of the last failure
+ * on the calling thread. No entry point exits the process.
+ *
+ * Each declaration names the interface of the reference (yonsei-hpcp/spid-join,
+ * paths relative to that project) that it replaces. The C++ facade in
+ * pidjoin.hpp maps the reference's pidjoin::JoinInstance onto these calls.
+ */
+#ifndef SPIDJOIN_H
+#define SPIDJOIN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* kv_pair_t, include/type_defs.hpp:53-56: lvalue = key, rvalue = payload.
+ * Output pairs reuse it as {lvalue = R payload, rvalue = S payload}. */
+typedef struct {
+    uint32_t lvalue;
+    uint32_t rvalue;
+} spj_kv_pair_t;
+
+enum spj_status {
+    SPJ_OK = 0,
+    SPJ_E_ARG = -1,         /* invalid argument or design */
+    SPJ_E_NOMEM = -2,       /* host or device allocation failed */
+    SPJ_E_CUDA = -3,        /* a CUDA call failed (message has the CUDA error) */
+    SPJ_E_STATE = -4,       /* call out of order (e.g. start before prepare) */
+    SPJ_E_OVERFLOW = -5,    /* a partition exceeded its shared-memory table */
+    SPJ_E_TIMEOUT = -6,     /* a bounded device wait gave up */
+    SPJ_E_NODEVICE = -7,    /* no CUDA device, or not an sm_100 device */
+    SPJ_E_UNSUPPORTED = -8  /* option not supported by this build */
+};
+
+/* join_alg values, include/idpHandler.hpp:135-138 */
+enum spj_join_alg {
+    SPJ_ALG_PHJ = 0,   /* partitioned hash join: at most one match per S tuple,
+                          unmatched S tuples dropped (a2a_srj_probe_inner_mt.c:136-148) */
+    SPJ_ALG_NPHJ = 1,  /* non-partitioned hash join (global table) */
+    SPJ_ALG_SMJ = 2,   /* sort-merge: S rewritten in place, unmatched S kept as is
+                          (mpsm_join_sort_probe.c:214-236) */
+    SPJ_ALG_NL = 3     /* nested loop over sub-partitions of <= 256 R tuples, S rewritten
+                          in place (nested_loop_join.c:184-231) */
+};
+
+enum spj_skew_mode {
+    SPJ_SKEW_ADAPTIVE = 0, /* heavy partitions split so no work unit exceeds unit_tuples S tuples
+                              (at least `group` units each); sampled heavy keys joined on the fly */
+    SPJ_SKEW_FIXED = 1     /* every heavy partition split into exactly `group` units, the
+                              reference's fixed rank-set x bank-set replication */
+};
+
+/* join_design_t, include/idpHandler.hpp:131-145, followed by B200 tuning fields
+ * (0 = chosen by the planner). rank_num, rank_set and bank_set keep the
+ * reference's meaning as replication knobs: 64 * rank_num is the minimum
+ * partition fan-out and rank_set * bank_set the replica group of a heavy
+ * partition (the CTAs that each build its R table and split its S). */
+typedef struct {
+    int64_t input_size; /* -s: |R| of the synthetic driver */
+    int rank_num;       /* -r */
+    int zipf_factor;    /* -z: Zipf exponent x 100 */
+    int rs_ratio;       /* -t: |S| / |R| */
+    int rank_set;       /* -R */
+    int bank_set;       /* -B: any power of two (the reference accepts 1, 8, 16, 32, 64) */
+    int tpch_example;   /* unused (must be 0) */
+    int join_alg;       /* enum spj_join_alg */
+    /* B200 tuning */
+    int radix_bits;     /* partition fan-out = 2^radix_bits */
+    int skew_mode;      /* enum spj_skew_mode */
+    int unit_tuples;    /* max S tuples per work unit in adaptive mode */
+    int heavy_sample;   /* S keys sampled for heavy-key detection (-1 = off) */
+    int table_slots;    /* shared-memory hash-table slots per CTA */
+    int reserved[7];
+} spj_design_t;
+
+/* Fills the reference's defaults (idpHandler.hpp:131-145) and automatic tuning. */
+void spj_design_default(spj_design_t *design);
+
+const char *spj_last_error(void);
+const char *spj_version(void);
+
+/* ------------------------------------------------------------- instance -- */
+
+typedef struct spj_handle spj_handle_t;
+
+/* JoinInstance(int num_rank_allocated, int num_rankgroup, int num_rank_in_rankgroup),
+ * include/join_internals.hpp:306. Binds to the current CUDA device. */
+int spj_create(int num_rank_allocated, int num_rankgroup, int num_rank_in_rankgroup, spj_handle_t **out);
+
+/* void LoadColumn(void *data_ptr, int64_t num_tuples, std::string col_name),
+ * include/join_internals.hpp:316; side 0 = "left" (R), 1 = "right" (S).
+ * Borrows the buffer (host or device memory) until spj_finish, as the
+ * reference aliases it (src/query.cc:305-310). */
+int spj_load_column(spj_handle_t *h, const void *tuples, int64_t num_tuples, int side);
+
+/* void PrepareJoin(join_design_t), include/join_internals.hpp:320: validates the
+ * design and allocates the device buffers of the plan. */
+int spj_prepare(spj_handle_t *h, const spj_design_t *design);
+
+/* void StartJoin(join_design_t), include/join_internals.hpp:321: enqueues the
+ * column copies and the join on the instance's stream and returns. */
+int spj_start(spj_handle_t *h, const spj_design_t *design);
+
+typedef struct {
+    const spj_kv_pair_t *pairs;   /* host memory owned by the instance; valid until the
+                                     next spj_start or spj_destroy */
+    int64_t n_pairs;
+    int num_rank;                 /* per-rank framing of ResultBuffers_t */
+    const int64_t *rank_offsets;  /* num_rank + 1 pair offsets into `pairs` */
+} spj_result_t;
+
+/* ResultBuffers_t FinishJoin(), include/join_internals.hpp:322: waits for the join
+ * and copies the pairs to host memory. No (0,0) padding is emitted. */
+int spj_finish(spj_handle_t *h, spj_result_t *out);
+
+/* Phase timings of the last join (CUDA events), milliseconds. */
+typedef struct {
+    double h2d_ms, partition_ms, join_ms, finish_ms, d2h_ms, total_ms;
+    int64_t n_pairs;
+    int64_t units;           /* work units executed */
+    int64_t heavy_keys;      /* keys joined on the fly */
+    int64_t heavy_tuples;    /* S tuples joined on the fly */
+    int64_t max_r_partition; /* largest R partition */
+    int64_t max_s_partition; /* largest S partition */
+    int radix_bits;
+    int table_slots;
+} spj_stats_t;
+
+/* void RecordLogs(struct timespec start, int rank_group), include/join_internals.hpp:323:
+ * fills `out` and, when `print` is non-zero, writes one line per phase to stdout. */
+int spj_record_logs(spj_handle_t *h, spj_stats_t *out, int print);
+
+void spj_destroy(spj_handle_t *h);
+
+/* ---------------------------------------------------- device-resident plan -- */
+/* The B200 form of the reference's query plan (include/execution.hpp:15-157):
+ * allocation happens once in spj_plan_create; spj_plan_execute allocates
+ * nothing, never synchronises with the host and can be captured in a CUDA graph. */
+
+typedef struct spj_plan spj_plan_t;
+
+int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_plan_t **out);
+
+/* Output capacity (pairs) that `out` must provide for this plan. */
+int64_t spj_plan_output_capacity(const spj_plan_t *plan);
+
+/* r, s, out: device pointers. n_out: device int64 that receives the pair count.
+ * stream: a cudaStream_t (NULL = legacy default stream). */
+int spj_plan_execute(spj_plan_t *plan, const spj_kv_pair_t *r, const spj_kv_pair_t *s, spj_kv_pair_t *out,
+                     int64_t *n_out, void *stream);
+
+/* Statistics of the last execution (synchronises with its stream). */
+int spj_plan_stats(spj_plan_t *plan, spj_stats_t *out);
+
+/* Per-kernel device times of one execution, from CUDA events recorded between
+ * the launches on the execution's stream (milliseconds). */
+typedef struct {
+    double hist_ms;     /* partition histograms of R and S */
+    double scan_ms;     /* offsets and partition starts */
+    double scatter_ms;  /* radix scatter of R and S */
+    double units_ms;    /* work-unit construction */
+    double join_ms;     /* build + probe kernel */
+    double fixup_ms;    /* output compaction */
+    double total_ms;
+} spj_kernel_times_t;
+
+/* Times of the execution `back` runs ago (0 = last); the plan keeps the last 128. */
+int spj_plan_kernel_times(spj_plan_t *plan, int back, spj_kernel_times_t *out);
+
+void spj_plan_destroy(spj_plan_t *plan);
+
+/* Histogram of glb_partition_hash(key) & (2^bits - 1) over a device column (key-0
+ * tuples skipped): the B200 form of the global partition count kernel
+ * (src/dpu/src/join/glb_partition_count.c:119-371, partition_type 0). hist is a
+ * device array of 2^bits uint32 counters. */
+int spj_partition_histogram(const spj_kv_pair_t *tuples, int64_t n, int bits, uint32_t *hist, void *stream);
+
+/* Order-independent checksum of a device pair array: the wrapping sum of
+ * splitmix64((u64)lvalue << 32 | rvalue). */
+int spj_checksum_device(const spj_kv_pair_t *pairs, const int64_t *n_dev, uint64_t *sum_dev, void *stream);
+
+/* -------------------------------------------------- synthetic relations ---- */
+/* The seeded generator of the benchmark relations (the reference's driver,
+ * test/join/main.cc:30-48, leaves Zipf inputs to external files): R keys are a
+ * permutation of 1..n_r with payload = row id; S payload = row id and S keys are
+ * R keys drawn uniformly (zipf_s = 0) or Zipf(zipf_s) over a seeded rank order.
+ * expected_checksum receives the checksum of the exact join output. */
+int spj_generate_host(uint64_t seed, int64_t n_r, int64_t n_s, double zipf_s, spj_kv_pair_t *r,
+                      spj_kv_pair_t *s, uint64_t *expected_checksum, int nthreads);
+int spj_generate_device(uint64_t seed, int64_t n_r, int64_t n_s, double zipf_s, spj_kv_pair_t *r,
+                        spj_kv_pair_t *s, uint64_t *expected_checksum_dev, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPIDJOIN_H */

@@ -1,0 +1,151 @@
+"""ctypes view of the oracle (oracle/liboracle.so).
+
+Test infrastructure only: tests/, ``__graft_entry__.smoke()`` and the CPU-baseline
+legs of ``bench.py`` import this module, as the checker or as the timed CPU
+baseline. The product library never depends on it.
+
+Arrays are numpy ``uint32`` arrays of shape (n, 2): column 0 = key (lvalue),
+column 1 = payload (rvalue), the layout of the reference's ``kv_pair_t``
+(include/type_defs.hpp:53-56 in yonsei-hpcp/spid-join).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_HASH_PATH = os.path.join(HERE, "_ref", "libref_hash.so")
+
+ALG_PHJ, ALG_NPHJ, ALG_SMJ, ALG_NL = 0, 1, 2, 3
+ERRORS = {-1: "bad argument", -2: "out of memory", -3: "local partition exceeds 4096 tuples"}
+
+_lib = None
+
+
+def build():
+    """Compile liboracle.so (and the reference hash library when the reference tree exists)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "all"])
+    if os.path.isdir("/root/reference/src/dpu/src"):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        u32, i64, i32 = ctypes.c_uint32, ctypes.c_int64, ctypes.c_int
+        vp = ctypes.c_void_p
+        for f in ("orc_glb_partition_hash", "orc_local_partition_hash", "orc_join_hash", "orc_join_hash2"):
+            getattr(L, f).restype = u32
+            getattr(L, f).argtypes = [u32]
+        L.orc_crc_table.restype = ctypes.POINTER(u32)
+        L.orc_checksum.restype = ctypes.c_uint64
+        L.orc_checksum.argtypes = [vp, i64]
+        L.orc_sort_pairs.restype = i32
+        L.orc_sort_pairs.argtypes = [vp, i64]
+        L.orc_glb_partition_count.restype = None
+        L.orc_glb_partition_count.argtypes = [vp, i64, i32, i32, i32, i32, vp]
+        L.orc_simple_join.restype = i64
+        L.orc_simple_join.argtypes = [vp, i64, vp, i64, i32, vp]
+        L.orc_refpipe_join.restype = i64
+        L.orc_refpipe_join.argtypes = [vp, i64, vp, i64, i32, i32, i32, i32, i32, vp]
+        L.orc_refpipe_dpu_sizes.restype = i32
+        L.orc_refpipe_dpu_sizes.argtypes = [vp, i64, vp, i64, i32, i32, i32, i32, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _tuples(a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    if a.ndim != 2 or a.shape[1] != 2:
+        raise ValueError("tuples must have shape (n, 2)")
+    return a
+
+
+def hashes(keys):
+    """(glb_partition_hash, local_partition_hash, join_hash, join_hash2) per key."""
+    L = lib()
+    out = np.zeros((len(keys), 4), dtype=np.uint32)
+    for i, k in enumerate(keys):
+        k = int(k)
+        out[i] = (L.orc_glb_partition_hash(k), L.orc_local_partition_hash(k),
+                  L.orc_join_hash(k), L.orc_join_hash2(k))
+    return out
+
+
+def glb_partition_hash_np(keys):
+    """Vectorised restatement of glb_partition_hash (src/dpu/src/hash.c:117-166)."""
+    k = np.asarray(keys, dtype=np.uint64)
+    m = np.uint64(0xFFFFFFFF)
+    h = (np.uint64(4) + (k & np.uint64(0xFFFF))) & m
+    tmp = (((k >> np.uint64(16)) & np.uint64(0xFFFF)) << np.uint64(11)) ^ h
+    h = ((h << np.uint64(16)) ^ tmp) & m
+    h = (h + (h >> np.uint64(11))) & m
+    h = (h ^ (h << np.uint64(3))) & m
+    h = (h + (h >> np.uint64(5))) & m
+    h = (h ^ (h << np.uint64(4))) & m
+    h = (h + (h >> np.uint64(17))) & m
+    h = (h ^ (h << np.uint64(25))) & m
+    h = (h + (h >> np.uint64(6))) & m
+    return h.astype(np.uint32)
+
+
+def checksum(pairs):
+    pairs = _tuples(pairs)
+    return int(lib().orc_checksum(_ptr(pairs), pairs.shape[0]))
+
+
+def sort_pairs(pairs):
+    p = _tuples(pairs).copy()
+    rc = lib().orc_sort_pairs(_ptr(p), p.shape[0])
+    if rc:
+        raise RuntimeError(ERRORS.get(rc, rc))
+    return p
+
+
+def partition_count(tuples, P, type_=0, rank_sets=1, ranks_per_set=1):
+    t = _tuples(tuples)
+    hist = np.zeros(P, dtype=np.uint32)
+    lib().orc_glb_partition_count(_ptr(t), t.shape[0], type_, P, rank_sets, ranks_per_set, _ptr(hist))
+    return hist
+
+
+def simple_join(R, S, keep_unmatched=False):
+    R, S = _tuples(R), _tuples(S)
+    out = np.zeros((max(S.shape[0], 1), 2), dtype=np.uint32)
+    m = lib().orc_simple_join(_ptr(R), R.shape[0], _ptr(S), S.shape[0], int(keep_unmatched), _ptr(out))
+    if m < 0:
+        raise RuntimeError(ERRORS.get(m, m))
+    return out[:m]
+
+
+def refpipe_join(R, S, ranks=1, rank_sets=1, bank_set=1, alg=ALG_PHJ, nthreads=None):
+    """The reference pipeline restated: split, partition, replicate, local join."""
+    R, S = _tuples(R), _tuples(S)
+    nthreads = nthreads or os.cpu_count() or 1
+    out = np.zeros((max(S.shape[0], 1), 2), dtype=np.uint32)
+    m = lib().orc_refpipe_join(_ptr(R), R.shape[0], _ptr(S), S.shape[0], ranks, rank_sets, bank_set, alg,
+                               nthreads, _ptr(out))
+    if m < 0:
+        raise RuntimeError(ERRORS.get(m, m))
+    return out[:m]
+
+
+def refpipe_dpu_sizes(R, S, ranks=1, rank_sets=1, bank_set=1, nthreads=None):
+    R, S = _tuples(R), _tuples(S)
+    D = 64 * ranks
+    rs = np.zeros(D, dtype=np.int64)
+    ss = np.zeros(D, dtype=np.int64)
+    rc = lib().orc_refpipe_dpu_sizes(_ptr(R), R.shape[0], _ptr(S), S.shape[0], ranks, rank_sets, bank_set,
+                                     nthreads or os.cpu_count() or 1, _ptr(rs), _ptr(ss))
+    if rc:
+        raise RuntimeError(ERRORS.get(rc, rc))
+    return rs, ss

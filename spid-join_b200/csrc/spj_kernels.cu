@@ -1,0 +1,632 @@
+// spj_kernels.cu -- sm_100a kernels of the B200 SPID-Join equi-join.
+//
+// One join is a fixed sequence of launches with no host synchronisation:
+//
+//   k_hist      per-chunk partition histograms of R and S (one read pass)
+//   k_colscan   per-partition exclusive offsets across chunks
+//   k_basescan  partition starts (exclusive scan of the totals)
+//   k_scatter   radix scatter of R and S into partition-contiguous columns
+//   k_units     work units: (partition, S range); heavy partitions split
+//   k_join_*    persistent CTAs: build the R partition's shared-memory table,
+//               probe the unit's S range, emit pairs with warp-aggregated
+//               reservations of 1024-pair output chunks
+//   k_fixup_*   move the pairs of the partially used last chunks into the holes
+//               those chunks left, so the output is dense
+//
+// This is the B200 form of the reference's pipeline (yonsei-hpcp/spid-join):
+// glb_partition_count.c (count), glb_partition_packet.c + the host-mediated
+// rotate-and-stream shuffle (scatter; on one GPU the shuffle is the scatter
+// itself), a2a_packetwise_srj_local_partition.c + a2a_srj_build.c +
+// a2a_srj_probe_inner_mt.c (the local join: a partition here is sized so its
+// table fits one CTA's shared memory, so no second local partitioning pass is
+// needed), finish_join.c (output framing: dense, no padding).
+#include <cuda_runtime.h>
+
+#include "spj_internal.h"
+
+namespace spj {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Chunk c of relation rel for a flat block index over R's chunks then S's.
+__device__ __forceinline__ void chunk_of(const PlanDev &P, unsigned bid, int &rel, unsigned &c) {
+    if (bid < P.rel[0].nchunks) {
+        rel = 0;
+        c = bid;
+    } else {
+        rel = 1;
+        c = bid - P.rel[0].nchunks;
+    }
+}
+
+// ------------------------------------------------------------- histogram --
+// glb_partition_count.c:119-236 on B200: each CTA counts one contiguous chunk
+// into a shared-memory histogram; key-0 tuples are skipped (:190-192).
+__global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P, int bits) {
+    extern __shared__ uint32_t sh[];
+    const uint32_t F = 1u << bits, mask = F - 1;
+    int rel;
+    unsigned c;
+    chunk_of(P, blockIdx.x, rel, c);
+    const RelDev R = rel == 0 ? P.rel[0] : P.rel[1];
+    for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const uint32_t b = c * R.chunk;
+    const uint32_t e = min(R.n, b + R.chunk);
+    if (b < e) {
+        const uint4 *in2 = reinterpret_cast<const uint4 *>(R.in);
+        const uint32_t b2 = b >> 1, e2 = e >> 1;
+        constexpr int U = 4;
+        for (uint32_t i = b2 + threadIdx.x; i < e2; i += U * blockDim.x) {
+            uint4 v[U];
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                uint32_t j = i + k * blockDim.x;
+                v[k] = j < e2 ? __ldcs(in2 + j) : make_uint4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                if (v[k].x) atomicAdd(&sh[glb_partition_hash(v[k].x) & mask], 1u);
+                if (v[k].z) atomicAdd(&sh[glb_partition_hash(v[k].z) & mask], 1u);
+            }
+        }
+        if ((e & 1u) && threadIdx.x == 0) {
+            uint32_t key = R.in[e - 1].key;
+            if (key) atomicAdd(&sh[glb_partition_hash(key) & mask], 1u);
+        }
+    }
+    __syncthreads();
+    uint32_t *out = R.hist + (size_t)c * F;
+    for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) out[i] = sh[i];
+}
+
+// Per partition: exclusive offsets of each chunk inside the partition (in place)
+// and the partition total.
+__global__ void k_colscan(PlanDev P, int bits) {
+    const uint32_t F = 1u << bits;
+    const RelDev R = blockIdx.y == 0 ? P.rel[0] : P.rel[1];
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= F) return;
+    uint32_t run = 0;
+    for (uint32_t c = 0; c < R.nchunks; c++) {
+        uint32_t *cell = R.hist + (size_t)c * F + p;
+        uint32_t v = *cell;
+        *cell = run;
+        run += v;
+    }
+    R.total[p] = run;
+}
+
+// Block-wide exclusive scan of up to 1024 * 16 values (one CTA per relation).
+__global__ void __launch_bounds__(1024) k_basescan(PlanDev P, int bits) {
+    __shared__ uint32_t warp_sums[32];
+    const uint32_t F = 1u << bits;
+    const RelDev R = blockIdx.x == 0 ? P.rel[0] : P.rel[1];
+    const uint32_t per = (F + blockDim.x - 1) / blockDim.x;
+    const uint32_t beg = threadIdx.x * per, end = min(F, beg + per);
+    uint32_t sum = 0, mx = 0;
+    for (uint32_t i = beg; i < end; i++) {
+        uint32_t v = R.total[i];
+        sum += v;
+        mx = max(mx, v);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        warp_sums[lane] = wi - w;
+    }
+    __syncthreads();
+    uint32_t run = warp_sums[warp] + incl - sum;
+    for (uint32_t i = beg; i < end; i++) {
+        uint32_t v = R.total[i];
+        R.base[i] = run;
+        run += v;
+    }
+    if (lane == 0) atomicMax(blockIdx.x == 0 ? &P.ctr->max_r_part : &P.ctr->max_s_part, mx);
+}
+
+// --------------------------------------------------------------- scatter --
+// glb_partition_packet.c:420-464 plus the rotate-and-stream shuffle, as one
+// pass: every CTA owns exact write cursors for its chunk's share of each
+// partition (from the histogram), so no global atomics are needed.
+__global__ void __launch_bounds__(kScatterThreads) k_scatter(PlanDev P, int bits) {
+    extern __shared__ uint32_t cursor[];
+    const uint32_t F = 1u << bits, mask = F - 1;
+    int rel;
+    unsigned c;
+    chunk_of(P, blockIdx.x, rel, c);
+    const RelDev R = rel == 0 ? P.rel[0] : P.rel[1];
+    const uint32_t *off = R.hist + (size_t)c * F;
+    for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) cursor[i] = R.base[i] + off[i];
+    __syncthreads();
+    const uint32_t b = c * R.chunk;
+    const uint32_t e = min(R.n, b + R.chunk);
+    if (b >= e) return;
+    const uint4 *in2 = reinterpret_cast<const uint4 *>(R.in);
+    uint2 *out = reinterpret_cast<uint2 *>(R.out);
+    const uint32_t b2 = b >> 1, e2 = e >> 1;
+    constexpr int U = 4;
+    for (uint32_t i = b2 + threadIdx.x; i < e2; i += U * blockDim.x) {
+        uint4 v[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            uint32_t j = i + k * blockDim.x;
+            v[k] = j < e2 ? __ldcs(in2 + j) : make_uint4(0, 0, 0, 0);
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            if (v[k].x) {
+                uint32_t pos = atomicAdd(&cursor[glb_partition_hash(v[k].x) & mask], 1u);
+                out[pos] = make_uint2(v[k].x, v[k].y);
+            }
+            if (v[k].z) {
+                uint32_t pos = atomicAdd(&cursor[glb_partition_hash(v[k].z) & mask], 1u);
+                out[pos] = make_uint2(v[k].z, v[k].w);
+            }
+        }
+    }
+    if ((e & 1u) && threadIdx.x == 0) {
+        Tuple t = R.in[e - 1];
+        if (t.key) {
+            uint32_t pos = atomicAdd(&cursor[glb_partition_hash(t.key) & mask], 1u);
+            out[pos] = make_uint2(t.key, t.pay);
+        }
+    }
+}
+
+// ----------------------------------------------------------------- units --
+// One thread per partition. The reference replicates every R partition to
+// rank_set x bank_set DPUs and splits S among the replicas by element index
+// (glb_partition_count.c:317-318, glb_chipwise_partition_count.c:251-255);
+// here the replicas are work units, each a CTA that builds the same table and
+// probes a contiguous slice of the partition's S.
+__global__ void k_units(PlanDev P, int bits, JoinParams jp) {
+    const uint32_t F = 1u << bits;
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= F) return;
+    const uint32_t nr = P.rel[0].total[p], ns = P.rel[1].total[p];
+    if (ns == 0) return;
+    if (nr == 0 && !jp.keep_unmatched) return;
+    uint32_t g;
+    if (jp.skew_mode == SPJ_SKEW_FIXED) {
+        g = (uint32_t)max(jp.group, 1);
+    } else {
+        g = 1;
+        if (ns > jp.unit_tuples) {
+            g = (ns + jp.unit_tuples - 1) / jp.unit_tuples;
+            g = max(g, (uint32_t)max(jp.group, 1));
+        }
+    }
+    g = min(g, ns);
+    uint32_t first = atomicAdd(&P.ctr->unit_count, g);
+    if (first + g > P.max_units) {
+        atomicOr(&P.ctr->error, 4u);
+        return;
+    }
+    const uint32_t s0 = P.rel[1].base[p];
+    for (uint32_t k = 0; k < g; k++) {
+        Unit u;
+        u.p = p;
+        u.s_begin = s0 + (uint32_t)(((uint64_t)ns * k) / g);
+        u.s_end = s0 + (uint32_t)(((uint64_t)ns * (k + 1)) / g);
+        u.pad = 0;
+        P.units[first + k] = u;
+    }
+}
+
+// ------------------------------------------------------- output emission --
+struct WarpOut {
+    unsigned long long cur, end;
+};
+
+// Warp-aggregated append: one ballot per 32 candidate pairs; a fresh 1024-pair
+// chunk is reserved with one global atomic when the warp's chunk runs out.
+__device__ __forceinline__ void warp_emit(const PlanDev &P, WarpOut &w, bool has, uint32_t lv, uint32_t rv) {
+    const unsigned mask = __ballot_sync(0xffffffffu, has);
+    if (mask == 0) return;
+    const unsigned m = __popc(mask);
+    const unsigned rank = __popc(mask & lanemask_lt());
+    unsigned long long pos;
+    if (w.cur + m <= w.end) {
+        pos = w.cur + rank;
+        w.cur += m;
+    } else {
+        const unsigned avail = (unsigned)(w.end - w.cur);
+        unsigned long long nb = 0;
+        if ((threadIdx.x & 31) == 0) nb = atomicAdd(&P.ctr->out_reserved, (unsigned long long)kOutChunk);
+        nb = __shfl_sync(0xffffffffu, nb, 0);
+        pos = rank < avail ? w.cur + rank : nb + (rank - avail);
+        w.cur = nb + (m - avail);
+        w.end = nb + kOutChunk;
+    }
+    if (has) {
+        if (pos < P.out_cap)
+            reinterpret_cast<uint2 *>(P.out)[pos] = make_uint2(lv, rv);
+        else
+            atomicOr(&P.ctr->error, 2u);
+    }
+}
+
+__device__ __forceinline__ void warp_close(const PlanDev &P, WarpOut &w) {
+    if ((threadIdx.x & 31) == 0 && w.end > w.cur) {
+        unsigned h = atomicAdd(&P.ctr->hole_count, 1u);
+        if (h < kMaxHoles) {
+            P.holes[h].begin = w.cur;
+            P.holes[h].end = w.end;
+        } else {
+            atomicOr(&P.ctr->error, 8u);
+        }
+    }
+}
+
+// Table slot of a key: the hash bits above the partition bits, scaled to the
+// table size (multiply-shift range reduction).
+__device__ __forceinline__ uint32_t slot_of(uint32_t key, uint32_t bits, uint32_t ts) {
+    const uint32_t hi = glb_partition_hash(key) >> bits;
+    return (uint32_t)(((unsigned long long)hi * ts) >> (32 - bits));
+}
+
+// Clears the table and inserts the R partition. Linear probing, key 0 = empty
+// (a2a_srj_build.c:208-246). A key already present is not inserted again, so the
+// probe returns the first-inserted tuple of a repeated key, one match per S tuple
+// (a2a_srj_probe_inner_mt.c:136-148).
+__device__ __forceinline__ void build_table(const PlanDev &P, const JoinParams &jp, unsigned long long *table,
+                                            uint32_t p) {
+    const uint32_t ts = jp.table_slots;
+    for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) table[i] = 0ull;
+    __syncthreads();
+    const uint32_t nr = P.rel[0].total[p];
+    const Tuple *pr = P.rel[0].out + P.rel[0].base[p];
+    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
+        const Tuple t = pr[i];
+        const unsigned long long ent = ((unsigned long long)t.pay << 32) | t.key;
+        uint32_t s = slot_of(t.key, jp.bits, ts);
+        for (uint32_t step = 0;; step++) {
+            const unsigned long long prev = atomicCAS(&table[s], 0ull, ent);
+            if (prev == 0ull || (uint32_t)prev == t.key) break;
+            if (++s == ts) s = 0;
+            if (step >= ts) {
+                atomicOr(&P.ctr->error, 1u);
+                break;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Probe of a2a_srj_probe_inner_mt.c:101-168: stop at the key (hit) or at an empty
+// slot (miss); the scan is bounded by the table size.
+__device__ __forceinline__ bool probe_table(const unsigned long long *table, uint32_t ts, uint32_t bits,
+                                            uint32_t key, uint32_t &rpay) {
+    uint32_t s = slot_of(key, bits, ts);
+    for (uint32_t step = 0; step < ts; step++) {
+        const unsigned long long e = table[s];
+        const uint32_t ek = (uint32_t)e;
+        if (ek == key) {
+            rpay = (uint32_t)(e >> 32);
+            return true;
+        }
+        if (ek == 0) return false;
+        if (++s == ts) s = 0;
+    }
+    return false;
+}
+
+// Fetches the next unit for the CTA; returns false when the queue is empty.
+__device__ __forceinline__ bool next_unit(const PlanDev &P, unsigned n_units, unsigned *s_slot, Unit &un) {
+    if (threadIdx.x == 0) *s_slot = atomicAdd(&P.ctr->unit_next, 1u);
+    __syncthreads();
+    const unsigned u = *s_slot;
+    __syncthreads();
+    if (u >= n_units) return false;
+    un = P.units[u];
+    return true;
+}
+
+// ----------------------------------------------------- partitioned hash join --
+__global__ void __launch_bounds__(kJoinThreads) k_join_phj(PlanDev P, JoinParams jp) {
+    extern __shared__ unsigned long long table[];
+    __shared__ unsigned s_slot;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t ts = jp.table_slots;
+    const unsigned n_units = *(volatile unsigned *)&P.ctr->unit_count;
+    const Tuple *ps = P.rel[1].out;
+    WarpOut w{0ull, 0ull};
+    uint32_t cur_p = 0xffffffffu;
+    Unit un;
+    while (next_unit(P, n_units, &s_slot, un)) {
+        if (un.p != cur_p) {
+            build_table(P, jp, table, un.p);
+            cur_p = un.p;
+        }
+        constexpr int U = 4;
+        for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
+            Tuple t[U];
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                const uint32_t idx = base + k * 32 + lane;
+                t[k] = idx < un.s_end ? ps[idx] : Tuple{0u, 0u};
+            }
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                uint32_t rp = 0;
+                const bool hit = t[k].key != 0 && probe_table(table, ts, jp.bits, t[k].key, rp);
+                warp_emit(P, w, hit, rp, t[k].pay);
+            }
+        }
+        __syncthreads();
+    }
+    warp_close(P, w);
+}
+
+// ------------------------------------------------------------------ fix-up --
+// Every reserved chunk is 1024-aligned and only a warp's last chunk can be
+// partly used, so the unused slots form at most one hole per warp at a chunk's
+// tail. With N = reserved - holes, the pairs stored at positions >= N outside
+// holes move into the holes below N.
+__global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
+    extern __shared__ unsigned long long keys[];  // kMaxHoles entries
+    __shared__ unsigned long long red[32];
+    const unsigned nh = min(P.ctr->hole_count, (unsigned)kMaxHoles);
+    unsigned npow = 1;
+    while (npow < nh) npow <<= 1;
+    for (unsigned i = threadIdx.x; i < npow; i += blockDim.x) {
+        if (i < nh) {
+            const Hole h = P.holes[i];
+            keys[i] = (h.begin << 11) | (h.end - h.begin);
+        } else {
+            keys[i] = ~0ull;
+        }
+    }
+    __syncthreads();
+    for (unsigned k = 2; k <= npow; k <<= 1) {
+        for (unsigned j = k >> 1; j > 0; j >>= 1) {
+            for (unsigned i = threadIdx.x; i < npow; i += blockDim.x) {
+                const unsigned ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long a = keys[i], b = keys[ixj];
+                    const bool up = (i & k) == 0;
+                    if ((a > b) == up) {
+                        keys[i] = b;
+                        keys[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // total hole length
+    unsigned long long part = 0;
+    for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) part += keys[i] & 2047ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long H = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) H += red[i];
+        const unsigned long long total = P.ctr->out_reserved;
+        const unsigned long long N = total - H;
+        P.ctr->n_out = N;
+        if (P.n_out_user) *P.n_out_user = N;
+        // Serial pass over the (sorted) holes: prefix sums of the parts below
+        // and above N. nh is at most kMaxHoles.
+        unsigned long long g = 0, cincl = 0;
+        unsigned nl = 0, nd = 0;
+        for (unsigned i = 0; i < nh; i++) {
+            const unsigned long long b = keys[i] >> 11, len = keys[i] & 2047ull, e = b + len;
+            if (b < N) {
+                const unsigned long long lo = (e < N ? e : N) - b;
+                P.gaps[nl].begin = b;
+                P.gap_off[nl] = g;
+                g += lo;
+                nl++;
+            }
+            if (e > N) {
+                const unsigned long long ub = b > N ? b : N;
+                const unsigned long long ulen = e - ub;
+                // data elements located before this hole
+                P.datas[nd].begin = ub - N - cincl;
+                cincl += ulen;
+                P.data_off[nd] = cincl;
+                nd++;
+            }
+        }
+        P.ctr->gap_total = g;
+        P.ctr->n_gaps = nl;
+        P.ctr->n_data = nd;
+    }
+}
+
+__device__ __forceinline__ unsigned upper_bound_u64(const unsigned long long *a, unsigned n,
+                                                    unsigned long long x) {
+    unsigned lo = 0, hi = n;
+    while (lo < hi) {
+        const unsigned mid = (lo + hi) >> 1;
+        if (a[mid] <= x)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_fixup_copy(PlanDev P) {
+    const unsigned long long G = P.ctr->gap_total;
+    if (G == 0 || (P.ctr->error & 8u)) return;  // holes were dropped: the count is unusable
+    const unsigned long long N = P.ctr->n_out;
+    const unsigned ng = P.ctr->n_gaps, nd = P.ctr->n_data;
+    uint2 *out = reinterpret_cast<uint2 *>(P.out);
+    for (unsigned long long x = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; x < G;
+         x += (unsigned long long)gridDim.x * blockDim.x) {
+        // destination: x-th slot of the holes below N
+        const unsigned gi = upper_bound_u64(P.gap_off, ng, x) - 1;
+        const unsigned long long dst = P.gaps[gi].begin + (x - P.gap_off[gi]);
+        // source: x-th stored pair at or above N (holes skipped)
+        unsigned lo = 0, hi = nd;
+        while (lo < hi) {
+            const unsigned mid = (lo + hi) >> 1;
+            if (P.datas[mid].begin <= x)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        const unsigned long long shift = lo > 0 ? P.data_off[lo - 1] : 0ull;
+        const unsigned long long src = N + x + shift;
+        if (src >= P.out_cap || dst >= N) {
+            atomicOr(&P.ctr->error, 16u);
+            continue;
+        }
+        out[dst] = out[src];
+    }
+}
+
+// ------------------------------------------------------------- utilities --
+__global__ void k_checksum(const spj_kv_pair_t *pairs, const int64_t *n_dev, unsigned long long *sum) {
+    const unsigned long long n = (unsigned long long)*n_dev;
+    unsigned long long acc = 0;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        acc += pair_digest(pairs[i].lvalue, pairs[i].rvalue);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(sum, acc);
+}
+
+__global__ void k_gen_r(Perm pr, uint64_t n, Tuple *r) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        r[i] = gen_r(pr, i);
+}
+
+__global__ void k_gen_s(GenSpec g, Zipf z, Perm pr, Perm prank, Tuple *s, unsigned long long *expect) {
+    unsigned long long acc = 0;
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < g.nS;
+         j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t row = gen_s_row(g, z, prank, j);
+        Tuple t;
+        t.key = (uint32_t)(1 + perm_apply(pr, row));
+        t.pay = (uint32_t)j;
+        s[j] = t;
+        acc += pair_digest((uint32_t)row, (uint32_t)j);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (expect && (threadIdx.x & 31) == 0) atomicAdd(expect, acc);
+}
+
+__global__ void k_hist_single(const Tuple *t, uint64_t n, int bits, uint32_t *hist) {
+    const uint32_t mask = (1u << bits) - 1;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = t[i].key;
+        if (k) atomicAdd(&hist[glb_partition_hash(k) & mask], 1u);
+    }
+}
+
+}  // namespace spj
+
+// Entry points used by spj_plan.cu (kept C++-linkage, internal).
+namespace spj {
+
+cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
+    PlanDev &P = pl->dev;
+    const JoinParams &jp = pl->jp;
+    const int bits = jp.bits;
+    const unsigned F = 1u << bits;
+    const unsigned nchunks = P.rel[0].nchunks + P.rel[1].nchunks;
+    const size_t hsmem = (size_t)F * 4;
+    cudaEvent_t *ev = pl->have_events ? pl->ring[pl->ring_next] : nullptr;
+    auto mark = [&](int i) {
+        if (ev) cudaEventRecord(ev[i], st);
+    };
+    mark(0);
+    k_hist<<<nchunks, kHistThreads, hsmem, st>>>(P, bits);
+    mark(1);
+    k_colscan<<<dim3((F + 255) / 256, 2), 256, 0, st>>>(P, bits);
+    k_basescan<<<2, 1024, 0, st>>>(P, bits);
+    mark(2);
+    k_scatter<<<nchunks, kScatterThreads, hsmem, st>>>(P, bits);
+    mark(3);
+    k_units<<<(F + 255) / 256, 256, 0, st>>>(P, bits, jp);
+    mark(4);
+    k_join_phj<<<pl->join_blocks, kJoinThreads, (size_t)jp.table_slots * 8, st>>>(P, jp);
+    mark(5);
+    k_fixup_prep<<<1, 1024, (size_t)kMaxHoles * 8, st>>>(P);
+    k_fixup_copy<<<pl->num_sms * 2, 256, 0, st>>>(P);
+    mark(6);
+    if (ev) {
+        pl->ring_next = (pl->ring_next + 1) % spj_plan::kRing;
+        pl->ring_filled = pl->ring_filled < spj_plan::kRing ? pl->ring_filled + 1 : spj_plan::kRing;
+    }
+    return cudaGetLastError();
+}
+
+// Kernel launches of one execution (for launch accounting).
+int pipeline_launches() { return 8; }
+
+cudaError_t configure_kernels(int table_slots, int *join_blocks_per_sm) {
+    cudaError_t e;
+    int dev = 0, max_smem = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (1 << kMaxRadixBits) * 4);
+    if (e) return e;
+    e = cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (1 << kMaxRadixBits) * 4);
+    if (e) return e;
+    // the largest table any plan may use, so plans of different sizes coexist
+    e = cudaFuncSetAttribute(k_join_phj, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - 1024);
+    if (e) return e;
+    e = cudaFuncSetAttribute(k_fixup_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxHoles * 8);
+    if (e) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(join_blocks_per_sm, k_join_phj, kJoinThreads,
+                                                         (size_t)table_slots * 8);
+}
+
+cudaError_t launch_checksum(const spj_kv_pair_t *pairs, const int64_t *n_dev, uint64_t *sum_dev, int sms,
+                            cudaStream_t st) {
+    cudaMemsetAsync(sum_dev, 0, 8, st);
+    k_checksum<<<sms * 4, 256, 0, st>>>(pairs, n_dev, reinterpret_cast<unsigned long long *>(sum_dev));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_generate(uint64_t seed, int64_t n_r, int64_t n_s, double zipf_s, spj_kv_pair_t *r,
+                            spj_kv_pair_t *s, uint64_t *expect, int sms, cudaStream_t st) {
+    const Perm pr = make_perm((uint64_t)n_r, seed_R(seed));
+    const Perm prank = make_perm((uint64_t)n_r, seed_rank(seed));
+    GenSpec g{seed, (uint64_t)n_r, (uint64_t)n_s, zipf_s};
+    const Zipf z = make_zipf((uint64_t)n_r, zipf_s > 0 ? zipf_s : 1.0);
+    if (expect) cudaMemsetAsync(expect, 0, 8, st);
+    if (r && n_r > 0) k_gen_r<<<sms * 8, 256, 0, st>>>(pr, (uint64_t)n_r, reinterpret_cast<Tuple *>(r));
+    if (s && n_s > 0)
+        k_gen_s<<<sms * 8, 256, 0, st>>>(g, z, pr, prank, reinterpret_cast<Tuple *>(s),
+                                          reinterpret_cast<unsigned long long *>(expect));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hist_single(const spj_kv_pair_t *t, int64_t n, int bits, uint32_t *hist, int sms,
+                               cudaStream_t st) {
+    cudaMemsetAsync(hist, 0, (size_t)4 << bits, st);
+    if (n > 0) k_hist_single<<<sms * 4, 256, 0, st>>>(reinterpret_cast<const Tuple *>(t), (uint64_t)n, bits, hist);
+    return cudaGetLastError();
+}
+
+}  // namespace spj

@@ -1,0 +1,260 @@
+"""Python host API of the B200 SPID-Join equi-join, over the C ABI of libspidjoin.so.
+
+Mirrors the reference's host interface ``pidjoin::JoinInstance``
+(include/join_internals.hpp:301-323 of yonsei-hpcp/spid-join): construct with the
+rank layout, ``LoadColumn`` the "left" (R) and "right" (S) columns, then
+``PrepareJoin`` / ``StartJoin`` / ``FinishJoin`` / ``RecordLogs``. Columns are
+numpy ``uint32`` arrays of shape (n, 2) (the ``kv_pair_t`` layout: key, payload)
+or device tensors given as ``(data_ptr, n)``. Errors raise ``SpjError`` instead
+of exiting the process (the reference calls ``exit(-1)``).
+
+The library has no CPU path: without a CUDA device every join call raises.
+"""
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libspidjoin.so")
+
+SPJ_OK = 0
+STATUS = {-1: "SPJ_E_ARG", -2: "SPJ_E_NOMEM", -3: "SPJ_E_CUDA", -4: "SPJ_E_STATE", -5: "SPJ_E_OVERFLOW",
+          -6: "SPJ_E_TIMEOUT", -7: "SPJ_E_NODEVICE", -8: "SPJ_E_UNSUPPORTED"}
+ALG = {"phj": 0, "nphj": 1, "smj": 2, "nl": 3}
+SKEW_ADAPTIVE, SKEW_FIXED = 0, 1
+
+# every symbol include/spidjoin.h declares
+EXPORTS = (
+    "spj_design_default", "spj_last_error", "spj_version", "spj_create", "spj_load_column", "spj_prepare",
+    "spj_start", "spj_finish", "spj_record_logs", "spj_destroy", "spj_plan_create", "spj_plan_output_capacity",
+    "spj_plan_execute", "spj_plan_stats", "spj_plan_destroy", "spj_partition_histogram", "spj_checksum_device",
+    "spj_generate_host", "spj_generate_device", "spj_plan_kernel_times",
+)
+
+
+class SpjError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Design(ctypes.Structure):
+    """spj_design_t = join_design_t (include/idpHandler.hpp:131-145) + B200 tuning."""
+    _fields_ = [("input_size", ctypes.c_int64), ("rank_num", ctypes.c_int), ("zipf_factor", ctypes.c_int),
+                ("rs_ratio", ctypes.c_int), ("rank_set", ctypes.c_int), ("bank_set", ctypes.c_int),
+                ("tpch_example", ctypes.c_int), ("join_alg", ctypes.c_int), ("radix_bits", ctypes.c_int),
+                ("skew_mode", ctypes.c_int), ("unit_tuples", ctypes.c_int), ("heavy_sample", ctypes.c_int),
+                ("table_slots", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("pairs", ctypes.c_void_p), ("n_pairs", ctypes.c_int64), ("num_rank", ctypes.c_int),
+                ("rank_offsets", ctypes.POINTER(ctypes.c_int64))]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("h2d_ms", ctypes.c_double), ("partition_ms", ctypes.c_double), ("join_ms", ctypes.c_double),
+                ("finish_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("n_pairs", ctypes.c_int64), ("units", ctypes.c_int64), ("heavy_keys", ctypes.c_int64),
+                ("heavy_tuples", ctypes.c_int64), ("max_r_partition", ctypes.c_int64),
+                ("max_s_partition", ctypes.c_int64), ("radix_bits", ctypes.c_int), ("table_slots", ctypes.c_int)]
+
+    def as_dict(self):
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+class KernelTimes(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ("hist_ms", "scan_ms", "scatter_ms", "units_ms", "join_ms", "fixup_ms", "total_ms")]
+
+    def as_dict(self):
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """Loads libspidjoin.so (built by ``make -C spid-join_b200``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SpjError(-7, f"{LIB_PATH} is missing: build it with `make -C {HERE}`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+        L.spj_last_error.restype = ctypes.c_char_p
+        L.spj_version.restype = ctypes.c_char_p
+        L.spj_design_default.argtypes = [ctypes.POINTER(Design)]
+        L.spj_design_default.restype = None
+        L.spj_create.argtypes = [i32, i32, i32, ctypes.POINTER(vp)]
+        L.spj_load_column.argtypes = [vp, vp, i64, i32]
+        L.spj_prepare.argtypes = [vp, ctypes.POINTER(Design)]
+        L.spj_start.argtypes = [vp, ctypes.POINTER(Design)]
+        L.spj_finish.argtypes = [vp, ctypes.POINTER(Result)]
+        L.spj_record_logs.argtypes = [vp, ctypes.POINTER(Stats), i32]
+        L.spj_destroy.argtypes = [vp]
+        L.spj_destroy.restype = None
+        L.spj_plan_create.argtypes = [i64, i64, ctypes.POINTER(Design), ctypes.POINTER(vp)]
+        L.spj_plan_output_capacity.argtypes = [vp]
+        L.spj_plan_output_capacity.restype = i64
+        L.spj_plan_execute.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.spj_plan_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+        L.spj_plan_kernel_times.argtypes = [vp, i32, ctypes.POINTER(KernelTimes)]
+        L.spj_plan_destroy.argtypes = [vp]
+        L.spj_plan_destroy.restype = None
+        L.spj_partition_histogram.argtypes = [vp, i64, i32, vp, vp]
+        L.spj_checksum_device.argtypes = [vp, vp, vp, vp]
+        L.spj_generate_host.argtypes = [ctypes.c_uint64, i64, i64, ctypes.c_double, vp, vp,
+                                        ctypes.POINTER(ctypes.c_uint64), i32]
+        L.spj_generate_device.argtypes = [ctypes.c_uint64, i64, i64, ctypes.c_double, vp, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != SPJ_OK:
+        raise SpjError(rc, lib().spj_last_error().decode())
+    return rc
+
+
+def make_design(**kw):
+    """A design with the reference's defaults; keyword overrides by field name
+    (``join_alg`` may also be "phj", "smj", "nl", "nphj")."""
+    d = Design()
+    lib().spj_design_default(ctypes.byref(d))
+    for k, v in kw.items():
+        if k == "join_alg" and isinstance(v, str):
+            v = ALG[v]
+        if k not in {f[0] for f in Design._fields_}:
+            raise KeyError(k)
+        setattr(d, k, int(v))
+    return d
+
+
+def _host_tuples(a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    if a.ndim != 2 or a.shape[1] != 2:
+        raise ValueError("tuples must have shape (n, 2)")
+    return a
+
+
+def generate_host(n_r, n_s, zipf=0.0, seed=0x5EED5EED, nthreads=0):
+    """The seeded benchmark relations and the checksum of their exact join."""
+    R = np.zeros((n_r, 2), dtype=np.uint32)
+    S = np.zeros((max(n_s, 0), 2), dtype=np.uint32)
+    cs = ctypes.c_uint64()
+    check(lib().spj_generate_host(seed, n_r, n_s, float(zipf), R.ctypes.data, S.ctypes.data if n_s else None,
+                                  ctypes.byref(cs), nthreads))
+    return R, S, int(cs.value)
+
+
+@dataclass
+class ResultBuffers:
+    """ResultBuffers_t (include/type_defs.hpp:82): one buffer per rank + byte sizes."""
+    buffers: list
+    byte_sizes: list
+
+    def pairs(self):
+        return np.concatenate(self.buffers) if self.buffers else np.zeros((0, 2), np.uint32)
+
+
+class JoinInstance:
+    """pidjoin::JoinInstance on one B200 (include/join_internals.hpp:301-323)."""
+
+    def __init__(self, num_rank_allocated=1, num_rankgroup=1, num_rank_in_rankgroup=None):
+        if num_rank_in_rankgroup is None:
+            num_rank_in_rankgroup = num_rank_allocated // max(num_rankgroup, 1)
+        self._h = ctypes.c_void_p()
+        check(lib().spj_create(num_rank_allocated, num_rankgroup, num_rank_in_rankgroup, ctypes.byref(self._h)))
+        self._keep = {}
+
+    def LoadColumn(self, data, num_tuples=None, col_name="left"):
+        side = {"left": 0, "right": 1}.get(col_name)
+        if side is None:
+            raise SpjError(-1, f"Column name error: {col_name} should be left or right")
+        if isinstance(data, tuple):  # (device pointer, n)
+            ptr, n = data
+        else:
+            arr = _host_tuples(data)
+            self._keep[side] = arr
+            ptr, n = arr.ctypes.data, arr.shape[0]
+        if num_tuples is not None:
+            n = int(num_tuples)
+        check(lib().spj_load_column(self._h, ptr, n, side))
+
+    def PrepareJoin(self, design=None):
+        check(lib().spj_prepare(self._h, ctypes.byref(design) if design is not None else None))
+
+    def StartJoin(self, design=None):
+        check(lib().spj_start(self._h, ctypes.byref(design) if design is not None else None))
+
+    def FinishJoin(self, copy=True):
+        res = Result()
+        check(lib().spj_finish(self._h, ctypes.byref(res)))
+        n = res.n_pairs
+        if n:
+            buf = (ctypes.c_uint32 * (2 * n)).from_address(res.pairs)
+            flat = np.frombuffer(buf, dtype=np.uint32).reshape(n, 2)
+        else:
+            flat = np.zeros((0, 2), dtype=np.uint32)
+        if copy:
+            flat = flat.copy()
+        offs = [res.rank_offsets[i] for i in range(res.num_rank + 1)]
+        bufs = [flat[offs[i]:offs[i + 1]] for i in range(res.num_rank)]
+        return ResultBuffers(bufs, [8 * (offs[i + 1] - offs[i]) for i in range(res.num_rank)])
+
+    def RecordLogs(self, print_=False):
+        st = Stats()
+        check(lib().spj_record_logs(self._h, ctypes.byref(st), int(print_)))
+        return st.as_dict()
+
+    def close(self):
+        if self._h:
+            lib().spj_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    """Device-resident plan: allocation at creation; execute() allocates nothing."""
+
+    def __init__(self, n_r, n_s, design=None):
+        self._p = ctypes.c_void_p()
+        design = design if design is not None else make_design()
+        check(lib().spj_plan_create(n_r, n_s, ctypes.byref(design), ctypes.byref(self._p)))
+        self.n_r, self.n_s = n_r, n_s
+
+    @property
+    def output_capacity(self):
+        return lib().spj_plan_output_capacity(self._p)
+
+    def execute(self, r_ptr, s_ptr, out_ptr, n_out_ptr, stream=0):
+        check(lib().spj_plan_execute(self._p, r_ptr, s_ptr, out_ptr, n_out_ptr, stream))
+
+    def stats(self):
+        st = Stats()
+        check(lib().spj_plan_stats(self._p, ctypes.byref(st)))
+        return st.as_dict()
+
+    def kernel_times(self, back=0):
+        kt = KernelTimes()
+        check(lib().spj_plan_kernel_times(self._p, back, ctypes.byref(kt)))
+        return kt.as_dict()
+
+    def close(self):
+        if self._p:
+            lib().spj_plan_destroy(self._p)
+            self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,73 @@
+"""CPU tests of the C-ABI library: it loads, exports every symbol the header
+declares, keeps the reference's defaults, refuses to run without a GPU, and its
+host-side generator produces the specified relations."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "spidjoin.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(spj_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_exports_every_declared_symbol(spj):
+    L = ctypes.CDLL(spj.LIB_PATH)
+    syms = header_symbols()
+    assert len(syms) >= 19
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+    assert set(spj.EXPORTS) == set(syms)
+
+
+def test_design_defaults_follow_reference(spj):
+    d = spj.make_design()
+    # include/idpHandler.hpp:131-145
+    assert (d.input_size, d.rank_num, d.zipf_factor, d.rs_ratio, d.rank_set, d.bank_set, d.join_alg) == \
+        (500000, 16, 0, 8, 1, 1, 0)
+
+
+def test_no_gpu_fails_loudly(spj):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(spj.SpjError, match="NODEVICE"):
+        spj.JoinInstance(1, 1, 1)
+    with pytest.raises(spj.SpjError, match="NODEVICE"):
+        spj.Plan(100, 100)
+
+
+def test_bad_arguments(spj):
+    with pytest.raises(spj.SpjError, match="ARG"):
+        spj.JoinInstance(4, 3, 1)  # ranks must equal groups x per group
+
+
+def test_generator_relations(spj, oracle):
+    R, S, expect = spj.generate_host(10000, 40000, 0.0, seed=123)
+    assert sorted(R[:, 0].tolist()) == list(range(1, 10001))     # permutation of 1..n
+    assert R[:, 1].tolist() == list(range(10000))                  # payload = row id
+    assert S[:, 1].tolist() == list(range(40000))
+    assert set(S[:, 0].tolist()) <= set(R[:, 0].tolist())          # foreign keys
+    assert oracle.checksum(oracle.simple_join(R, S)) == expect
+
+
+def test_generator_deterministic_across_threads(spj):
+    a = spj.generate_host(3000, 7000, 1.0, seed=9, nthreads=1)
+    b = spj.generate_host(3000, 7000, 1.0, seed=9, nthreads=7)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+
+
+@pytest.mark.parametrize("s", [1.0, 1.5])
+def test_generator_zipf_head(spj, s):
+    n, m = 1 << 14, 1 << 18
+    R, S, _ = spj.generate_host(n, m, s, seed=99)
+    counts = np.bincount(S[:, 0], minlength=n + 1)
+    top = counts.max() / m
+    h = sum(1.0 / k ** s for k in range(1, n + 1))
+    assert abs(top - 1.0 / h) < 0.01, (top, 1.0 / h)

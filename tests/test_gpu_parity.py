@@ -1,0 +1,157 @@
+"""GPU parity: the CUDA join through the C ABI against the oracle on the same
+seeded inputs -- exact pair multisets (canonical sort), counts and checksums."""
+import ctypes
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import main_cc_tables
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def run_instance(spj, R, S, ranks=1, rank_sets=1, **design_kw):
+    inst = spj.JoinInstance(ranks, rank_sets, ranks // rank_sets)
+    inst.LoadColumn(R, R.shape[0], "left")
+    inst.LoadColumn(S, S.shape[0], "right")
+    d = spj.make_design(rank_num=ranks, rank_set=rank_sets, **design_kw)
+    inst.PrepareJoin(d)
+    inst.StartJoin(d)
+    res = inst.FinishJoin()
+    logs = inst.RecordLogs()
+    inst.close()
+    return res, logs
+
+
+def same_multiset(oracle, a, b):
+    return a.shape == b.shape and np.array_equal(oracle.sort_pairs(a), oracle.sort_pairs(b))
+
+
+@pytest.mark.parametrize("case", json.load(open(os.path.join(GOLDEN, "kat_main_cc.json")))["cases"],
+                         ids=lambda c: f"N{c['N']}x{c['ratio']}")
+def test_kat_main_cc(spj, oracle, case):
+    R, S = main_cc_tables(case["N"], case["ratio"])
+    res, _ = run_instance(spj, R, S)
+    out = res.pairs()
+    assert out.shape[0] == case["n_pairs"]
+    assert oracle.checksum(out) == case["checksum"]
+    assert sum(res.byte_sizes) == 8 * case["n_pairs"]
+
+
+@pytest.mark.parametrize("zipf", [0.0, 1.0, 1.5])
+@pytest.mark.parametrize("n_r,ratio", [(1 << 10, 2), (1 << 16, 4), (100003, 3), (1 << 20, 2)])
+def test_generated_joins(spj, oracle, zipf, n_r, ratio):
+    R, S, expect = spj.generate_host(n_r, n_r * ratio, zipf, seed=n_r + int(10 * zipf))
+    res, logs = run_instance(spj, R, S)
+    out = res.pairs()
+    assert out.shape[0] == S.shape[0]
+    assert oracle.checksum(out) == expect
+    assert same_multiset(oracle, out, oracle.simple_join(R, S))
+    assert logs["n_pairs"] == S.shape[0]
+
+
+@pytest.mark.parametrize("layout", [(1, 1, 1, 0), (4, 4, 1, 1), (16, 4, 4, 1), (4, 1, 16, 1), (4, 1, 4, 0)])
+def test_replication_groups_bit_exact(spj, oracle, layout):
+    ranks, rsets, bset, mode = layout
+    R, S, expect = spj.generate_host(1 << 17, 1 << 19, 1.5, seed=31)
+    res, logs = run_instance(spj, R, S, ranks=ranks, rank_sets=rsets, bank_set=bset, skew_mode=mode)
+    out = res.pairs()
+    assert out.shape[0] == S.shape[0] and oracle.checksum(out) == expect
+
+
+@pytest.mark.parametrize("bits,slots", [(6, 4096), (9, 2048), (12, 12288), (14, 12288), (3, 28000)])
+def test_tuning_variants(spj, oracle, bits, slots):
+    R, S, expect = spj.generate_host(1 << 15, 1 << 17, 1.0, seed=bits)
+    res, logs = run_instance(spj, R, S, radix_bits=bits, table_slots=slots, unit_tuples=4096)
+    out = res.pairs()
+    assert oracle.checksum(out) == expect and out.shape[0] == S.shape[0]
+    assert logs["radix_bits"] == bits
+
+
+def test_non_fk_and_key_zero(spj, oracle):
+    rng = np.random.default_rng(5)
+    R = np.stack([rng.permutation(np.arange(1, 50001)), rng.integers(0, 2**32, 50000)], 1).astype(np.uint32)
+    R[::97, 0] = 0
+    S = np.stack([rng.integers(0, 100000, 300001), np.arange(300001)], 1).astype(np.uint32)
+    res, _ = run_instance(spj, R, S)
+    assert same_multiset(oracle, res.pairs(), oracle.simple_join(R, S))
+
+
+def test_duplicate_r_keys_one_match_each(spj, oracle):
+    rng = np.random.default_rng(6)
+    keys = rng.integers(1, 2000, 40000)
+    R = np.stack([keys, np.arange(40000)], 1).astype(np.uint32)
+    S = np.stack([rng.integers(1, 4000, 100000), np.arange(100000)], 1).astype(np.uint32)
+    out = run_instance(spj, R, S)[0].pairs()
+    present = np.zeros(4001, bool)
+    present[keys] = True
+    assert out.shape[0] == int(present[S[:, 0]].sum())        # one match per S tuple with a key in R
+    assert np.array_equal(np.sort(out[:, 1]), np.sort(S[present[S[:, 0]], 1]))
+    assert np.array_equal(R[out[:, 0], 0], S[out[:, 1], 0])   # each pair joins equal keys
+
+
+@pytest.mark.parametrize("nr,ns", [(0, 10), (10, 0), (0, 0), (1, 1), (3, 5), (1, 100000), (100000, 1)])
+def test_edge_sizes(spj, oracle, nr, ns):
+    rng = np.random.default_rng(nr * 7 + ns)
+    R = np.stack([rng.permutation(np.arange(1, nr + 1)), np.arange(nr)], 1).astype(np.uint32).reshape(nr, 2)
+    S = np.stack([rng.integers(1, max(nr, 1) + 1, ns), np.arange(ns)], 1).astype(np.uint32).reshape(ns, 2)
+    res, _ = run_instance(spj, R, S)
+    assert same_multiset(oracle, res.pairs(), oracle.simple_join(R, S))
+
+
+def test_partition_histogram_matches_count_kernel(spj, oracle):
+    import torch
+    R, S, _ = spj.generate_host(1 << 18, 1 << 18, 1.0, seed=4)
+    dR = torch.from_numpy(R.view(np.int32)).cuda()
+    for bits in (6, 10, 14):
+        hist = torch.zeros(1 << bits, dtype=torch.int32, device="cuda")
+        spj.check(spj.lib().spj_partition_histogram(dR.data_ptr(), R.shape[0], bits, hist.data_ptr(), None))
+        torch.cuda.synchronize()
+        assert np.array_equal(hist.cpu().numpy().view(np.uint32), oracle.partition_count(R, 1 << bits))
+
+
+def test_device_plan_full_size_property(spj):
+    """|R| = 2^24, |S| = 2^26 Zipf 1.0 on device: pair count and checksum equal the
+    generator's exact answer (a size-independent property; the oracle is not needed)."""
+    import torch
+    n_r, n_s = 1 << 24, 1 << 26
+    dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
+    dS = torch.empty((n_s, 2), dtype=torch.int32, device="cuda")
+    exp = torch.zeros(1, dtype=torch.int64, device="cuda")
+    spj.check(spj.lib().spj_generate_device(77, n_r, n_s, 1.0, dR.data_ptr(), dS.data_ptr(), exp.data_ptr(), None))
+    plan = spj.Plan(n_r, n_s, spj.make_design(rank_num=1))
+    out = torch.empty((plan.output_capacity, 2), dtype=torch.int32, device="cuda")
+    n_out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    cs = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for _ in range(2):  # twice: the plan is reusable
+        plan.execute(dR.data_ptr(), dS.data_ptr(), out.data_ptr(), n_out.data_ptr(), 0)
+        spj.check(spj.lib().spj_checksum_device(out.data_ptr(), n_out.data_ptr(), cs.data_ptr(), None))
+        torch.cuda.synchronize()
+        st = plan.stats()
+        assert int(n_out.item()) == n_s
+        assert int(cs.item()) == int(exp.item())
+        assert st["n_pairs"] == n_s
+    plan.close()
+
+
+def test_device_generator_matches_host(spj):
+    import torch
+    n_r, n_s = 1 << 16, 1 << 18
+    for z in (0.0, 1.0):
+        R, S, exp_h = spj.generate_host(n_r, n_s, z, seed=123)
+        dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
+        dS = torch.empty((n_s, 2), dtype=torch.int32, device="cuda")
+        exp = torch.zeros(1, dtype=torch.int64, device="cuda")
+        spj.check(spj.lib().spj_generate_device(123, n_r, n_s, z, dR.data_ptr(), dS.data_ptr(), exp.data_ptr(),
+                                                None))
+        torch.cuda.synchronize()
+        assert np.array_equal(dR.cpu().numpy().view(np.uint32), R)
+        diff = (dS.cpu().numpy().view(np.uint32) != S).any(axis=1).sum()
+        if z == 0.0:
+            assert diff == 0 and int(exp.item()) & (2**64 - 1) == exp_h
+        else:
+            assert diff <= 2  # libm and CUDA double exp/log may differ in the last ulp
