@@ -31,6 +31,8 @@ WORKLOADS = {
            "plain equi-join |R|=2^27 |S|=2^29 Zipf 1.0, replication groups of 4 (-r 4 -R 4 -B 1)"),
     "c3": (1 << 26, 1 << 29, 1.5, (4, 4, 1), "plain equi-join |R|=2^26 |S|=2^29 Zipf 1.5, groups of 4"),
     "c2u": (1 << 27, 1 << 29, 0.0, (4, 4, 1), "plain equi-join |R|=2^27 |S|=2^29 uniform, groups of 4"),
+    # 1/8 of C2 (same Zipf and layout): the small case for ncu captures
+    "c2s": (1 << 24, 1 << 26, 1.0, (4, 4, 1), "plain equi-join |R|=2^24 |S|=2^26 Zipf 1.0, groups of 4"),
 }
 SEED = 0x5EED5EED
 METRIC = "join tuples/s (|R|+|S|)"
@@ -169,7 +171,8 @@ def run_ours(args):
     n_r, n_s, zipf, (ranks, rsets, bset), desc = WORKLOADS[args.workload]
     design = spj.make_design(rank_num=ranks, rank_set=rsets, bank_set=bset, join_alg=args.alg,
                              skew_mode=args.skew, input_size=n_r, rs_ratio=max(n_s // n_r, 1),
-                             zipf_factor=int(round(zipf * 100)))
+                             zipf_factor=int(round(zipf * 100)), radix_bits=args.bits,
+                             table_slots=args.slots, unit_tuples=args.unit)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
     lib = spj.lib()
@@ -320,6 +323,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--alg", type=int, default=0)
     ap.add_argument("--skew", type=int, default=0)
+    ap.add_argument("--bits", type=int, default=0, help="radix bits (0 = planner)")
+    ap.add_argument("--slots", type=int, default=0, help="table slots per CTA (0 = planner)")
+    ap.add_argument("--unit", type=int, default=0, help="max S tuples per work unit (0 = planner)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -10,12 +10,15 @@
 
 namespace spj {
 
-constexpr int kHistThreads = 512;
+constexpr int kHistThreads = 1024;
 constexpr int kScatterThreads = 512;
-constexpr int kJoinThreads = 512;
+constexpr int kJoinThreads = 1024;
 constexpr int kOutChunk = 1024;      // output pairs reserved per warp at a time
-constexpr int kMaxHoles = 8192;      // warps of the emitting kernels (one hole each)
-constexpr int kMaxRadixBits = 14;
+constexpr int kMaxHoles = 12288;     // warps of the emitting kernels (one hole each)
+constexpr int kHoleSortSlots = 16384; // power of two >= kMaxHoles
+constexpr int kMaxRadixBits = 15;
+constexpr int kMaxPassBits = 8;      // buckets per scatter pass <= 256
+constexpr int kTile = 4096;          // tuples sorted per tile in shared memory
 constexpr int kDefaultTableSlots = 12288;  // 96 KB of shared memory
 constexpr int kDefaultUnitTuples = 65536;
 constexpr int kHeavyCap = 1024;      // heavy keys joined on the fly
@@ -24,10 +27,12 @@ constexpr int kHeavyCap = 1024;      // heavy keys joined on the fly
 struct RelDev {
     const Tuple *in;     // input column (device)
     Tuple *out;          // partitioned column
+    Tuple *tmp;          // pass-1 (coarse) layout when two passes are used
     uint32_t n;          // tuples
     uint32_t chunk;      // tuples per chunk (even)
     uint32_t nchunks;
     uint32_t *hist;      // [nchunks][F] counts, then exclusive offsets within each partition
+    uint32_t *chist;     // [nchunks][F1] counts of the coarse buckets (two-pass scatter)
     uint32_t *total;     // [F] tuples per partition
     uint32_t *base;      // [F] partition starts
 };
@@ -59,10 +64,12 @@ struct Counters {
     unsigned long long n_out;         // final pair count
     unsigned long long gap_total;     // fix-up: hole space below n_out
     unsigned int n_gaps, n_data;
+    unsigned int item_count, item_next;  // pass-2 work list
 };
 
 struct JoinParams {
     int bits;             // radix bits of the partition fan-out
+    int fine_bits;        // bits resolved by the second scatter pass (0 = one pass)
     int table_slots;      // shared-memory table entries (8 bytes each)
     int alg;              // spj_join_alg
     int skew_mode;
@@ -75,6 +82,8 @@ struct PlanDev {
     RelDev rel[2];        // 0 = R, 1 = S
     Unit *units;
     uint32_t max_units;
+    uint4 *items;         // pass-2 work items: (relation, coarse bucket, first chunk, end chunk)
+    uint32_t max_items;
     Hole *holes;
     Hole *gaps;           // fix-up scratch
     Hole *datas;
@@ -96,6 +105,7 @@ struct spj_plan {
     int device = 0;
     int num_sms = 0;
     int join_blocks = 0;
+    uint32_t item_target = 0;    // tuples per pass-2 work item
     void *arena = nullptr;        // one device allocation for all scratch
     size_t arena_bytes = 0;
     static constexpr int kRing = 128;   // executions whose kernel times are kept

@@ -22,6 +22,7 @@
 // needed), finish_join.c (output framing: dense, no padding).
 #include <cuda_runtime.h>
 
+#include "spj_async.cuh"
 #include "spj_internal.h"
 
 namespace spj {
@@ -46,7 +47,7 @@ __device__ __forceinline__ void chunk_of(const PlanDev &P, unsigned bid, int &re
 // ------------------------------------------------------------- histogram --
 // glb_partition_count.c:119-236 on B200: each CTA counts one contiguous chunk
 // into a shared-memory histogram; key-0 tuples are skipped (:190-192).
-__global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P, int bits) {
+__global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P, int bits, int b2) {
     extern __shared__ uint32_t sh[];
     const uint32_t F = 1u << bits, mask = F - 1;
     int rel;
@@ -82,6 +83,17 @@ __global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P, int bits) {
     __syncthreads();
     uint32_t *out = R.hist + (size_t)c * F;
     for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) out[i] = sh[i];
+    if (b2 > 0) {  // per-chunk counts of the coarse buckets (the pass-2 work list)
+        const uint32_t f1 = F >> b2, q_per = 1u << b2;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (uint32_t cb = warp; cb < f1; cb += blockDim.x >> 5) {
+            uint32_t sum = 0;
+            for (uint32_t q = lane; q < q_per; q += 32) sum += sh[(cb << b2) + q];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) R.chist[(size_t)c * f1 + cb] = sum;
+        }
+    }
 }
 
 // Per partition: exclusive offsets of each chunk inside the partition (in place)
@@ -146,51 +158,257 @@ __global__ void __launch_bounds__(1024) k_basescan(PlanDev P, int bits) {
 }
 
 // --------------------------------------------------------------- scatter --
-// glb_partition_packet.c:420-464 plus the rotate-and-stream shuffle, as one
-// pass: every CTA owns exact write cursors for its chunk's share of each
-// partition (from the histogram), so no global atomics are needed.
-__global__ void __launch_bounds__(kScatterThreads) k_scatter(PlanDev P, int bits) {
-    extern __shared__ uint32_t cursor[];
+// The partition id p = glb_partition_hash(key) & (F-1) is split into a coarse
+// bucket (its high b1 bits) and a fine bucket (its low b2 bits). Pass 1 moves
+// every chunk's tuples to their coarse region, pass 2 every (chunk, coarse)
+// segment to its final fine positions; with b2 = 0 pass 1 is the only pass. No
+// pass has more than 256 buckets, and each CTA sorts a 4096-tuple tile by bucket
+// in shared memory before it writes, so stores leave in runs of ~16-32 tuples
+// (128-256 bytes) and only #CTAs x 256 write fronts are open at any time --
+// few enough to stay in L2. Positions are exact (from the count pass): no global
+// atomics. This replaces glb_partition_packet.c:420-464 and the host-mediated
+// rotate-and-stream shuffle (queryHostFunc.cc:481-777); on one GPU the shuffle
+// is the scatter itself.
+struct __align__(128) TileSmem {
+    Tuple inbuf[2][kTile];     // bulk-copy double buffer of input tiles
+    Tuple stage[kTile];        // tile sorted by bucket
+    uint8_t bkt[kTile];
+    uint32_t cnt[256];
+    uint32_t off[256];
+    uint32_t wpos[256];        // cursor - off: global position of stage slot j is wpos[b] + j
+    uint32_t cursor[256];
+    uint64_t bar[2];
+    uint32_t valid;
+    uint32_t seg_begin, seg_len;
+    uint32_t item;
+};
+
+// Scatters in[b, e) to out[cursor[bucket] ...], advancing the cursors. Input
+// tiles arrive by bulk copy (TMA) into a double buffer, so the next tile is in
+// flight while this one is sorted and written. A tuple at an odd boundary index
+// is moved with an ordinary load (bulk copies need 16-byte alignment).
+// Returns false (the same value in every thread) when a bulk copy timed out.
+template <typename BucketFn>
+__device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint32_t b, uint32_t e,
+                                              Tuple *__restrict__ out, TileSmem &S, int nb, BucketFn bucket_of,
+                                              uint32_t (&uses)[2], unsigned int *err) {
+    constexpr int PER = kTile / kScatterThreads;
+    uint2 *o2 = reinterpret_cast<uint2 *>(out);
+    if (b >= e) return true;
+    if (threadIdx.x < 2) {  // boundary tuples at odd indices
+        const bool head = threadIdx.x == 0;
+        const uint32_t idx = head ? b : e - 1;
+        // head: index b when odd; tail: index e-1 when e is odd, unless that is the head
+        if ((head && (b & 1u)) || (!head && (e & 1u) && !((b & 1u) && e - 1 == b))) {
+            const Tuple t = in[idx];
+            if (t.key) {
+                const uint32_t pos = atomicAdd(&S.cursor[bucket_of(t.key)], 1u);
+                o2[pos] = make_uint2(t.key, t.pay);
+            }
+        }
+    }
+    __syncthreads();
+    const uint32_t tb = b + (b & 1u), te = e - (e & 1u);
+    if (tb >= te) return true;
+    const uint32_t ntiles = (te - tb + kTile - 1) / kTile;
+    if (threadIdx.x == 0) {
+        const uint32_t n0 = min((uint32_t)kTile, te - tb);
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&S.bar[0], n0 * 8);
+        bulk_load(S.inbuf[0], in + tb, n0 * 8, &S.bar[0]);
+    }
+    for (uint32_t t = 0; t < ntiles; t++) {
+        const int buf = t & 1;
+        const uint32_t t0 = tb + t * kTile;
+        const uint32_t nt = min((uint32_t)kTile, te - t0);
+        if (threadIdx.x == 0 && t + 1 < ntiles) {
+            const uint32_t t1 = t0 + kTile, n1 = min((uint32_t)kTile, te - t1);
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&S.bar[buf ^ 1], n1 * 8);
+            bulk_load(S.inbuf[buf ^ 1], in + t1, n1 * 8, &S.bar[buf ^ 1]);
+        }
+        const bool ok = mbar_wait(&S.bar[buf], uses[buf] & 1u, err);
+        uses[buf]++;
+        if (__syncthreads_or(!ok)) {  // a copy timed out (error bit set): all threads stop alike
+            // copies already issued may still land: give them a bounded wait before leaving
+            if (threadIdx.x == 0 && t + 1 < ntiles) mbar_wait(&S.bar[buf ^ 1], uses[buf ^ 1] & 1u, err);
+            return false;
+        }
+        Tuple v[PER];
+        uint32_t br[PER];  // bucket << 16 | rank inside the tile; 0xffff0000 = no tuple
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t idx = threadIdx.x + k * kScatterThreads;
+            br[k] = 0xffff0000u;
+            v[k] = idx < nt ? S.inbuf[buf][idx] : Tuple{0u, 0u};
+            if (v[k].key) {
+                const uint32_t bk = (uint32_t)bucket_of(v[k].key);
+                br[k] = (bk << 16) | atomicAdd(&S.cnt[bk], 1u);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {  // exclusive scan of the <= 256 bucket counts
+            const int lane = threadIdx.x;
+            uint32_t c[8], sum = 0;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int j = lane * 8 + i;
+                c[i] = j < nb ? S.cnt[j] : 0;
+                sum += c[i];
+            }
+            uint32_t incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += x;
+            }
+            uint32_t run = incl - sum;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int j = lane * 8 + i;
+                if (j < nb) {
+                    S.off[j] = run;
+                    S.wpos[j] = S.cursor[j] - run;
+                    S.cursor[j] += c[i];
+                    S.cnt[j] = 0;
+                }
+                run += c[i];
+            }
+            if (lane == 31) S.valid = incl;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t bk = br[k] >> 16;
+            if (bk != 0xffffu) {
+                const uint32_t slot = S.off[bk] + (br[k] & 0xffffu);
+                S.stage[slot] = v[k];
+                S.bkt[slot] = (uint8_t)bk;
+            }
+        }
+        __syncthreads();
+        const uint32_t valid = S.valid;
+        for (uint32_t j = threadIdx.x; j < valid; j += kScatterThreads) {
+            const Tuple x = S.stage[j];
+            o2[S.wpos[S.bkt[j]] + j] = make_uint2(x.key, x.pay);
+        }
+        // the next tile's rank phase may start: counts are zero, and its first
+        // barrier orders these reads of stage/wpos before they are rewritten
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tile_init(TileSmem &S) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) S.cnt[i] = 0;
+    if (threadIdx.x == 0) {
+        mbar_init(&S.bar[0], 1);
+        mbar_init(&S.bar[1], 1);
+        fence_mbar_init();
+    }
+}
+
+// Pass 1: one CTA per chunk. Coarse bucket P = p >> b2; the write cursor of
+// (chunk c, bucket P) is base[P << b2] + sum_q off[c][(P << b2) + q].
+__global__ void __launch_bounds__(kScatterThreads, 2) k_scatter1(PlanDev P, int bits, int b2) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
     const uint32_t F = 1u << bits, mask = F - 1;
+    const int nb = 1 << (bits - b2);
+    const int q_per = 1 << b2;
     int rel;
     unsigned c;
     chunk_of(P, blockIdx.x, rel, c);
     const RelDev R = rel == 0 ? P.rel[0] : P.rel[1];
     const uint32_t *off = R.hist + (size_t)c * F;
-    for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) cursor[i] = R.base[i] + off[i];
+    tile_init(S);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b = warp; b < nb; b += kScatterThreads / 32) {
+        uint32_t sum = 0;
+        for (int q = lane; q < q_per; q += 32) sum += off[(b << b2) + q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) S.cursor[b] = R.base[b << b2] + sum;
+    }
     __syncthreads();
-    const uint32_t b = c * R.chunk;
-    const uint32_t e = min(R.n, b + R.chunk);
-    if (b >= e) return;
-    const uint4 *in2 = reinterpret_cast<const uint4 *>(R.in);
-    uint2 *out = reinterpret_cast<uint2 *>(R.out);
-    const uint32_t b2 = b >> 1, e2 = e >> 1;
-    constexpr int U = 4;
-    for (uint32_t i = b2 + threadIdx.x; i < e2; i += U * blockDim.x) {
-        uint4 v[U];
-#pragma unroll
-        for (int k = 0; k < U; k++) {
-            uint32_t j = i + k * blockDim.x;
-            v[k] = j < e2 ? __ldcs(in2 + j) : make_uint4(0, 0, 0, 0);
-        }
-#pragma unroll
-        for (int k = 0; k < U; k++) {
-            if (v[k].x) {
-                uint32_t pos = atomicAdd(&cursor[glb_partition_hash(v[k].x) & mask], 1u);
-                out[pos] = make_uint2(v[k].x, v[k].y);
+    const uint32_t b0 = c * R.chunk;
+    const uint32_t e0 = min(R.n, b0 + R.chunk);
+    Tuple *dst = b2 ? R.tmp : R.out;
+    uint32_t uses[2] = {0, 0};
+    scatter_range(R.in, b0, e0, dst, S, nb,
+                  [=](uint32_t key) { return (int)((glb_partition_hash(key) & mask) >> b2); }, uses,
+                  &P.ctr->error);
+}
+
+// Work list of pass 2: for every (relation, coarse bucket), runs of consecutive
+// chunks holding at least `target` tuples. Within a coarse region the chunks'
+// segments follow each other in chunk order, as do the fine offsets, so cursors
+// set from a run's first chunk stay exact. A heavy single segment is its own item.
+__global__ void k_items(PlanDev P, int bits, int b2, uint32_t target) {
+    const uint32_t f1 = 1u << (bits - b2);
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * f1) return;
+    const int rel = t < f1 ? 0 : 1;
+    const uint32_t cb = t < f1 ? t : t - f1;
+    const RelDev R = rel == 0 ? P.rel[0] : P.rel[1];
+    uint32_t acc = 0, c0 = 0;
+    for (uint32_t c = 0; c < R.nchunks; c++) {
+        acc += R.chist[(size_t)c * f1 + cb];
+        if (acc >= target || c + 1 == R.nchunks) {
+            if (acc) {
+                const unsigned i = atomicAdd(&P.ctr->item_count, 1u);
+                if (i < P.max_items)
+                    P.items[i] = make_uint4((uint32_t)rel, cb, c0, c + 1);
+                else
+                    atomicOr(&P.ctr->error, 4u);
             }
-            if (v[k].z) {
-                uint32_t pos = atomicAdd(&cursor[glb_partition_hash(v[k].z) & mask], 1u);
-                out[pos] = make_uint2(v[k].z, v[k].w);
-            }
+            acc = 0;
+            c0 = c + 1;
         }
     }
-    if ((e & 1u) && threadIdx.x == 0) {
-        Tuple t = R.in[e - 1];
-        if (t.key) {
-            uint32_t pos = atomicAdd(&cursor[glb_partition_hash(t.key) & mask], 1u);
-            out[pos] = make_uint2(t.key, t.pay);
+}
+
+// Pass 2: persistent CTAs over the work list; each item scatters one run of a
+// coarse region to the final fine positions.
+__global__ void __launch_bounds__(kScatterThreads, 2) k_scatter2(PlanDev P, int bits, int b2) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
+    const uint32_t F = 1u << bits;
+    const int nb = 1 << b2;
+    const uint32_t qmask = (uint32_t)nb - 1;
+    tile_init(S);
+    uint32_t uses[2] = {0, 0};
+    const unsigned n_items = min(*(volatile unsigned *)&P.ctr->item_count, P.max_items);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            S.item = atomicAdd(&P.ctr->item_next, 1u);
+            S.seg_begin = 0;
+            S.seg_len = 0;
         }
+        __syncthreads();
+        const unsigned it = S.item;
+        if (it >= n_items) break;
+        const uint4 item = P.items[it];
+        const RelDev R = item.x == 0 ? P.rel[0] : P.rel[1];
+        const uint32_t cb = item.y, c0 = item.z, c1 = item.w;
+        const uint32_t *off = R.hist + (size_t)c0 * F;
+        const uint32_t *nxt = c1 < R.nchunks ? R.hist + (size_t)c1 * F : R.total;
+        uint32_t mine_off = 0, mine_cnt = 0;
+        for (int q = threadIdx.x; q < nb; q += kScatterThreads) {
+            const uint32_t p = (cb << b2) + q;
+            const uint32_t o = off[p];
+            mine_off += o;
+            mine_cnt += nxt[p] - o;
+            S.cursor[q] = R.base[p] + o;
+        }
+        if (mine_off) atomicAdd(&S.seg_begin, mine_off);
+        if (mine_cnt) atomicAdd(&S.seg_len, mine_cnt);
+        __syncthreads();
+        const uint32_t beg = R.base[cb << b2] + S.seg_begin;
+        const bool ok = scatter_range(R.tmp, beg, beg + S.seg_len, R.out, S, nb,
+                                      [=](uint32_t key) { return (int)(glb_partition_hash(key) & qmask); }, uses,
+                                      &P.ctr->error);
+        __syncthreads();
+        if (!ok) break;
     }
 }
 
@@ -297,17 +515,27 @@ __device__ __forceinline__ void build_table(const PlanDev &P, const JoinParams &
     __syncthreads();
     const uint32_t nr = P.rel[0].total[p];
     const Tuple *pr = P.rel[0].out + P.rel[0].base[p];
-    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
-        const Tuple t = pr[i];
-        const unsigned long long ent = ((unsigned long long)t.pay << 32) | t.key;
-        uint32_t s = slot_of(t.key, jp.bits, ts);
-        for (uint32_t step = 0;; step++) {
-            const unsigned long long prev = atomicCAS(&table[s], 0ull, ent);
-            if (prev == 0ull || (uint32_t)prev == t.key) break;
-            if (++s == ts) s = 0;
-            if (step >= ts) {
-                atomicOr(&P.ctr->error, 1u);
-                break;
+    constexpr int B = 4;  // loads in flight per thread
+    for (uint32_t i0 = threadIdx.x; i0 < nr; i0 += B * blockDim.x) {
+        Tuple t[B];
+#pragma unroll
+        for (int k = 0; k < B; k++) {
+            const uint32_t i = i0 + k * blockDim.x;
+            t[k] = i < nr ? pr[i] : Tuple{0u, 0u};
+        }
+#pragma unroll
+        for (int k = 0; k < B; k++) {
+            if (t[k].key == 0) continue;
+            const unsigned long long ent = ((unsigned long long)t[k].pay << 32) | t[k].key;
+            uint32_t s = slot_of(t[k].key, jp.bits, ts);
+            for (uint32_t step = 0;; step++) {
+                const unsigned long long prev = atomicCAS(&table[s], 0ull, ent);
+                if (prev == 0ull || (uint32_t)prev == t[k].key) break;
+                if (++s == ts) s = 0;
+                if (step >= ts) {
+                    atomicOr(&P.ctr->error, 1u);
+                    break;
+                }
             }
         }
     }
@@ -344,7 +572,7 @@ __device__ __forceinline__ bool next_unit(const PlanDev &P, unsigned n_units, un
 }
 
 // ----------------------------------------------------- partitioned hash join --
-__global__ void __launch_bounds__(kJoinThreads) k_join_phj(PlanDev P, JoinParams jp) {
+__global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P, JoinParams jp) {
     extern __shared__ unsigned long long table[];
     __shared__ unsigned s_slot;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -384,9 +612,54 @@ __global__ void __launch_bounds__(kJoinThreads) k_join_phj(PlanDev P, JoinParams
 // partly used, so the unused slots form at most one hole per warp at a chunk's
 // tail. With N = reserved - holes, the pairs stored at positions >= N outside
 // holes move into the holes below N.
+// Exclusive scan in place of a[0..n) (n <= 12 * 1024) by a 1024-thread block;
+// returns the total. Each thread scans 12 consecutive entries.
+__device__ unsigned long long block_exclusive_scan(unsigned long long *a, unsigned n, unsigned long long *warp_tot) {
+    constexpr int PER = 12;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned beg = threadIdx.x * PER;
+    unsigned long long v[PER], sum = 0;
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        v[i] = beg + i < n ? a[beg + i] : 0ull;
+        sum += v[i];
+    }
+    unsigned long long incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += t;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned long long w = warp_tot[lane];
+        unsigned long long wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= (unsigned)o) wi += t;
+        }
+        warp_tot[lane] = wi - w;
+        if (lane == 31) warp_tot[32] = wi;
+    }
+    __syncthreads();
+    unsigned long long run = warp_tot[warp] + incl - sum;
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        if (beg + i < n) a[beg + i] = run;
+        run += v[i];
+    }
+    const unsigned long long total = warp_tot[32];
+    __syncthreads();
+    return total;
+}
+
 __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
-    extern __shared__ unsigned long long keys[];  // kMaxHoles entries
-    __shared__ unsigned long long red[32];
+    extern __shared__ unsigned long long keys[];  // kHoleSortSlots sorted holes, then kMaxHoles scan slots
+    __shared__ unsigned long long warp_tot[33];
+    __shared__ unsigned s_nl, s_i0;
+    unsigned long long *scan = keys + kHoleSortSlots;
     const unsigned nh = min(P.ctr->hole_count, (unsigned)kMaxHoles);
     unsigned npow = 1;
     while (npow < nh) npow <<= 1;
@@ -398,6 +671,10 @@ __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
             keys[i] = ~0ull;
         }
     }
+    if (threadIdx.x == 0) {
+        s_nl = 0;
+        s_i0 = nh;
+    }
     __syncthreads();
     for (unsigned k = 2; k <= npow; k <<= 1) {
         for (unsigned j = k >> 1; j > 0; j >>= 1) {
@@ -405,8 +682,7 @@ __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
                 const unsigned ixj = i ^ j;
                 if (ixj > i) {
                     const unsigned long long a = keys[i], b = keys[ixj];
-                    const bool up = (i & k) == 0;
-                    if ((a > b) == up) {
+                    if ((a > b) == ((i & k) == 0)) {
                         keys[i] = b;
                         keys[ixj] = a;
                     }
@@ -415,46 +691,46 @@ __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
             __syncthreads();
         }
     }
-    // total hole length
-    unsigned long long part = 0;
-    for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) part += keys[i] & 2047ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+    // total hole length -> N
+    for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) scan[i] = keys[i] & 2047ull;
     __syncthreads();
+    const unsigned long long H = block_exclusive_scan(scan, nh, warp_tot);
+    const unsigned long long total = P.ctr->out_reserved;
+    const unsigned long long N = total - H;
+    // parts of each hole below N (gaps to fill) and above N (skipped by the data)
+    for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) {
+        const unsigned long long b = keys[i] >> 11, e = b + (keys[i] & 2047ull);
+        scan[i] = b < N ? (e < N ? e : N) - b : 0ull;
+        if (b < N && (i + 1 == nh || (keys[i + 1] >> 11) >= N)) s_nl = i + 1;       // holes below N: a prefix
+        if (e > N && (i == 0 || (keys[i - 1] >> 11) + (keys[i - 1] & 2047ull) <= N)) s_i0 = i;  // above: a suffix
+    }
+    __syncthreads();
+    const unsigned long long G = block_exclusive_scan(scan, nh, warp_tot);
+    const unsigned nl = s_nl, i0 = s_i0;
+    for (unsigned i = threadIdx.x; i < nl; i += blockDim.x) {
+        P.gaps[i].begin = keys[i] >> 11;
+        P.gap_off[i] = scan[i];
+    }
+    __syncthreads();
+    for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) {
+        const unsigned long long b = keys[i] >> 11, e = b + (keys[i] & 2047ull);
+        scan[i] = e > N ? e - (b > N ? b : N) : 0ull;
+    }
+    __syncthreads();
+    block_exclusive_scan(scan, nh, warp_tot);
+    for (unsigned i = i0 + threadIdx.x; i < nh; i += blockDim.x) {
+        const unsigned long long b = keys[i] >> 11, e = b + (keys[i] & 2047ull);
+        const unsigned long long ub = b > N ? b : N;
+        // data elements stored before this hole, and holes' length up to and including it
+        P.datas[i - i0].begin = ub - N - scan[i];
+        P.data_off[i - i0] = scan[i] + (e - ub);
+    }
     if (threadIdx.x == 0) {
-        unsigned long long H = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); i++) H += red[i];
-        const unsigned long long total = P.ctr->out_reserved;
-        const unsigned long long N = total - H;
         P.ctr->n_out = N;
         if (P.n_out_user) *P.n_out_user = N;
-        // Serial pass over the (sorted) holes: prefix sums of the parts below
-        // and above N. nh is at most kMaxHoles.
-        unsigned long long g = 0, cincl = 0;
-        unsigned nl = 0, nd = 0;
-        for (unsigned i = 0; i < nh; i++) {
-            const unsigned long long b = keys[i] >> 11, len = keys[i] & 2047ull, e = b + len;
-            if (b < N) {
-                const unsigned long long lo = (e < N ? e : N) - b;
-                P.gaps[nl].begin = b;
-                P.gap_off[nl] = g;
-                g += lo;
-                nl++;
-            }
-            if (e > N) {
-                const unsigned long long ub = b > N ? b : N;
-                const unsigned long long ulen = e - ub;
-                // data elements located before this hole
-                P.datas[nd].begin = ub - N - cincl;
-                cincl += ulen;
-                P.data_off[nd] = cincl;
-                nd++;
-            }
-        }
-        P.ctr->gap_total = g;
+        P.ctr->gap_total = G;
         P.ctr->n_gaps = nl;
-        P.ctr->n_data = nd;
+        P.ctr->n_data = nh - i0;
     }
 }
 
@@ -554,23 +830,29 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
     const unsigned F = 1u << bits;
     const unsigned nchunks = P.rel[0].nchunks + P.rel[1].nchunks;
     const size_t hsmem = (size_t)F * 4;
+    const int b2 = jp.fine_bits;
     cudaEvent_t *ev = pl->have_events ? pl->ring[pl->ring_next] : nullptr;
     auto mark = [&](int i) {
         if (ev) cudaEventRecord(ev[i], st);
     };
     mark(0);
-    k_hist<<<nchunks, kHistThreads, hsmem, st>>>(P, bits);
+    k_hist<<<nchunks, kHistThreads, hsmem, st>>>(P, bits, b2);
     mark(1);
     k_colscan<<<dim3((F + 255) / 256, 2), 256, 0, st>>>(P, bits);
     k_basescan<<<2, 1024, 0, st>>>(P, bits);
     mark(2);
-    k_scatter<<<nchunks, kScatterThreads, hsmem, st>>>(P, bits);
+    k_scatter1<<<nchunks, kScatterThreads, sizeof(TileSmem), st>>>(P, bits, b2);
+    if (b2) {
+        const uint32_t f1 = 1u << (bits - b2);
+        k_items<<<(2 * f1 + 255) / 256, 256, 0, st>>>(P, bits, b2, pl->item_target);
+        k_scatter2<<<pl->num_sms * 2, kScatterThreads, sizeof(TileSmem), st>>>(P, bits, b2);
+    }
     mark(3);
     k_units<<<(F + 255) / 256, 256, 0, st>>>(P, bits, jp);
     mark(4);
     k_join_phj<<<pl->join_blocks, kJoinThreads, (size_t)jp.table_slots * 8, st>>>(P, jp);
     mark(5);
-    k_fixup_prep<<<1, 1024, (size_t)kMaxHoles * 8, st>>>(P);
+    k_fixup_prep<<<1, 1024, (size_t)(kHoleSortSlots + kMaxHoles) * 8, st>>>(P);
     k_fixup_copy<<<pl->num_sms * 2, 256, 0, st>>>(P);
     mark(6);
     if (ev) {
@@ -581,7 +863,7 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
 }
 
 // Kernel launches of one execution (for launch accounting).
-int pipeline_launches() { return 8; }
+int pipeline_launches(const spj_plan *pl) { return pl->jp.fine_bits ? 10 : 8; }
 
 cudaError_t configure_kernels(int table_slots, int *join_blocks_per_sm) {
     cudaError_t e;
@@ -590,12 +872,20 @@ cudaError_t configure_kernels(int table_slots, int *join_blocks_per_sm) {
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (1 << kMaxRadixBits) * 4);
     if (e) return e;
-    e = cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (1 << kMaxRadixBits) * 4);
-    if (e) return e;
     // the largest table any plan may use, so plans of different sizes coexist
     e = cudaFuncSetAttribute(k_join_phj, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - 1024);
     if (e) return e;
-    e = cudaFuncSetAttribute(k_fixup_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxHoles * 8);
+    e = cudaFuncSetAttribute(k_scatter1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));
+    if (e) return e;
+    e = cudaFuncSetAttribute(k_scatter2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));
+    if (e) return e;
+    for (const void *k : {(const void *)k_scatter1, (const void *)k_scatter2, (const void *)k_join_phj,
+                          (const void *)k_hist})
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared)))
+            return e;
+    e = cudaFuncSetAttribute(k_fixup_prep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (kHoleSortSlots + kMaxHoles) * 8);
     if (e) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(join_blocks_per_sm, k_join_phj, kJoinThreads,
                                                          (size_t)table_slots * 8);

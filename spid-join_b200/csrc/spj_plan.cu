@@ -2,6 +2,7 @@
 // JoinInstance-shaped handle of the C ABI, the synthetic-data generator and the
 // error reporting. No CPU join path exists: every join runs on the GPU.
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -110,7 +111,7 @@ static int validate_design(const spj_design_t *d) {
     if (d->skew_mode != SPJ_SKEW_ADAPTIVE && d->skew_mode != SPJ_SKEW_FIXED)
         return set_error(SPJ_E_ARG, "skew_mode must be 0 (adaptive) or 1 (fixed)");
     if (d->radix_bits < 0 || d->radix_bits > kMaxRadixBits)
-        return set_error(SPJ_E_ARG, "radix_bits must be in [0, 14]");
+        return set_error(SPJ_E_ARG, "radix_bits must be in [0, 15]");
     if (d->table_slots < 0 || d->unit_tuples < 0) return set_error(SPJ_E_ARG, "negative tuning value");
     return SPJ_OK;
 }
@@ -135,17 +136,29 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
     const spj_design_t &d = *design;
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    jp.table_slots = d.table_slots > 0 ? d.table_slots : kDefaultTableSlots;
-    jp.table_slots = std::min(jp.table_slots, (max_smem - 1024) / 8);
+    const int max_slots = (max_smem - 1024) / 8;
+    int ts = d.table_slots > 0 ? std::min(d.table_slots, max_slots) : kDefaultTableSlots;
     if (d.radix_bits > 0) {
         jp.bits = d.radix_bits;
     } else {
-        // mean R partition at most 2/3 of the table, at least 64 partitions per rank
-        const uint64_t target = (uint64_t)jp.table_slots * 2 / 3;
-        int need = ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + target - 1) / target));
-        int minb = ceil_log2((uint64_t)64 * d.rank_num);
-        jp.bits = std::min(std::max(need, minb), kMaxRadixBits);
+        // Mean R partition at a third of the table (short linear-probe runs), at
+        // least 8 partitions per SM for small joins, and at least 64 per rank.
+        const uint64_t target = std::max<uint64_t>(1, (uint64_t)ts / 3);
+        const int need = ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + target - 1) / target));
+        const int par = ceil_log2((uint64_t)8 * sms);
+        const int minb = ceil_log2((uint64_t)64 * d.rank_num);
+        jp.bits = std::min(std::max(std::max(need, par), minb), kMaxRadixBits);
     }
+    if (d.table_slots <= 0) {
+        // shrink the table to three times a generous bound on the largest partition
+        const double mean = (double)n_r / (double)(1ull << jp.bits);
+        const double bound = mean + 6.0 * sqrt(mean) + 32.0;
+        const int want = (int)std::min<double>(max_slots, std::max(1024.0, 3.0 * bound));
+        ts = std::min(ts, (want + 255) / 256 * 256);
+        ts = std::max(ts, 1024);
+    }
+    jp.table_slots = ts;
+    jp.fine_bits = jp.bits > kMaxPassBits ? jp.bits - (jp.bits + 1) / 2 : 0;
     jp.alg = d.join_alg;
     jp.skew_mode = d.skew_mode;
     jp.group = d.rank_set * d.bank_set;
@@ -163,15 +176,22 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
 
     const uint64_t F = 1ull << jp.bits;
     const int64_t ns[2] = {n_r, n_s};
+    // One chunk size for both relations so every pass-1 CTA does the same work;
+    // about one wave of 3 CTAs per SM.
     uint32_t nch[2], chunk[2];
-    for (int r = 0; r < 2; r++) {
-        int64_t n = ns[r];
-        int64_t want = std::max<int64_t>(1, std::min<int64_t>((n + 16383) / 16384, 2 * sms));
-        int64_t c = (n + want - 1) / want;
-        c = std::max<int64_t>(2, (c + 1) & ~1ll);
-        nch[r] = (uint32_t)std::max<int64_t>(1, (n + c - 1) / c);
-        chunk[r] = (uint32_t)c;
+    {
+        const int64_t total = n_r + n_s;
+        int64_t c = std::max<int64_t>(4096, (total + 2 * sms - 3) / (2 * sms - 2));
+        c = (c + 1) & ~1ll;
+        for (int r = 0; r < 2; r++) {
+            nch[r] = (uint32_t)std::max<int64_t>(1, (ns[r] + c - 1) / c);
+            chunk[r] = (uint32_t)c;
+        }
     }
+    // pass-2 work items of ~1/32 of a CTA's share of the tuples
+    const uint64_t f1 = 1ull << (jp.bits - jp.fine_bits);
+    pl->item_target = (uint32_t)std::max<int64_t>(16384, (n_r + n_s) / (64 * sms));
+    const uint64_t max_items = jp.fine_bits ? (uint64_t)(nch[0] + nch[1]) * f1 + 2 * f1 : 1;
     const uint64_t max_units = F * (uint64_t)std::max(jp.group, 1) + (uint64_t)n_s / jp.unit_tuples + F + 64;
     const uint64_t out_cap = (uint64_t)n_s + (uint64_t)pl->join_blocks * (kJoinThreads / 32) * kOutChunk;
 
@@ -184,8 +204,12 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
     };
     const size_t o_ctr = take(sizeof(Counters));
     const size_t o_hist0 = take((size_t)nch[0] * F * 4), o_hist1 = take((size_t)nch[1] * F * 4);
+    const size_t o_ch0 = take((size_t)nch[0] * f1 * 4), o_ch1 = take((size_t)nch[1] * f1 * 4);
+    const size_t o_items = take(max_items * 16);
     const size_t o_tot0 = take(F * 4), o_tot1 = take(F * 4), o_base0 = take(F * 4), o_base1 = take(F * 4);
     const size_t o_pr = take((size_t)n_r * 8 + 16), o_ps = take((size_t)n_s * 8 + 16);
+    const bool two = jp.fine_bits > 0;
+    const size_t o_tr = two ? take((size_t)n_r * 8 + 16) : 0, o_ts = two ? take((size_t)n_s * 8 + 16) : 0;
     const size_t o_units = take(max_units * sizeof(Unit));
     const size_t o_holes = take(kMaxHoles * sizeof(Hole));
     const size_t o_gaps = take(kMaxHoles * sizeof(Hole)), o_datas = take(kMaxHoles * sizeof(Hole));
@@ -207,12 +231,18 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
     }
     P.rel[0].hist = (uint32_t *)(a + o_hist0);
     P.rel[1].hist = (uint32_t *)(a + o_hist1);
+    P.rel[0].chist = (uint32_t *)(a + o_ch0);
+    P.rel[1].chist = (uint32_t *)(a + o_ch1);
+    P.items = (uint4 *)(a + o_items);
+    P.max_items = (uint32_t)std::min<uint64_t>(max_items, 0xFFFFFFFFull);
     P.rel[0].total = (uint32_t *)(a + o_tot0);
     P.rel[1].total = (uint32_t *)(a + o_tot1);
     P.rel[0].base = (uint32_t *)(a + o_base0);
     P.rel[1].base = (uint32_t *)(a + o_base1);
     P.rel[0].out = (Tuple *)(a + o_pr);
     P.rel[1].out = (Tuple *)(a + o_ps);
+    P.rel[0].tmp = two ? (Tuple *)(a + o_tr) : nullptr;
+    P.rel[1].tmp = two ? (Tuple *)(a + o_ts) : nullptr;
     P.units = (Unit *)(a + o_units);
     P.max_units = (uint32_t)std::min<uint64_t>(max_units, 0xFFFFFFFFull);
     P.holes = (Hole *)(a + o_holes);
@@ -271,6 +301,7 @@ int spj_plan_stats(spj_plan_t *pl, spj_stats_t *out) {
     out->max_s_partition = c.max_s_part;
     out->radix_bits = pl->jp.bits;
     out->table_slots = pl->jp.table_slots;
+    if (c.error & 32u) return set_error(SPJ_E_TIMEOUT, "a bulk copy did not complete in time");
     if (c.error & 1u)
         return set_error(SPJ_E_OVERFLOW, "an R partition (" + std::to_string(c.max_r_part) +
                                               " tuples) did not fit the shared-memory table of " +
