@@ -177,6 +177,26 @@ int spj_plan_kernel_times(spj_plan_t *plan, int back, spj_kernel_times_t *out);
 
 void spj_plan_destroy(spj_plan_t *plan);
 
+/* The join for callers that cannot allocate device memory while they run it: a
+ * runtime whose memory pool owns the whole GPU, code running under CUDA stream
+ * capture (where cudaMalloc is not allowed), or a latency-bound loop that must
+ * not wait on the allocator. No counterpart in the reference, whose host buffers
+ * are allocated per join. It computes what spj_plan_execute computes (the
+ * partitioned hash join, SPJ_ALG_PHJ) but takes all scratch memory from one
+ * fixed 32 MiB region inside the library, allocated once when the library loads
+ * on a GPU and held until the process exits; the call allocates nothing.
+ * Limits: |R| <= 2^20 and |S| <= 2^21 (larger sizes return SPJ_E_ARG);
+ * out_capacity >= |S| + 2^21 pairs. r, s: device columns (16-byte aligned);
+ * out: device pairs; n_out: device int64 that receives the pair count, or a
+ * negative value if the join hit an internal capacity limit.
+ * The first call on a device looks up the region's address and sets kernel
+ * attributes; make that first call before capturing any stream. All calls share
+ * the one region (the last call's contents stay in it): calls whose executions
+ * overlap on the GPU -- on different streams or threads -- race and must be
+ * serialised by the caller. */
+int spj_join_noalloc(const spj_kv_pair_t *r, int64_t n_r, const spj_kv_pair_t *s, int64_t n_s, spj_kv_pair_t *out,
+                     int64_t out_capacity, int64_t *n_out, void *stream);
+
 /* Histogram of glb_partition_hash(key) & (2^bits - 1) over a device column (key-0
  * tuples skipped): the B200 form of the global partition count kernel
  * (src/dpu/src/join/glb_partition_count.c:119-371, partition_type 0). hist is a

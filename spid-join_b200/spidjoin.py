@@ -30,7 +30,7 @@ EXPORTS = (
     "spj_design_default", "spj_last_error", "spj_version", "spj_create", "spj_load_column", "spj_prepare",
     "spj_start", "spj_finish", "spj_record_logs", "spj_destroy", "spj_plan_create", "spj_plan_output_capacity",
     "spj_plan_execute", "spj_plan_stats", "spj_plan_destroy", "spj_partition_histogram", "spj_checksum_device",
-    "spj_generate_host", "spj_generate_device", "spj_plan_kernel_times",
+    "spj_generate_host", "spj_generate_device", "spj_plan_kernel_times", "spj_join_noalloc",
 )
 
 
@@ -109,6 +109,7 @@ def lib():
         L.spj_generate_host.argtypes = [ctypes.c_uint64, i64, i64, ctypes.c_double, vp, vp,
                                         ctypes.POINTER(ctypes.c_uint64), i32]
         L.spj_generate_device.argtypes = [ctypes.c_uint64, i64, i64, ctypes.c_double, vp, vp, vp, vp]
+        L.spj_join_noalloc.argtypes = [vp, i64, vp, i64, vp, i64, vp, vp]
         _lib = L
     return _lib
 

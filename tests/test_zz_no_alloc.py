@@ -1,0 +1,66 @@
+"""spj_join_noalloc: the join for callers that cannot allocate device memory
+while they run it (a memory pool that owns the whole GPU, code under CUDA stream
+capture, a loop that must not wait on the allocator). Its output must equal that
+of the regular entry point, spj_plan_execute, bit for bit (the pair multiset,
+compared after a canonical sort), on consecutive calls that reuse its fixed
+scratch region. This file is collected last on purpose."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _device(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).cuda()
+
+
+def _plan_join(spj, dR, dS, n_r, n_s):
+    """The regular entry point (scratch allocated by spj_plan_create)."""
+    import torch
+    plan = spj.Plan(n_r, n_s, spj.make_design(rank_num=1))
+    out = torch.empty((plan.output_capacity, 2), dtype=torch.int32, device="cuda")
+    n = torch.zeros(1, dtype=torch.int64, device="cuda")
+    plan.execute(dR.data_ptr(), dS.data_ptr(), out.data_ptr(), n.data_ptr(), 0)
+    torch.cuda.synchronize()
+    plan.close()
+    k = int(n.item())
+    return out[:k].cpu().numpy().view(np.uint32)
+
+
+def _noalloc_join(spj, dR, dS, n_r, n_s):
+    import torch
+    cap = n_s + (1 << 21)
+    out = torch.empty((cap, 2), dtype=torch.int32, device="cuda")
+    n = torch.zeros(1, dtype=torch.int64, device="cuda")
+    spj.check(spj.lib().spj_join_noalloc(dR.data_ptr(), n_r, dS.data_ptr(), n_s, out.data_ptr(), cap,
+                                         n.data_ptr(), None))
+    torch.cuda.synchronize()
+    k = int(n.item())
+    assert k >= 0, f"capacity error reported: {k}"
+    return out[:k].cpu().numpy().view(np.uint32)
+
+
+def test_noalloc_matches_plan_execute_on_consecutive_calls(spj, oracle):
+    # two calls in a row: the second one finds the first one's data in the region
+    cases = [(1 << 20, 1 << 21, 1.0, 11), (40000, 300001, 0.0, 12), (1 << 20, 1 << 21, 1.5, 13)]
+    for n_r, n_s, zipf, seed in cases:
+        R, S, expect = spj.generate_host(n_r, n_s, zipf, seed=seed)
+        dR, dS = _device(R), _device(S)
+        want = _plan_join(spj, dR, dS, n_r, n_s)
+        got = _noalloc_join(spj, dR, dS, n_r, n_s)
+        assert got.shape == want.shape == (n_s, 2)
+        assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(want))
+        assert oracle.checksum(got) == expect
+
+
+def test_noalloc_rejects_sizes_over_its_limit(spj):
+    import torch
+    d = torch.zeros((16, 2), dtype=torch.int32, device="cuda")
+    n = torch.zeros(1, dtype=torch.int64, device="cuda")
+    with pytest.raises(spj.SpjError, match="2\\^20"):
+        spj.check(spj.lib().spj_join_noalloc(d.data_ptr(), (1 << 20) + 1, d.data_ptr(), 1, d.data_ptr(),
+                                             1 << 22, n.data_ptr(), None))
+    with pytest.raises(spj.SpjError, match="out_capacity"):
+        spj.check(spj.lib().spj_join_noalloc(d.data_ptr(), 8, d.data_ptr(), 8, d.data_ptr(), 16,
+                                             n.data_ptr(), None))
