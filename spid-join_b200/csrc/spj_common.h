@@ -42,6 +42,22 @@ SPJ_HD uint32_t glb_partition_hash(uint32_t key) {
     return h;
 }
 
+// join_hash2 of src/dpu/src/hash.c:85-112 (one-at-a-time over the four
+// little-endian key bytes): the slot hash of the reference's non-partitioned
+// hash join.
+SPJ_HD uint32_t join_hash2(uint32_t key) {
+    uint32_t h = 0;
+    for (int b = 0; b < 4; b++) {
+        h += (key >> (8 * b)) & 0xffu;
+        h += h << 10;
+        h ^= h >> 6;
+    }
+    h += h << 3;
+    h ^= h >> 11;
+    h += h << 15;
+    return h;
+}
+
 // splitmix64 (Steele, Lea, Flood 2014): the counter-based mixer of the generator
 // and the finaliser of the order-independent output checksum.
 SPJ_HD uint64_t mix64(uint64_t z) {

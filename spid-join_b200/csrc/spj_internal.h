@@ -92,6 +92,7 @@ struct PlanDev {
     Counters *ctr;
     Tuple *out;
     unsigned long long out_cap;
+    unsigned long long *gtable;       // global table of the non-partitioned hash join
     unsigned long long *n_out_user;   // optional user destination of the pair count
 };
 
@@ -106,6 +107,7 @@ struct spj_plan {
     int num_sms = 0;
     int join_blocks = 0;
     uint32_t item_target = 0;    // tuples per pass-2 work item
+    uint64_t gtable_slots = 0;   // non-partitioned hash join: table slots (power of two)
     void *arena = nullptr;        // one device allocation for all scratch
     size_t arena_bytes = 0;
     static constexpr int kRing = 128;   // executions whose kernel times are kept

@@ -419,8 +419,10 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_scatter2(PlanDev P, int 
 // here the replicas are work units, each a CTA that builds the same table and
 // probes a contiguous slice of the partition's S.
 __global__ void k_units(PlanDev P, int bits, JoinParams jp) {
+    // one warp per partition: lane 0 reserves, the lanes write the units
     const uint32_t F = 1u << bits;
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (p >= F) return;
     const uint32_t nr = P.rel[0].total[p], ns = P.rel[1].total[p];
     if (ns == 0) return;
@@ -436,13 +438,15 @@ __global__ void k_units(PlanDev P, int bits, JoinParams jp) {
         }
     }
     g = min(g, ns);
-    uint32_t first = atomicAdd(&P.ctr->unit_count, g);
+    uint32_t first = 0;
+    if (lane == 0) first = atomicAdd(&P.ctr->unit_count, g);
+    first = __shfl_sync(0xffffffffu, first, 0);
     if (first + g > P.max_units) {
-        atomicOr(&P.ctr->error, 4u);
+        if (lane == 0) atomicOr(&P.ctr->error, 4u);
         return;
     }
     const uint32_t s0 = P.rel[1].base[p];
-    for (uint32_t k = 0; k < g; k++) {
+    for (uint32_t k = lane; k < g; k += 32) {
         Unit u;
         u.p = p;
         u.s_begin = s0 + (uint32_t)(((uint64_t)ns * k) / g);
@@ -543,19 +547,46 @@ __device__ __forceinline__ void build_table(const PlanDev &P, const JoinParams &
 }
 
 // Probe of a2a_srj_probe_inner_mt.c:101-168: stop at the key (hit) or at an empty
-// slot (miss); the scan is bounded by the table size.
+// slot (miss). Slots are read in aligned pairs (one 16-byte shared load), which
+// halves the steps of the linear scan; when the home slot s is odd, slot s-1 of
+// the first pair lies before the probe sequence and is ignored. The scan is
+// bounded by the table size.
 __device__ __forceinline__ bool probe_table(const unsigned long long *table, uint32_t ts, uint32_t bits,
                                             uint32_t key, uint32_t &rpay) {
-    uint32_t s = slot_of(key, bits, ts);
-    for (uint32_t step = 0; step < ts; step++) {
-        const unsigned long long e = table[s];
-        const uint32_t ek = (uint32_t)e;
-        if (ek == key) {
-            rpay = (uint32_t)(e >> 32);
+    const uint32_t s = slot_of(key, bits, ts);
+    const ulonglong2 *t2 = reinterpret_cast<const ulonglong2 *>(table);
+    uint32_t p = s & ~1u;
+    {
+        const ulonglong2 e = t2[p >> 1];
+        if (p == s) {
+            if ((uint32_t)e.x == key) {
+                rpay = (uint32_t)(e.x >> 32);
+                return true;
+            }
+            if ((uint32_t)e.x == 0) return false;
+        }
+        if ((uint32_t)e.y == key) {
+            rpay = (uint32_t)(e.y >> 32);
             return true;
         }
-        if (ek == 0) return false;
-        if (++s == ts) s = 0;
+        if ((uint32_t)e.y == 0) return false;
+        p += 2;
+        if (p >= ts) p = 0;
+    }
+    for (uint32_t step = 1; step < ts / 2; step++) {
+        const ulonglong2 e = t2[p >> 1];
+        if ((uint32_t)e.x == key) {
+            rpay = (uint32_t)(e.x >> 32);
+            return true;
+        }
+        if ((uint32_t)e.x == 0) return false;
+        if ((uint32_t)e.y == key) {
+            rpay = (uint32_t)(e.y >> 32);
+            return true;
+        }
+        if ((uint32_t)e.y == 0) return false;
+        p += 2;
+        if (p >= ts) p = 0;
     }
     return false;
 }
@@ -603,6 +634,274 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P, JoinPar
             }
         }
         __syncthreads();
+    }
+    warp_close(P, w);
+}
+
+// Block-wide exclusive scan of n <= 256 counters by warp 0 (8 per lane); writes
+// off[0..n) and returns nothing (callers synchronise).
+__device__ __forceinline__ void warp0_scan256(const uint32_t *cnt, uint32_t *off, int n) {
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    uint32_t c[8], sum = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int j = lane * 8 + i;
+        c[i] = j < n ? cnt[j] : 0;
+        sum += c[i];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    uint32_t run = incl - sum;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int j = lane * 8 + i;
+        if (j < n) off[j] = run;
+        run += c[i];
+    }
+    if (lane == 31) off[n] = incl;
+}
+
+// ---------------------------------------------------------- nested-loop join --
+// nested_loop_join.c:184-231 on B200. The R partition is counting-sorted in
+// shared memory into L sub-partitions (hash bits above the partition bits) of
+// about 64 tuples on average (well under the 256 of the sweep's definition);
+// each S tuple compares its key with every R tuple of its sub-partition and takes
+// the first equal one. S is rewritten in place: unmatched S tuples are emitted
+// unchanged.
+__global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P, JoinParams jp) {
+    extern __shared__ unsigned long long smem_u64[];
+    __shared__ unsigned s_slot;
+    __shared__ uint32_t bcnt[256], boff[257];
+    Tuple *rs = reinterpret_cast<Tuple *>(smem_u64);
+    const uint32_t cap = jp.table_slots;  // R tuples that fit
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const unsigned n_units = *(volatile unsigned *)&P.ctr->unit_count;
+    const Tuple *ps = P.rel[1].out;
+    WarpOut w{0ull, 0ull};
+    uint32_t cur_p = 0xffffffffu, nr = 0, lmask = 0;
+    Unit un;
+    while (next_unit(P, n_units, &s_slot, un)) {
+        if (un.p != cur_p) {
+            cur_p = un.p;
+            nr = min(P.rel[0].total[un.p], cap);
+            if (threadIdx.x == 0 && P.rel[0].total[un.p] > cap) atomicOr(&P.ctr->error, 1u);
+            uint32_t L = 1;
+            while (L < 256 && L * 64 < nr) L <<= 1;
+            lmask = L - 1;
+            for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) bcnt[i] = 0;
+            __syncthreads();
+            const Tuple *pr = P.rel[0].out + P.rel[0].base[un.p];
+            for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x)
+                atomicAdd(&bcnt[(glb_partition_hash(pr[i].key) >> jp.bits) & lmask], 1u);
+            __syncthreads();
+            warp0_scan256(bcnt, boff, (int)L);
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) bcnt[i] = boff[i];
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
+                const Tuple t = pr[i];
+                const uint32_t b = (glb_partition_hash(t.key) >> jp.bits) & lmask;
+                rs[atomicAdd(&bcnt[b], 1u)] = t;
+            }
+            __syncthreads();
+        }
+        constexpr int U = 4;
+        for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
+            Tuple t[U];
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                const uint32_t idx = base + k * 32 + lane;
+                t[k] = idx < un.s_end ? ps[idx] : Tuple{0u, 0u};
+            }
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                bool valid = t[k].key != 0, hit = false;
+                uint32_t rp = 0;
+                if (valid && nr) {
+                    const uint32_t b = (glb_partition_hash(t[k].key) >> jp.bits) & lmask;
+                    for (uint32_t i = boff[b], e = boff[b + 1]; i < e; i++) {
+                        const Tuple r = rs[i];
+                        if (r.key == t[k].key) {
+                            rp = r.pay;
+                            hit = true;
+                            break;
+                        }
+                    }
+                }
+                warp_emit(P, w, valid, hit ? rp : t[k].key, t[k].pay);
+            }
+        }
+        __syncthreads();
+    }
+    warp_close(P, w);
+}
+
+// ----------------------------------------------------------- sort-merge join --
+// mpsm_join_sort_probe.c:152-236 on B200. The R partition is bitonic-sorted by
+// key in shared memory; S is taken in runs of 32 tuples that each warp sorts with
+// a shuffle network, and every sorted S key is merged into R by a lower-bound
+// search (merge path). A matched S tuple becomes (R.payload, S.payload), an
+// unmatched one stays as it is (S is rewritten in place).
+__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool up = (lane & k) == 0;
+            const bool low = (lane & j) == 0;
+            v = (low == up) ? (v < o ? v : o) : (v < o ? o : v);
+        }
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P, JoinParams jp) {
+    extern __shared__ unsigned long long sorted[];
+    __shared__ unsigned s_slot;
+    uint32_t cap = 1;  // largest power of two that fits the shared-memory budget
+    while (cap * 2 <= (uint32_t)jp.table_slots) cap <<= 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const unsigned n_units = *(volatile unsigned *)&P.ctr->unit_count;
+    const Tuple *ps = P.rel[1].out;
+    WarpOut w{0ull, 0ull};
+    uint32_t cur_p = 0xffffffffu, nr = 0;
+    Unit un;
+    while (next_unit(P, n_units, &s_slot, un)) {
+        if (un.p != cur_p) {
+            cur_p = un.p;
+            nr = min(P.rel[0].total[un.p], cap);
+            if (threadIdx.x == 0 && P.rel[0].total[un.p] > cap) atomicOr(&P.ctr->error, 1u);
+            uint32_t npad = 1;
+            while (npad < nr) npad <<= 1;
+            const Tuple *pr = P.rel[0].out + P.rel[0].base[un.p];
+            for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x)
+                sorted[i] = i < nr ? ((unsigned long long)pr[i].key << 32) | pr[i].pay : ~0ull;
+            __syncthreads();
+            for (uint32_t k = 2; k <= npad; k <<= 1) {
+                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                    for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x) {
+                        const uint32_t ixj = i ^ j;
+                        if (ixj > i) {
+                            const unsigned long long a = sorted[i], b = sorted[ixj];
+                            if ((a > b) == ((i & k) == 0)) {
+                                sorted[i] = b;
+                                sorted[ixj] = a;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+        for (uint32_t base = un.s_begin + warp * 32; base < un.s_end; base += nwarps * 32) {
+            const uint32_t idx = base + lane;
+            const bool in = idx < un.s_end;
+            Tuple t = in ? ps[idx] : Tuple{0u, 0u};
+            const bool valid = in && t.key != 0;
+            const unsigned nvalid = __popc(__ballot_sync(0xffffffffu, valid));
+            unsigned long long v = valid ? ((unsigned long long)t.key << 32) | t.pay : ~0ull;
+            v = warp_sort32(v);
+            const bool mine = (unsigned)lane < nvalid;
+            t.key = (uint32_t)(v >> 32);
+            t.pay = (uint32_t)v;
+            bool hit = false;
+            uint32_t rp = 0;
+            if (mine && nr) {
+                const unsigned long long target = (unsigned long long)t.key << 32;
+                uint32_t lo = 0, hi = nr;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (sorted[mid] < target)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                if (lo < nr && (uint32_t)(sorted[lo] >> 32) == t.key) {
+                    hit = true;
+                    rp = (uint32_t)sorted[lo];
+                }
+            }
+            warp_emit(P, w, mine, hit ? rp : t.key, t.pay);
+        }
+        __syncthreads();
+    }
+    warp_close(P, w);
+}
+
+// ------------------------------------------- non-partitioned hash join (NPHJ) --
+// packetwise_no_partitioned_hash_join_build.c:88-160 / _probe.c:86-140 on B200:
+// one linear-probe table over all of R in HBM (2^k >= 2|R| slots, slot from
+// join_hash2 as in the reference), built with 64-bit global CAS, then probed by
+// a stream over S. No partitioning pass; the table's random reads are served by
+// L2 when R is small.
+__global__ void k_nphj_build(PlanDev P, uint32_t tmask) {
+    const Tuple *r = P.rel[0].in;
+    const uint32_t n = P.rel[0].n;
+    unsigned long long *table = P.gtable;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Tuple t = r[i];
+        if (t.key == 0) continue;
+        const unsigned long long ent = ((unsigned long long)t.pay << 32) | t.key;
+        uint32_t s = join_hash2(t.key) & tmask;
+        for (uint32_t step = 0; step <= tmask; step++) {
+            const unsigned long long prev = atomicCAS(&table[s], 0ull, ent);
+            if (prev == 0ull || (uint32_t)prev == t.key) break;
+            s = (s + 1) & tmask;
+            if (step == tmask) atomicOr(&P.ctr->error, 1u);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P, uint32_t tmask) {
+    const Tuple *s = P.rel[1].in;
+    const uint32_t n = P.rel[1].n;
+    const unsigned long long *table = P.gtable;
+    const int lane = threadIdx.x & 31;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    WarpOut w{0ull, 0ull};
+    constexpr int U = 4;
+    for (uint32_t base = gw * 32 * U; base < n; base += nw * 32 * U) {
+        Tuple t[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const uint32_t idx = base + k * 32 + lane;
+            t[k] = idx < n ? s[idx] : Tuple{0u, 0u};
+        }
+        uint32_t sl[U];
+        unsigned long long e[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            sl[k] = join_hash2(t[k].key) & tmask;
+            e[k] = t[k].key ? __ldg(&table[sl[k]]) : 0ull;
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            bool hit = false;
+            uint32_t rp = 0;
+            if (t[k].key) {
+                uint32_t sx = sl[k];
+                unsigned long long ex = e[k];
+                for (uint32_t step = 0; step <= tmask; step++) {
+                    if ((uint32_t)ex == t[k].key) {
+                        hit = true;
+                        rp = (uint32_t)(ex >> 32);
+                        break;
+                    }
+                    if ((uint32_t)ex == 0) break;
+                    sx = (sx + 1) & tmask;
+                    ex = __ldg(&table[sx]);
+                }
+            }
+            warp_emit(P, w, hit, rp, t[k].pay);
+        }
     }
     warp_close(P, w);
 }
@@ -836,21 +1135,38 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
         if (ev) cudaEventRecord(ev[i], st);
     };
     mark(0);
-    k_hist<<<nchunks, kHistThreads, hsmem, st>>>(P, bits, b2);
-    mark(1);
-    k_colscan<<<dim3((F + 255) / 256, 2), 256, 0, st>>>(P, bits);
-    k_basescan<<<2, 1024, 0, st>>>(P, bits);
-    mark(2);
-    k_scatter1<<<nchunks, kScatterThreads, sizeof(TileSmem), st>>>(P, bits, b2);
-    if (b2) {
-        const uint32_t f1 = 1u << (bits - b2);
-        k_items<<<(2 * f1 + 255) / 256, 256, 0, st>>>(P, bits, b2, pl->item_target);
-        k_scatter2<<<pl->num_sms * 2, kScatterThreads, sizeof(TileSmem), st>>>(P, bits, b2);
+    if (jp.alg == SPJ_ALG_NPHJ) {
+        const uint32_t tmask = (uint32_t)(pl->gtable_slots - 1);
+        cudaMemsetAsync(P.gtable, 0, pl->gtable_slots * 8, st);
+        mark(1);
+        mark(2);
+        k_nphj_build<<<pl->num_sms * 8, 256, 0, st>>>(P, tmask);
+        mark(3);
+        mark(4);
+        k_nphj_probe<<<pl->join_blocks, kJoinThreads, 0, st>>>(P, tmask);
+    } else {
+        k_hist<<<nchunks, kHistThreads, hsmem, st>>>(P, bits, b2);
+        mark(1);
+        k_colscan<<<dim3((F + 255) / 256, 2), 256, 0, st>>>(P, bits);
+        k_basescan<<<2, 1024, 0, st>>>(P, bits);
+        mark(2);
+        k_scatter1<<<nchunks, kScatterThreads, sizeof(TileSmem), st>>>(P, bits, b2);
+        if (b2) {
+            const uint32_t f1 = 1u << (bits - b2);
+            k_items<<<(2 * f1 + 255) / 256, 256, 0, st>>>(P, bits, b2, pl->item_target);
+            k_scatter2<<<pl->num_sms * 2, kScatterThreads, sizeof(TileSmem), st>>>(P, bits, b2);
+        }
+        mark(3);
+        k_units<<<(F * 32 + 255) / 256, 256, 0, st>>>(P, bits, jp);
+        mark(4);
+        const size_t jsm = (size_t)jp.table_slots * 8;
+        if (jp.alg == SPJ_ALG_SMJ)
+            k_join_smj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P, jp);
+        else if (jp.alg == SPJ_ALG_NL)
+            k_join_nl<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P, jp);
+        else
+            k_join_phj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P, jp);
     }
-    mark(3);
-    k_units<<<(F + 255) / 256, 256, 0, st>>>(P, bits, jp);
-    mark(4);
-    k_join_phj<<<pl->join_blocks, kJoinThreads, (size_t)jp.table_slots * 8, st>>>(P, jp);
     mark(5);
     k_fixup_prep<<<1, 1024, (size_t)(kHoleSortSlots + kMaxHoles) * 8, st>>>(P);
     k_fixup_copy<<<pl->num_sms * 2, 256, 0, st>>>(P);
@@ -865,7 +1181,7 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
 // Kernel launches of one execution (for launch accounting).
 int pipeline_launches(const spj_plan *pl) { return pl->jp.fine_bits ? 10 : 8; }
 
-cudaError_t configure_kernels(int table_slots, int *join_blocks_per_sm) {
+cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm) {
     cudaError_t e;
     int dev = 0, max_smem = 0;
     cudaGetDevice(&dev);
@@ -873,13 +1189,15 @@ cudaError_t configure_kernels(int table_slots, int *join_blocks_per_sm) {
     e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (1 << kMaxRadixBits) * 4);
     if (e) return e;
     // the largest table any plan may use, so plans of different sizes coexist
-    e = cudaFuncSetAttribute(k_join_phj, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - 1024);
-    if (e) return e;
+    for (const void *k : {(const void *)k_join_phj, (const void *)k_join_smj, (const void *)k_join_nl})
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - 1024 - 2048)))
+            return e;
     e = cudaFuncSetAttribute(k_scatter1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));
     if (e) return e;
     e = cudaFuncSetAttribute(k_scatter2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));
     if (e) return e;
     for (const void *k : {(const void *)k_scatter1, (const void *)k_scatter2, (const void *)k_join_phj,
+                          (const void *)k_join_smj, (const void *)k_join_nl, (const void *)k_nphj_probe,
                           (const void *)k_hist})
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       cudaSharedmemCarveoutMaxShared)))
@@ -887,8 +1205,12 @@ cudaError_t configure_kernels(int table_slots, int *join_blocks_per_sm) {
     e = cudaFuncSetAttribute(k_fixup_prep, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (kHoleSortSlots + kMaxHoles) * 8);
     if (e) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(join_blocks_per_sm, k_join_phj, kJoinThreads,
-                                                         (size_t)table_slots * 8);
+    const void *jk = alg == SPJ_ALG_SMJ ? (const void *)k_join_smj
+                     : alg == SPJ_ALG_NL  ? (const void *)k_join_nl
+                     : alg == SPJ_ALG_NPHJ ? (const void *)k_nphj_probe
+                                           : (const void *)k_join_phj;
+    const size_t dyn = alg == SPJ_ALG_NPHJ ? 0 : (size_t)table_slots * 8;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(join_blocks_per_sm, jk, kJoinThreads, dyn);
 }
 
 cudaError_t launch_checksum(const spj_kv_pair_t *pairs, const int64_t *n_dev, uint64_t *sum_dev, int sms,

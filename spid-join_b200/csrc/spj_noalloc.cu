@@ -21,7 +21,7 @@
 namespace spj {
 
 cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st);
-cudaError_t configure_kernels(int table_slots, int *join_blocks_per_sm);
+cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm);
 
 namespace {
 
@@ -65,7 +65,7 @@ int setup_device(int dev, DeviceSetup **out) {
         e = cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         if (e != cudaSuccess) return cuda_error(e, "cudaDeviceGetAttribute");
         int per_sm = 0;
-        e = configure_kernels(kDefaultTableSlots, &per_sm);
+        e = configure_kernels(kDefaultTableSlots, SPJ_ALG_PHJ, &per_sm);
         if (e != cudaSuccess) return cuda_error(e, "configure kernels");
         s.scratch = ptr;
         s.sms = prop.multiProcessorCount;

@@ -16,7 +16,7 @@
 namespace spj {
 
 cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st);
-cudaError_t configure_kernels(int table_slots, int *join_blocks_per_sm);
+cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm);
 cudaError_t launch_checksum(const spj_kv_pair_t *pairs, const int64_t *n_dev, uint64_t *sum_dev, int sms,
                             cudaStream_t st);
 cudaError_t launch_generate(uint64_t seed, int64_t n_r, int64_t n_s, double zipf_s, spj_kv_pair_t *r,
@@ -106,8 +106,8 @@ static int validate_design(const spj_design_t *d) {
         return set_error(SPJ_E_ARG, "rank_set must divide rank_num");
     if (!is_pow2(d->bank_set) || d->bank_set > 64) return set_error(SPJ_E_ARG, "bank_set must be a power of two <= 64");
     if (d->tpch_example) return set_error(SPJ_E_UNSUPPORTED, "tpch_example is not part of the join path");
-    if (d->join_alg != SPJ_ALG_PHJ)
-        return set_error(SPJ_E_UNSUPPORTED, "join_alg " + std::to_string(d->join_alg) + " is not built yet");
+    if (d->join_alg < SPJ_ALG_PHJ || d->join_alg > SPJ_ALG_NL)
+        return set_error(SPJ_E_ARG, "join_alg must be 0 (phj), 1 (nphj), 2 (smj) or 3 (nl)");
     if (d->skew_mode != SPJ_SKEW_ADAPTIVE && d->skew_mode != SPJ_SKEW_FIXED)
         return set_error(SPJ_E_ARG, "skew_mode must be 0 (adaptive) or 1 (fixed)");
     if (d->radix_bits < 0 || d->radix_bits > kMaxRadixBits)
@@ -136,7 +136,7 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
     const spj_design_t &d = *design;
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const int max_slots = (max_smem - 1024) / 8;
+    const int max_slots = (max_smem - 4096) / 8 & ~1;
     int ts = d.table_slots > 0 ? std::min(d.table_slots, max_slots) : kDefaultTableSlots;
     if (d.radix_bits > 0) {
         jp.bits = d.radix_bits;
@@ -157,7 +157,7 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
         ts = std::min(ts, (want + 255) / 256 * 256);
         ts = std::max(ts, 1024);
     }
-    jp.table_slots = ts;
+    jp.table_slots = ts & ~1;  // pairs of slots are probed together
     jp.fine_bits = jp.bits > kMaxPassBits ? jp.bits - (jp.bits + 1) / 2 : 0;
     jp.alg = d.join_alg;
     jp.skew_mode = d.skew_mode;
@@ -166,7 +166,7 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
     jp.keep_unmatched = (d.join_alg == SPJ_ALG_SMJ || d.join_alg == SPJ_ALG_NL) ? 1 : 0;
 
     int per_sm = 0;
-    cudaError_t ce = configure_kernels(jp.table_slots, &per_sm);
+    cudaError_t ce = configure_kernels(jp.table_slots, jp.alg, &per_sm);
     if (ce != cudaSuccess || per_sm < 1) {
         delete pl;
         return ce != cudaSuccess ? cuda_error(ce, "configure kernels")
@@ -207,8 +207,15 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
     const size_t o_ch0 = take((size_t)nch[0] * f1 * 4), o_ch1 = take((size_t)nch[1] * f1 * 4);
     const size_t o_items = take(max_items * 16);
     const size_t o_tot0 = take(F * 4), o_tot1 = take(F * 4), o_base0 = take(F * 4), o_base1 = take(F * 4);
-    const size_t o_pr = take((size_t)n_r * 8 + 16), o_ps = take((size_t)n_s * 8 + 16);
-    const bool two = jp.fine_bits > 0;
+    const bool nphj = jp.alg == SPJ_ALG_NPHJ;
+    const size_t o_pr = take(nphj ? 0 : (size_t)n_r * 8 + 16), o_ps = take(nphj ? 0 : (size_t)n_s * 8 + 16);
+    if (nphj) {
+        uint64_t slots = 1024;
+        while (slots < 2 * (uint64_t)n_r) slots <<= 1;
+        pl->gtable_slots = slots;
+    }
+    const size_t o_gt = take(nphj ? pl->gtable_slots * 8 : 0);
+    const bool two = !nphj && jp.fine_bits > 0;
     const size_t o_tr = two ? take((size_t)n_r * 8 + 16) : 0, o_ts = two ? take((size_t)n_s * 8 + 16) : 0;
     const size_t o_units = take(max_units * sizeof(Unit));
     const size_t o_holes = take(kMaxHoles * sizeof(Hole));
@@ -252,6 +259,7 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
     P.data_off = (unsigned long long *)(a + o_doff);
     P.out = nullptr;
     P.out_cap = out_cap;
+    P.gtable = nphj ? (unsigned long long *)(a + o_gt) : nullptr;
     P.n_out_user = nullptr;
     pl->have_events = true;
     for (int i = 0; i < spj_plan::kRing && pl->have_events; i++)

@@ -155,3 +155,67 @@ def test_device_generator_matches_host(spj):
             assert diff == 0 and int(exp.item()) & (2**64 - 1) == exp_h
         else:
             assert diff <= 2  # libm and CUDA double exp/log may differ in the last ulp
+
+
+ALGS = ["phj", "nphj", "smj", "nl"]
+
+
+@pytest.mark.parametrize("alg", ALGS)
+@pytest.mark.parametrize("zipf", [0.0, 1.0, 1.5])
+def test_algorithms_on_fk_joins(spj, oracle, alg, zipf):
+    R, S, expect = spj.generate_host(1 << 16, 1 << 18, zipf, seed=77 + int(zipf * 10))
+    res, _ = run_instance(spj, R, S, join_alg=alg)
+    out = res.pairs()
+    assert out.shape[0] == S.shape[0] and oracle.checksum(out) == expect
+    assert same_multiset(oracle, out, oracle.simple_join(R, S))
+
+
+@pytest.mark.parametrize("alg", ALGS)
+def test_algorithms_non_fk_semantics(spj, oracle, alg):
+    """PHJ/NPHJ drop unmatched S tuples; SMJ/NL rewrite S in place and keep them."""
+    rng = np.random.default_rng(8)
+    R = np.stack([rng.permutation(np.arange(1, 30001)), rng.integers(0, 2**32, 30000)], 1).astype(np.uint32)
+    R[::101, 0] = 0
+    S = np.stack([rng.integers(0, 60000, 200003), np.arange(200003)], 1).astype(np.uint32)
+    out = run_instance(spj, R, S, join_alg=alg)[0].pairs()
+    keep = alg in ("smj", "nl")
+    assert same_multiset(oracle, out, oracle.simple_join(R, S, keep_unmatched=keep))
+
+
+@pytest.mark.parametrize("alg", ALGS)
+def test_algorithms_duplicate_r_keys(spj, alg):
+    rng = np.random.default_rng(9)
+    keys = np.concatenate([np.arange(1, 3000), rng.integers(1, 3000, 30000 - 2999)])  # every key present
+    rng.shuffle(keys)
+    R = np.stack([keys, np.arange(30000)], 1).astype(np.uint32)
+    S = np.stack([rng.integers(1, 3000, 90000), np.arange(90000)], 1).astype(np.uint32)
+    out = run_instance(spj, R, S, join_alg=alg)[0].pairs()
+    assert out.shape[0] == S.shape[0]  # every S key occurs in R here
+    assert np.array_equal(np.sort(out[:, 1]), np.arange(90000, dtype=np.uint32))
+    assert np.array_equal(R[out[:, 0], 0], S[out[:, 1], 0])
+
+
+def test_config3_sweep_all_bit_exact(spj, oracle):
+    """Config-3 shape at 1/512 scale (|R| = 2^17, |S| = 2^20, Zipf 1.5): hash, sort-merge,
+    nested-loop and non-partitioned joins, and replication groups of 1, 4 and 16 CTAs,
+    all give the same multiset."""
+    R, S, expect = spj.generate_host(1 << 17, 1 << 20, 1.5, seed=3)
+    ref = oracle.sort_pairs(oracle.simple_join(R, S))
+    variants = [dict(join_alg=a) for a in ALGS]
+    variants += [dict(join_alg="phj", skew_mode=1, ranks=g, rank_sets=g) for g in (1, 4, 16)]
+    for v in variants:
+        v = dict(v)
+        ranks, rsets = v.pop("ranks", 1), v.pop("rank_sets", 1)
+        out = run_instance(spj, R, S, ranks=ranks, rank_sets=rsets, **v)[0].pairs()
+        assert oracle.checksum(out) == expect, v
+        assert np.array_equal(oracle.sort_pairs(out), ref), v
+
+
+@pytest.mark.parametrize("alg", ALGS)
+@pytest.mark.parametrize("nr,ns", [(0, 10), (10, 0), (1, 1), (3, 5), (7, 100000)])
+def test_algorithms_edge_sizes(spj, oracle, alg, nr, ns):
+    rng = np.random.default_rng(nr * 13 + ns)
+    R = np.stack([rng.permutation(np.arange(1, nr + 1)), np.arange(nr)], 1).astype(np.uint32).reshape(nr, 2)
+    S = np.stack([rng.integers(1, nr + 3, ns), np.arange(ns)], 1).astype(np.uint32).reshape(ns, 2)
+    out = run_instance(spj, R, S, join_alg=alg)[0].pairs()
+    assert same_multiset(oracle, out, oracle.simple_join(R, S, keep_unmatched=alg in ("smj", "nl")))
