@@ -177,6 +177,25 @@ int spj_plan_kernel_times(spj_plan_t *plan, int back, spj_kernel_times_t *out);
 
 void spj_plan_destroy(spj_plan_t *plan);
 
+/* ------------------------------------------------------------------ batches --
+ * Many joins of uneven sizes and skew in one launch sequence: the kernels of a
+ * batch plan cover every join, and one persistent work queue of
+ * (join, partition, S range) units feeds the local-join CTAs. The plan's
+ * tuning (fan-out, pass count, table size, output chunk) is chosen per join from
+ * its sizes. No counterpart in the reference, which runs one JoinInstance per
+ * join. Usage: create, bind the device pointers once, then execute any number
+ * of times (execute allocates nothing, does not synchronise and can be captured
+ * in a CUDA graph). Join j's pair count is written to n_out[j] (device array). */
+int spj_batch_create(int n_joins, const int64_t *n_r, const int64_t *n_s, const spj_design_t *design,
+                     spj_plan_t **out);
+int64_t spj_batch_output_capacity(const spj_plan_t *plan, int join);
+/* r, s, out: host arrays of n_joins device pointers; n_out: device int64[n_joins] (may be NULL). */
+int spj_batch_bind(spj_plan_t *plan, const spj_kv_pair_t *const *r, const spj_kv_pair_t *const *s,
+                   spj_kv_pair_t *const *out, int64_t *n_out);
+int spj_batch_execute(spj_plan_t *plan, void *stream);
+/* Counters of join `join` after an execution (synchronises). */
+int spj_batch_stats(spj_plan_t *plan, int join, spj_stats_t *out);
+
 /* The join for callers that cannot allocate device memory while they run it: a
  * runtime whose memory pool owns the whole GPU, code running under CUDA stream
  * capture (where cudaMalloc is not allowed), or a latency-bound loop that must

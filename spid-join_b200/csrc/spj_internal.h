@@ -1,9 +1,16 @@
 // spj_internal.h -- plan layout shared by the kernels and the host orchestration.
+//
+// A plan describes a batch of J joins (J = 1 for the plain join). Every kernel
+// covers all joins of the batch in one launch: chunks, partitions and coarse
+// buckets of all relations live in flat index spaces, mapped back to
+// (relation, local index) through prefix arrays, and the join kernels pull
+// (join, partition, S range) work units from one queue.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/spidjoin.h"
 #include "spj_common.h"
@@ -13,17 +20,16 @@ namespace spj {
 constexpr int kHistThreads = 1024;
 constexpr int kScatterThreads = 512;
 constexpr int kJoinThreads = 1024;
-constexpr int kOutChunk = 1024;      // output pairs reserved per warp at a time
-constexpr int kMaxHoles = 12288;     // warps of the emitting kernels (one hole each)
+constexpr int kOutChunk = 1024;       // output pairs reserved per warp at a time
+constexpr int kMaxHoles = 12288;      // per join: warps of the emitting kernels (one hole each)
 constexpr int kHoleSortSlots = 16384; // power of two >= kMaxHoles
 constexpr int kMaxRadixBits = 15;
-constexpr int kMaxPassBits = 8;      // buckets per scatter pass <= 256
-constexpr int kTile = 4096;          // tuples sorted per tile in shared memory
+constexpr int kMaxPassBits = 8;       // buckets per scatter pass <= 256
+constexpr int kTile = 4096;           // tuples sorted per tile in shared memory
 constexpr int kDefaultTableSlots = 12288;  // 96 KB of shared memory
 constexpr int kDefaultUnitTuples = 65536;
-constexpr int kHeavyCap = 1024;      // heavy keys joined on the fly
 
-// One relation's partitioning state.
+// One relation (R or S) of one join.
 struct RelDev {
     const Tuple *in;     // input column (device)
     Tuple *out;          // partitioned column
@@ -31,85 +37,123 @@ struct RelDev {
     uint32_t n;          // tuples
     uint32_t chunk;      // tuples per chunk (even)
     uint32_t nchunks;
+    uint32_t join;       // owning join
     uint32_t *hist;      // [nchunks][F] counts, then exclusive offsets within each partition
     uint32_t *chist;     // [nchunks][F1] counts of the coarse buckets (two-pass scatter)
     uint32_t *total;     // [F] tuples per partition
     uint32_t *base;      // [F] partition starts
 };
 
-// A work unit: partition p, S range [s_begin, s_end) of the partitioned S column.
-struct Unit {
-    uint32_t p;
-    uint32_t s_begin;
-    uint32_t s_end;
-    uint32_t pad;
-};
-
 struct Hole {
     unsigned long long begin, end;
 };
 
-// Device-side counters of one execution (zeroed at the start of each execution).
-struct Counters {
+// Per-join counters of one execution (zeroed at its start).
+struct JoinCtr {
     unsigned long long out_reserved;  // output slots handed out (pairs + holes)
-    unsigned int unit_count;
-    unsigned int unit_next;
-    unsigned int hole_count;
-    unsigned int error;               // bit 0: table overflow, bit 1: output overflow
-    unsigned int max_r_part;
-    unsigned int max_s_part;
-    unsigned int heavy_keys;
-    unsigned int pad;
-    unsigned long long heavy_tuples;
     unsigned long long n_out;         // final pair count
     unsigned long long gap_total;     // fix-up: hole space below n_out
+    unsigned int hole_count;
+    unsigned int error;               // 1 table, 2 output, 4 work list, 8 holes, 16 fix-up, 32 timeout
+    unsigned int max_r_part, max_s_part;
     unsigned int n_gaps, n_data;
-    unsigned int item_count, item_next;  // pass-2 work list
+    unsigned int units;               // work units of the join
+    unsigned int unit_base;           // its first unit in the queue
+    unsigned int unit_fill;
+    unsigned int pad[3];
 };
 
-struct JoinParams {
+// Per-join constants and output state.
+struct JoinDev {
     int bits;             // radix bits of the partition fan-out
     int fine_bits;        // bits resolved by the second scatter pass (0 = one pass)
     int table_slots;      // shared-memory table entries (8 bytes each)
     int alg;              // spj_join_alg
     int skew_mode;
     int group;            // rank_set * bank_set
-    uint32_t unit_tuples;
     int keep_unmatched;   // SMJ/NL rewrite S in place and keep unmatched tuples
-};
-
-struct PlanDev {
-    RelDev rel[2];        // 0 = R, 1 = S
-    Unit *units;
-    uint32_t max_units;
-    uint4 *items;         // pass-2 work items: (relation, coarse bucket, first chunk, end chunk)
-    uint32_t max_items;
-    Hole *holes;
-    Hole *gaps;           // fix-up scratch
-    Hole *datas;
-    unsigned long long *gap_off;
-    unsigned long long *data_off;
-    Counters *ctr;
+    uint32_t unit_tuples;
+    uint32_t item_target; // tuples per pass-2 work item
+    uint32_t out_chunk;   // output pairs a warp reserves at a time (<= kOutChunk)
     Tuple *out;
     unsigned long long out_cap;
-    unsigned long long *gtable;       // global table of the non-partitioned hash join
-    unsigned long long *n_out_user;   // optional user destination of the pair count
+    unsigned long long *n_out_user;   // optional device destination of the pair count
+    JoinCtr *ctr;
+    Hole *holes, *gaps, *datas;
+    unsigned long long *gap_off, *data_off;
+    unsigned long long *gtable;       // non-partitioned hash join: global table
+    unsigned long long gtable_slots;
+};
+
+// A work unit: join j, partition p, S range [s_begin, s_end) of the partitioned S column.
+struct Unit {
+    uint32_t p;
+    uint32_t s_begin;
+    uint32_t s_end;
+    uint32_t join;
+};
+
+// Batch-wide queues (zeroed per execution).
+struct BatchCtr {
+    unsigned int unit_count, unit_next;
+    unsigned int item_count, item_next;
+    unsigned int error;
+    unsigned int pad[3];
+};
+
+// Kernel-parameter view of a plan.
+struct PlanDev {
+    RelDev *rel;              // [2J]: rel[2j] = R of join j, rel[2j+1] = S of join j
+    JoinDev *join;            // [J]
+    uint32_t *chunk_prefix;   // [2J+1] first flat chunk of each relation
+    uint32_t *part_prefix;    // [2J+1] first flat partition of each relation (F_j each)
+    uint32_t *coarse_prefix;  // [2J+1] first flat coarse bucket (F1_j, or 0 for one pass)
+    uint32_t *jpart_prefix;   // [J+1] first flat partition of each join (R side)
+    uint32_t nrel, njoin;
+    uint32_t total_chunks, total_parts, total_coarse, total_jparts;
+    int max_bits;             // histogram shared memory
+    int max_table_slots;      // join-kernel shared memory
+    int alg;                  // one local-join algorithm per batch
+    int any_two_pass;
+    Unit *units;
+    uint32_t max_units;
+    uint4 *items;             // pass-2 work items: (relation, coarse bucket, first chunk, end chunk)
+    uint32_t max_items;
+    BatchCtr *bctr;
+    JoinCtr *jctr;            // [J], contiguous after bctr (one memset clears both)
+};
+
+// Host-side description of one join of a plan.
+struct JoinHost {
+    int64_t n_r = 0, n_s = 0;
+    JoinDev dev{};
+    RelDev rel[2]{};
+};
+
+// Per-join tuning chosen from the sizes and the design.
+struct JoinShape {
+    int bits = 0, fine_bits = 0, table_slots = 0;
+    uint32_t nchunks[2] = {1, 1}, chunk[2] = {2, 2};
+    uint32_t item_target = 0;
+    uint32_t out_chunk = kOutChunk;
+    unsigned long long gtable_slots = 0;
 };
 
 }  // namespace spj
 
 struct spj_plan {
-    int64_t n_r = 0, n_s = 0;
+    int64_t n_r = 0, n_s = 0;      // join 0 (plain plans)
     spj_design_t design{};
-    spj::JoinParams jp{};
+    std::vector<spj::JoinHost> joins;
+    std::vector<spj::JoinShape> shapes;
     spj::PlanDev dev{};
     int device = 0;
     int num_sms = 0;
     int join_blocks = 0;
-    uint32_t item_target = 0;    // tuples per pass-2 work item
-    uint64_t gtable_slots = 0;   // non-partitioned hash join: table slots (power of two)
-    void *arena = nullptr;        // one device allocation for all scratch
+    void *arena = nullptr;         // one device allocation for all scratch
     size_t arena_bytes = 0;
+    size_t desc_offset = 0;        // descriptor arrays inside the arena
+    std::vector<unsigned char> desc_host;  // their host image
     static constexpr int kRing = 128;   // executions whose kernel times are kept
     static constexpr int kMarks = 7;    // events per execution
     cudaEvent_t ring[kRing][kMarks]{};
@@ -122,4 +166,13 @@ struct spj_plan {
 namespace spj {
 int set_error(int code, const std::string &msg);
 int cuda_error(cudaError_t e, const char *what);
+
+JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots);
+// Computes the arena layout of pl->joins/pl->shapes (arena == nullptr: size only)
+// and fills pl->dev, the per-join descriptors and the host image of the
+// descriptor arrays.
+size_t layout_plan(spj_plan *pl, char *arena, bool image);
+cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st);
+cudaError_t init_single(spj_plan *pl, cudaStream_t st);
+cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm);
 }  // namespace spj

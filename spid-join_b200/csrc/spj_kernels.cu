@@ -1,17 +1,20 @@
 // spj_kernels.cu -- sm_100a kernels of the B200 SPID-Join equi-join.
 //
-// One join is a fixed sequence of launches with no host synchronisation:
+// A plan runs a batch of J joins (J = 1 for the plain join) as one fixed
+// sequence of launches, each covering every join, with no host synchronisation:
 //
-//   k_hist      per-chunk partition histograms of R and S (one read pass)
-//   k_colscan   per-partition exclusive offsets across chunks
-//   k_basescan  partition starts (exclusive scan of the totals)
-//   k_scatter   radix scatter of R and S into partition-contiguous columns
-//   k_units     work units: (partition, S range); heavy partitions split
-//   k_join_*    persistent CTAs: build the R partition's shared-memory table,
-//               probe the unit's S range, emit pairs with warp-aggregated
-//               reservations of 1024-pair output chunks
-//   k_fixup_*   move the pairs of the partially used last chunks into the holes
-//               those chunks left, so the output is dense
+//   k_hist       per-chunk partition histograms of every R and S (one read pass)
+//   k_colscan    per-partition exclusive offsets across chunks
+//   k_basescan   partition starts (exclusive scan of the totals)
+//   k_scatter1   radix scatter pass 1 (coarse buckets; the only pass for <= 256 partitions)
+//   k_items      skew-bounded work list of pass 2
+//   k_scatter2   radix scatter pass 2 (fine partitions), persistent CTAs
+//   k_units      work units: (join, partition, S range); heavy partitions split
+//   k_join_*     persistent CTAs over the unit queue: build the R partition's
+//                shared-memory structure, probe the unit's S range, emit pairs with
+//                warp-aggregated reservations of 1024-pair output chunks
+//   k_fixup_*    per join: move the pairs of partly used last chunks into the
+//                holes those chunks left, so the output is dense
 //
 // This is the B200 form of the reference's pipeline (yonsei-hpcp/spid-join):
 // glb_partition_count.c (count), glb_partition_packet.c + the host-mediated
@@ -33,36 +36,58 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
-// Chunk c of relation rel for a flat block index over R's chunks then S's.
-__device__ __forceinline__ void chunk_of(const PlanDev &P, unsigned bid, int &rel, unsigned &c) {
-    if (bid < P.rel[0].nchunks) {
-        rel = 0;
-        c = bid;
-    } else {
-        rel = 1;
-        c = bid - P.rel[0].nchunks;
+// Largest r < n with prefix[r] <= x (prefix has n + 1 non-decreasing entries).
+__device__ __forceinline__ uint32_t find_slot(const uint32_t *prefix, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (prefix[mid] <= x)
+            lo = mid;
+        else
+            hi = mid;
     }
+    return lo;
+}
+
+// Writes the descriptors of a one-join plan from kernel parameters (no host copy).
+__global__ void k_init_single(PlanDev P, RelDev r0, RelDev r1, JoinDev j0, uint32_t nch0, uint32_t nch1, uint32_t f,
+                              uint32_t f1) {
+    if (threadIdx.x != 0) return;
+    P.rel[0] = r0;
+    P.rel[1] = r1;
+    P.join[0] = j0;
+    P.chunk_prefix[0] = 0;
+    P.chunk_prefix[1] = nch0;
+    P.chunk_prefix[2] = nch0 + nch1;
+    P.part_prefix[0] = 0;
+    P.part_prefix[1] = f;
+    P.part_prefix[2] = 2 * f;
+    P.coarse_prefix[0] = 0;
+    P.coarse_prefix[1] = f1;
+    P.coarse_prefix[2] = 2 * f1;
+    P.jpart_prefix[0] = 0;
+    P.jpart_prefix[1] = f;
 }
 
 // ------------------------------------------------------------- histogram --
 // glb_partition_count.c:119-236 on B200: each CTA counts one contiguous chunk
 // into a shared-memory histogram; key-0 tuples are skipped (:190-192).
-__global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P, int bits, int b2) {
+__global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P) {
     extern __shared__ uint32_t sh[];
+    const uint32_t r = find_slot(P.chunk_prefix, P.nrel, blockIdx.x);
+    const uint32_t c = blockIdx.x - P.chunk_prefix[r];
+    const RelDev R = P.rel[r];
+    const int bits = P.join[R.join].bits, b2 = P.join[R.join].fine_bits;
     const uint32_t F = 1u << bits, mask = F - 1;
-    int rel;
-    unsigned c;
-    chunk_of(P, blockIdx.x, rel, c);
-    const RelDev R = rel == 0 ? P.rel[0] : P.rel[1];
     for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) sh[i] = 0;
     __syncthreads();
     const uint32_t b = c * R.chunk;
     const uint32_t e = min(R.n, b + R.chunk);
     if (b < e) {
         const uint4 *in2 = reinterpret_cast<const uint4 *>(R.in);
-        const uint32_t b2 = b >> 1, e2 = e >> 1;
+        const uint32_t b2i = b >> 1, e2 = e >> 1;
         constexpr int U = 4;
-        for (uint32_t i = b2 + threadIdx.x; i < e2; i += U * blockDim.x) {
+        for (uint32_t i = b2i + threadIdx.x; i < e2; i += U * blockDim.x) {
             uint4 v[U];
 #pragma unroll
             for (int k = 0; k < U; k++) {
@@ -98,31 +123,33 @@ __global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P, int bits, int 
 
 // Per partition: exclusive offsets of each chunk inside the partition (in place)
 // and the partition total.
-__global__ void k_colscan(PlanDev P, int bits) {
-    const uint32_t F = 1u << bits;
-    const RelDev R = blockIdx.y == 0 ? P.rel[0] : P.rel[1];
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= F) return;
+__global__ void k_colscan(PlanDev P) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.total_parts) return;
+    const uint32_t r = find_slot(P.part_prefix, P.nrel, t);
+    const RelDev R = P.rel[r];
+    const uint32_t F = 1u << P.join[R.join].bits;
+    const uint32_t p = t - P.part_prefix[r];
     uint32_t run = 0;
     for (uint32_t c = 0; c < R.nchunks; c++) {
         uint32_t *cell = R.hist + (size_t)c * F + p;
-        uint32_t v = *cell;
+        const uint32_t v = *cell;
         *cell = run;
         run += v;
     }
     R.total[p] = run;
 }
 
-// Block-wide exclusive scan of up to 1024 * 16 values (one CTA per relation).
-__global__ void __launch_bounds__(1024) k_basescan(PlanDev P, int bits) {
+// Block-wide exclusive scan of up to 1024 * 32 totals (one CTA per relation).
+__global__ void __launch_bounds__(1024) k_basescan(PlanDev P) {
     __shared__ uint32_t warp_sums[32];
-    const uint32_t F = 1u << bits;
-    const RelDev R = blockIdx.x == 0 ? P.rel[0] : P.rel[1];
+    const RelDev R = P.rel[blockIdx.x];
+    const uint32_t F = 1u << P.join[R.join].bits;
     const uint32_t per = (F + blockDim.x - 1) / blockDim.x;
     const uint32_t beg = threadIdx.x * per, end = min(F, beg + per);
     uint32_t sum = 0, mx = 0;
     for (uint32_t i = beg; i < end; i++) {
-        uint32_t v = R.total[i];
+        const uint32_t v = R.total[i];
         sum += v;
         mx = max(mx, v);
     }
@@ -130,7 +157,7 @@ __global__ void __launch_bounds__(1024) k_basescan(PlanDev P, int bits) {
     uint32_t incl = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
     if (lane == 31) warp_sums[warp] = incl;
@@ -138,11 +165,11 @@ __global__ void __launch_bounds__(1024) k_basescan(PlanDev P, int bits) {
     for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+        const uint32_t w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
         uint32_t wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
             if (lane >= o) wi += t;
         }
         warp_sums[lane] = wi - w;
@@ -150,11 +177,12 @@ __global__ void __launch_bounds__(1024) k_basescan(PlanDev P, int bits) {
     __syncthreads();
     uint32_t run = warp_sums[warp] + incl - sum;
     for (uint32_t i = beg; i < end; i++) {
-        uint32_t v = R.total[i];
+        const uint32_t v = R.total[i];
         R.base[i] = run;
         run += v;
     }
-    if (lane == 0) atomicMax(blockIdx.x == 0 ? &P.ctr->max_r_part : &P.ctr->max_s_part, mx);
+    JoinCtr *jc = P.join[R.join].ctr;
+    if (lane == 0) atomicMax((blockIdx.x & 1) == 0 ? &jc->max_r_part : &jc->max_s_part, mx);
 }
 
 // --------------------------------------------------------------- scatter --
@@ -309,16 +337,17 @@ __device__ __forceinline__ void tile_init(TileSmem &S) {
 
 // Pass 1: one CTA per chunk. Coarse bucket P = p >> b2; the write cursor of
 // (chunk c, bucket P) is base[P << b2] + sum_q off[c][(P << b2) + q].
-__global__ void __launch_bounds__(kScatterThreads, 2) k_scatter1(PlanDev P, int bits, int b2) {
+__global__ void __launch_bounds__(kScatterThreads, 2) k_scatter1(PlanDev P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
+    const uint32_t r = find_slot(P.chunk_prefix, P.nrel, blockIdx.x);
+    const uint32_t c = blockIdx.x - P.chunk_prefix[r];
+    const RelDev R = P.rel[r];
+    const JoinDev &J = P.join[R.join];
+    const int bits = J.bits, b2 = J.fine_bits;
     const uint32_t F = 1u << bits, mask = F - 1;
     const int nb = 1 << (bits - b2);
     const int q_per = 1 << b2;
-    int rel;
-    unsigned c;
-    chunk_of(P, blockIdx.x, rel, c);
-    const RelDev R = rel == 0 ? P.rel[0] : P.rel[1];
     const uint32_t *off = R.hist + (size_t)c * F;
     tile_init(S);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -336,30 +365,32 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_scatter1(PlanDev P, int 
     uint32_t uses[2] = {0, 0};
     scatter_range(R.in, b0, e0, dst, S, nb,
                   [=](uint32_t key) { return (int)((glb_partition_hash(key) & mask) >> b2); }, uses,
-                  &P.ctr->error);
+                  &J.ctr->error);
 }
 
 // Work list of pass 2: for every (relation, coarse bucket), runs of consecutive
-// chunks holding at least `target` tuples. Within a coarse region the chunks'
-// segments follow each other in chunk order, as do the fine offsets, so cursors
-// set from a run's first chunk stay exact. A heavy single segment is its own item.
-__global__ void k_items(PlanDev P, int bits, int b2, uint32_t target) {
-    const uint32_t f1 = 1u << (bits - b2);
+// chunks holding at least `item_target` tuples. Within a coarse region the
+// chunks' segments follow each other in chunk order, as do the fine offsets, so
+// cursors set from a run's first chunk stay exact. A heavy single segment is its
+// own item.
+__global__ void k_items(PlanDev P) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * f1) return;
-    const int rel = t < f1 ? 0 : 1;
-    const uint32_t cb = t < f1 ? t : t - f1;
-    const RelDev R = rel == 0 ? P.rel[0] : P.rel[1];
+    if (t >= P.total_coarse) return;
+    const uint32_t r = find_slot(P.coarse_prefix, P.nrel, t);
+    const uint32_t cb = t - P.coarse_prefix[r];
+    const RelDev R = P.rel[r];
+    const JoinDev &J = P.join[R.join];
+    const uint32_t f1 = 1u << (J.bits - J.fine_bits);
     uint32_t acc = 0, c0 = 0;
     for (uint32_t c = 0; c < R.nchunks; c++) {
         acc += R.chist[(size_t)c * f1 + cb];
-        if (acc >= target || c + 1 == R.nchunks) {
+        if (acc >= J.item_target || c + 1 == R.nchunks) {
             if (acc) {
-                const unsigned i = atomicAdd(&P.ctr->item_count, 1u);
+                const unsigned i = atomicAdd(&P.bctr->item_count, 1u);
                 if (i < P.max_items)
-                    P.items[i] = make_uint4((uint32_t)rel, cb, c0, c + 1);
+                    P.items[i] = make_uint4(r, cb, c0, c + 1);
                 else
-                    atomicOr(&P.ctr->error, 4u);
+                    atomicOr(&J.ctr->error, 4u);
             }
             acc = 0;
             c0 = c + 1;
@@ -369,18 +400,15 @@ __global__ void k_items(PlanDev P, int bits, int b2, uint32_t target) {
 
 // Pass 2: persistent CTAs over the work list; each item scatters one run of a
 // coarse region to the final fine positions.
-__global__ void __launch_bounds__(kScatterThreads, 2) k_scatter2(PlanDev P, int bits, int b2) {
+__global__ void __launch_bounds__(kScatterThreads, 2) k_scatter2(PlanDev P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
-    const uint32_t F = 1u << bits;
-    const int nb = 1 << b2;
-    const uint32_t qmask = (uint32_t)nb - 1;
     tile_init(S);
     uint32_t uses[2] = {0, 0};
-    const unsigned n_items = min(*(volatile unsigned *)&P.ctr->item_count, P.max_items);
+    const unsigned n_items = min(*(volatile unsigned *)&P.bctr->item_count, P.max_items);
     for (;;) {
         if (threadIdx.x == 0) {
-            S.item = atomicAdd(&P.ctr->item_next, 1u);
+            S.item = atomicAdd(&P.bctr->item_next, 1u);
             S.seg_begin = 0;
             S.seg_len = 0;
         }
@@ -388,7 +416,12 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_scatter2(PlanDev P, int 
         const unsigned it = S.item;
         if (it >= n_items) break;
         const uint4 item = P.items[it];
-        const RelDev R = item.x == 0 ? P.rel[0] : P.rel[1];
+        const RelDev R = P.rel[item.x];
+        const JoinDev &J = P.join[R.join];
+        const int b2 = J.fine_bits;
+        const uint32_t F = 1u << J.bits;
+        const int nb = 1 << b2;
+        const uint32_t qmask = (uint32_t)nb - 1;
         const uint32_t cb = item.y, c0 = item.z, c1 = item.w;
         const uint32_t *off = R.hist + (size_t)c0 * F;
         const uint32_t *nxt = c1 < R.nchunks ? R.hist + (size_t)c1 * F : R.total;
@@ -406,64 +439,158 @@ __global__ void __launch_bounds__(kScatterThreads, 2) k_scatter2(PlanDev P, int 
         const uint32_t beg = R.base[cb << b2] + S.seg_begin;
         const bool ok = scatter_range(R.tmp, beg, beg + S.seg_len, R.out, S, nb,
                                       [=](uint32_t key) { return (int)(glb_partition_hash(key) & qmask); }, uses,
-                                      &P.ctr->error);
+                                      &J.ctr->error);
         __syncthreads();
         if (!ok) break;
     }
 }
 
 // ----------------------------------------------------------------- units --
-// One thread per partition. The reference replicates every R partition to
+// One warp per (join, partition). The reference replicates every R partition to
 // rank_set x bank_set DPUs and splits S among the replicas by element index
 // (glb_partition_count.c:317-318, glb_chipwise_partition_count.c:251-255);
 // here the replicas are work units, each a CTA that builds the same table and
 // probes a contiguous slice of the partition's S.
-__global__ void k_units(PlanDev P, int bits, JoinParams jp) {
-    // one warp per partition: lane 0 reserves, the lanes write the units
-    const uint32_t F = 1u << bits;
-    const uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (p >= F) return;
-    const uint32_t nr = P.rel[0].total[p], ns = P.rel[1].total[p];
-    if (ns == 0) return;
-    if (nr == 0 && !jp.keep_unmatched) return;
+// Number of units of flat partition t of join j (0 when there is nothing to join).
+__device__ __forceinline__ uint32_t unit_count_of(const PlanDev &P, uint32_t j, uint32_t p, uint32_t &ns,
+                                                  uint32_t &s0) {
+    const JoinDev &J = P.join[j];
+    const RelDev &Rr = P.rel[2 * j], &Rs = P.rel[2 * j + 1];
+    uint32_t nr;
+    if (J.alg == SPJ_ALG_NPHJ) {  // no partitions: units are raw ranges of S
+        if (p > 0) return 0;
+        nr = Rr.n;
+        ns = Rs.n;
+        s0 = 0;
+    } else {
+        nr = Rr.total[p];
+        ns = Rs.total[p];
+        s0 = Rs.base[p];
+    }
+    if (ns == 0) return 0;
+    if (nr == 0 && !J.keep_unmatched) return 0;
     uint32_t g;
-    if (jp.skew_mode == SPJ_SKEW_FIXED) {
-        g = (uint32_t)max(jp.group, 1);
+    if (J.skew_mode == SPJ_SKEW_FIXED && J.alg != SPJ_ALG_NPHJ) {
+        g = (uint32_t)max(J.group, 1);
     } else {
         g = 1;
-        if (ns > jp.unit_tuples) {
-            g = (ns + jp.unit_tuples - 1) / jp.unit_tuples;
-            g = max(g, (uint32_t)max(jp.group, 1));
+        if (ns > J.unit_tuples) {
+            g = (ns + J.unit_tuples - 1) / J.unit_tuples;
+            g = max(g, (uint32_t)max(J.group, 1));
         }
     }
-    g = min(g, ns);
+    return min(g, ns);
+}
+
+// Units, step 1: every (join, partition) adds its unit count to its join.
+__global__ void k_units_count(PlanDev P) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.total_jparts) return;
+    const uint32_t j = find_slot(P.jpart_prefix, P.njoin, t);
+    uint32_t ns = 0, s0 = 0;
+    const uint32_t g = unit_count_of(P, j, t - P.jpart_prefix[j], ns, s0);
+    if (g) atomicAdd(&P.join[j].ctr->units, g);
+}
+
+// Units, step 2: each join's units get a contiguous range of the queue, so a
+// CTA meets every join in one stretch (at most one output hole per warp and join).
+__global__ void __launch_bounds__(1024) k_units_scan(PlanDev P) {
+    __shared__ uint32_t warp_sums[32];
+    const uint32_t J = P.njoin;
+    const uint32_t per = (J + blockDim.x - 1) / blockDim.x;
+    const uint32_t beg = threadIdx.x * per, end = min(J, beg + per);
+    uint32_t sum = 0;
+    for (uint32_t j = beg; j < end; j++) sum += P.join[j].ctr->units;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = warp_sums[lane];
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += x;
+        }
+        warp_sums[lane] = wi - w;
+        if (lane == 31) P.bctr->unit_count = wi;
+    }
+    __syncthreads();
+    uint32_t run = warp_sums[warp] + incl - sum;
+    for (uint32_t j = beg; j < end; j++) {
+        JoinCtr *c = P.join[j].ctr;
+        c->unit_base = run;
+        run += c->units;
+    }
+}
+
+// Units, step 3: one warp per (join, partition) writes its units. The reference
+// replicates every R partition to rank_set x bank_set DPUs and splits S among
+// the replicas by element index (glb_partition_count.c:317-318,
+// glb_chipwise_partition_count.c:251-255); here the replicas are work units,
+// each a CTA that builds the same table and probes a contiguous slice of the
+// partition's S.
+__global__ void k_units(PlanDev P) {
+    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= P.total_jparts) return;
+    const uint32_t j = find_slot(P.jpart_prefix, P.njoin, t);
+    const uint32_t p = t - P.jpart_prefix[j];
+    uint32_t ns = 0, s0 = 0;
+    const uint32_t g = unit_count_of(P, j, p, ns, s0);
+    if (g == 0) return;
+    JoinCtr *c = P.join[j].ctr;
     uint32_t first = 0;
-    if (lane == 0) first = atomicAdd(&P.ctr->unit_count, g);
+    if (lane == 0) first = c->unit_base + atomicAdd(&c->unit_fill, g);
     first = __shfl_sync(0xffffffffu, first, 0);
     if (first + g > P.max_units) {
-        if (lane == 0) atomicOr(&P.ctr->error, 4u);
+        if (lane == 0) atomicOr(&c->error, 4u);
         return;
     }
-    const uint32_t s0 = P.rel[1].base[p];
     for (uint32_t k = lane; k < g; k += 32) {
         Unit u;
         u.p = p;
         u.s_begin = s0 + (uint32_t)(((uint64_t)ns * k) / g);
         u.s_end = s0 + (uint32_t)(((uint64_t)ns * (k + 1)) / g);
-        u.pad = 0;
+        u.join = j;
         P.units[first + k] = u;
     }
 }
 
 // ------------------------------------------------------- output emission --
+// The output state of the join a CTA is working on.
+struct OutCtx {
+    Tuple *out;
+    unsigned long long cap;
+    JoinCtr *ctr;
+    Hole *holes;
+    uint32_t chunk;
+};
+
+__device__ __forceinline__ OutCtx out_ctx(const JoinDev &J) {
+    OutCtx o;
+    o.out = J.out;
+    o.cap = J.out_cap;
+    o.ctr = J.ctr;
+    o.holes = J.holes;
+    o.chunk = J.out_chunk;
+    return o;
+}
+
 struct WarpOut {
     unsigned long long cur, end;
 };
 
-// Warp-aggregated append: one ballot per 32 candidate pairs; a fresh 1024-pair
-// chunk is reserved with one global atomic when the warp's chunk runs out.
-__device__ __forceinline__ void warp_emit(const PlanDev &P, WarpOut &w, bool has, uint32_t lv, uint32_t rv) {
+// Warp-aggregated append: one ballot per 32 candidate pairs; a fresh chunk of
+// the join's output (out_chunk pairs, <= 1024) is reserved with one global
+// atomic when the warp's chunk runs out.
+__device__ __forceinline__ void warp_emit(const OutCtx &o, WarpOut &w, bool has, uint32_t lv, uint32_t rv) {
     const unsigned mask = __ballot_sync(0xffffffffu, has);
     if (mask == 0) return;
     const unsigned m = __popc(mask);
@@ -475,30 +602,32 @@ __device__ __forceinline__ void warp_emit(const PlanDev &P, WarpOut &w, bool has
     } else {
         const unsigned avail = (unsigned)(w.end - w.cur);
         unsigned long long nb = 0;
-        if ((threadIdx.x & 31) == 0) nb = atomicAdd(&P.ctr->out_reserved, (unsigned long long)kOutChunk);
+        if ((threadIdx.x & 31) == 0) nb = atomicAdd(&o.ctr->out_reserved, (unsigned long long)o.chunk);
         nb = __shfl_sync(0xffffffffu, nb, 0);
         pos = rank < avail ? w.cur + rank : nb + (rank - avail);
         w.cur = nb + (m - avail);
-        w.end = nb + kOutChunk;
+        w.end = nb + o.chunk;
     }
     if (has) {
-        if (pos < P.out_cap)
-            reinterpret_cast<uint2 *>(P.out)[pos] = make_uint2(lv, rv);
+        if (pos < o.cap)
+            reinterpret_cast<uint2 *>(o.out)[pos] = make_uint2(lv, rv);
         else
-            atomicOr(&P.ctr->error, 2u);
+            atomicOr(&o.ctr->error, 2u);
     }
 }
 
-__device__ __forceinline__ void warp_close(const PlanDev &P, WarpOut &w) {
+// Records the unused tail of the warp's chunk as the warp's hole in this join.
+__device__ __forceinline__ void warp_close(const OutCtx &o, WarpOut &w) {
     if ((threadIdx.x & 31) == 0 && w.end > w.cur) {
-        unsigned h = atomicAdd(&P.ctr->hole_count, 1u);
+        const unsigned h = atomicAdd(&o.ctr->hole_count, 1u);
         if (h < kMaxHoles) {
-            P.holes[h].begin = w.cur;
-            P.holes[h].end = w.end;
+            o.holes[h].begin = w.cur;
+            o.holes[h].end = w.end;
         } else {
-            atomicOr(&P.ctr->error, 8u);
+            atomicOr(&o.ctr->error, 8u);
         }
     }
+    w.cur = w.end = 0ull;
 }
 
 // Table slot of a key: the hash bits above the partition bits, scaled to the
@@ -512,13 +641,15 @@ __device__ __forceinline__ uint32_t slot_of(uint32_t key, uint32_t bits, uint32_
 // (a2a_srj_build.c:208-246). A key already present is not inserted again, so the
 // probe returns the first-inserted tuple of a repeated key, one match per S tuple
 // (a2a_srj_probe_inner_mt.c:136-148).
-__device__ __forceinline__ void build_table(const PlanDev &P, const JoinParams &jp, unsigned long long *table,
-                                            uint32_t p) {
-    const uint32_t ts = jp.table_slots;
+__device__ __forceinline__ void build_table(const PlanDev &P, const JoinDev &J, uint32_t j, uint32_t p,
+                                            unsigned long long *table) {
+    const uint32_t ts = J.table_slots;
+    const uint32_t bits = J.bits;
     for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) table[i] = 0ull;
     __syncthreads();
-    const uint32_t nr = P.rel[0].total[p];
-    const Tuple *pr = P.rel[0].out + P.rel[0].base[p];
+    const RelDev &Rr = P.rel[2 * j];
+    const uint32_t nr = Rr.total[p];
+    const Tuple *pr = Rr.out + Rr.base[p];
     constexpr int B = 4;  // loads in flight per thread
     for (uint32_t i0 = threadIdx.x; i0 < nr; i0 += B * blockDim.x) {
         Tuple t[B];
@@ -531,13 +662,13 @@ __device__ __forceinline__ void build_table(const PlanDev &P, const JoinParams &
         for (int k = 0; k < B; k++) {
             if (t[k].key == 0) continue;
             const unsigned long long ent = ((unsigned long long)t[k].pay << 32) | t[k].key;
-            uint32_t s = slot_of(t[k].key, jp.bits, ts);
+            uint32_t s = slot_of(t[k].key, bits, ts);
             for (uint32_t step = 0;; step++) {
                 const unsigned long long prev = atomicCAS(&table[s], 0ull, ent);
                 if (prev == 0ull || (uint32_t)prev == t[k].key) break;
                 if (++s == ts) s = 0;
                 if (step >= ts) {
-                    atomicOr(&P.ctr->error, 1u);
+                    atomicOr(&J.ctr->error, 1u);
                     break;
                 }
             }
@@ -593,7 +724,7 @@ __device__ __forceinline__ bool probe_table(const unsigned long long *table, uin
 
 // Fetches the next unit for the CTA; returns false when the queue is empty.
 __device__ __forceinline__ bool next_unit(const PlanDev &P, unsigned n_units, unsigned *s_slot, Unit &un) {
-    if (threadIdx.x == 0) *s_slot = atomicAdd(&P.ctr->unit_next, 1u);
+    if (threadIdx.x == 0) *s_slot = atomicAdd(&P.bctr->unit_next, 1u);
     __syncthreads();
     const unsigned u = *s_slot;
     __syncthreads();
@@ -602,22 +733,34 @@ __device__ __forceinline__ bool next_unit(const PlanDev &P, unsigned n_units, un
     return true;
 }
 
+// Switches the CTA's output state to join j (closing the warp's chunk of the
+// previous join, which leaves that join at most one hole per warp).
+__device__ __forceinline__ void switch_join(const PlanDev &P, uint32_t j, uint32_t &cur_j, OutCtx &o, WarpOut &w) {
+    if (j == cur_j) return;
+    if (cur_j != 0xffffffffu) warp_close(o, w);
+    cur_j = j;
+    o = out_ctx(P.join[j]);
+}
+
 // ----------------------------------------------------- partitioned hash join --
-__global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P, JoinParams jp) {
+__global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
     extern __shared__ unsigned long long table[];
     __shared__ unsigned s_slot;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const uint32_t ts = jp.table_slots;
-    const unsigned n_units = *(volatile unsigned *)&P.ctr->unit_count;
-    const Tuple *ps = P.rel[1].out;
+    const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
     WarpOut w{0ull, 0ull};
-    uint32_t cur_p = 0xffffffffu;
+    OutCtx o{};
+    uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu;
     Unit un;
     while (next_unit(P, n_units, &s_slot, un)) {
-        if (un.p != cur_p) {
-            build_table(P, jp, table, un.p);
+        const JoinDev &J = P.join[un.join];
+        if (un.join != cur_j || un.p != cur_p) {
+            switch_join(P, un.join, cur_j, o, w);
+            build_table(P, J, un.join, un.p, table);
             cur_p = un.p;
         }
+        const uint32_t ts = J.table_slots, bits = J.bits;
+        const Tuple *ps = P.rel[2 * un.join + 1].out;
         constexpr int U = 4;
         for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
             Tuple t[U];
@@ -629,13 +772,13 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P, JoinPar
 #pragma unroll
             for (int k = 0; k < U; k++) {
                 uint32_t rp = 0;
-                const bool hit = t[k].key != 0 && probe_table(table, ts, jp.bits, t[k].key, rp);
-                warp_emit(P, w, hit, rp, t[k].pay);
+                const bool hit = t[k].key != 0 && probe_table(table, ts, bits, t[k].key, rp);
+                warp_emit(o, w, hit, rp, t[k].pay);
             }
         }
         __syncthreads();
     }
-    warp_close(P, w);
+    if (cur_j != 0xffffffffu) warp_close(o, w);
 }
 
 // Block-wide exclusive scan of n <= 256 counters by warp 0 (8 per lane); writes
@@ -673,31 +816,35 @@ __device__ __forceinline__ void warp0_scan256(const uint32_t *cnt, uint32_t *off
 // each S tuple compares its key with every R tuple of its sub-partition and takes
 // the first equal one. S is rewritten in place: unmatched S tuples are emitted
 // unchanged.
-__global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P, JoinParams jp) {
+__global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
     extern __shared__ unsigned long long smem_u64[];
     __shared__ unsigned s_slot;
     __shared__ uint32_t bcnt[256], boff[257];
     Tuple *rs = reinterpret_cast<Tuple *>(smem_u64);
-    const uint32_t cap = jp.table_slots;  // R tuples that fit
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const unsigned n_units = *(volatile unsigned *)&P.ctr->unit_count;
-    const Tuple *ps = P.rel[1].out;
+    const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
     WarpOut w{0ull, 0ull};
-    uint32_t cur_p = 0xffffffffu, nr = 0, lmask = 0;
+    OutCtx o{};
+    uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0, lmask = 0;
     Unit un;
     while (next_unit(P, n_units, &s_slot, un)) {
-        if (un.p != cur_p) {
+        const JoinDev &J = P.join[un.join];
+        const uint32_t bits = J.bits;
+        if (un.join != cur_j || un.p != cur_p) {
+            switch_join(P, un.join, cur_j, o, w);
             cur_p = un.p;
-            nr = min(P.rel[0].total[un.p], cap);
-            if (threadIdx.x == 0 && P.rel[0].total[un.p] > cap) atomicOr(&P.ctr->error, 1u);
+            const RelDev &Rr = P.rel[2 * un.join];
+            const uint32_t cap = J.table_slots;  // R tuples that fit
+            nr = min(Rr.total[un.p], cap);
+            if (threadIdx.x == 0 && Rr.total[un.p] > cap) atomicOr(&J.ctr->error, 1u);
             uint32_t L = 1;
             while (L < 256 && L * 64 < nr) L <<= 1;
             lmask = L - 1;
             for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) bcnt[i] = 0;
             __syncthreads();
-            const Tuple *pr = P.rel[0].out + P.rel[0].base[un.p];
+            const Tuple *pr = Rr.out + Rr.base[un.p];
             for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x)
-                atomicAdd(&bcnt[(glb_partition_hash(pr[i].key) >> jp.bits) & lmask], 1u);
+                atomicAdd(&bcnt[(glb_partition_hash(pr[i].key) >> bits) & lmask], 1u);
             __syncthreads();
             warp0_scan256(bcnt, boff, (int)L);
             __syncthreads();
@@ -705,11 +852,12 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P, JoinPara
             __syncthreads();
             for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
                 const Tuple t = pr[i];
-                const uint32_t b = (glb_partition_hash(t.key) >> jp.bits) & lmask;
+                const uint32_t b = (glb_partition_hash(t.key) >> bits) & lmask;
                 rs[atomicAdd(&bcnt[b], 1u)] = t;
             }
             __syncthreads();
         }
+        const Tuple *ps = P.rel[2 * un.join + 1].out;
         constexpr int U = 4;
         for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
             Tuple t[U];
@@ -720,10 +868,11 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P, JoinPara
             }
 #pragma unroll
             for (int k = 0; k < U; k++) {
-                bool valid = t[k].key != 0, hit = false;
+                const bool valid = t[k].key != 0;
+                bool hit = false;
                 uint32_t rp = 0;
                 if (valid && nr) {
-                    const uint32_t b = (glb_partition_hash(t[k].key) >> jp.bits) & lmask;
+                    const uint32_t b = (glb_partition_hash(t[k].key) >> bits) & lmask;
                     for (uint32_t i = boff[b], e = boff[b + 1]; i < e; i++) {
                         const Tuple r = rs[i];
                         if (r.key == t[k].key) {
@@ -733,12 +882,12 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P, JoinPara
                         }
                     }
                 }
-                warp_emit(P, w, valid, hit ? rp : t[k].key, t[k].pay);
+                warp_emit(o, w, valid, hit ? rp : t[k].key, t[k].pay);
             }
         }
         __syncthreads();
     }
-    warp_close(P, w);
+    if (cur_j != 0xffffffffu) warp_close(o, w);
 }
 
 // ----------------------------------------------------------- sort-merge join --
@@ -762,32 +911,35 @@ __device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v) 
     return v;
 }
 
-__global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P, JoinParams jp) {
+__global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
     extern __shared__ unsigned long long sorted[];
     __shared__ unsigned s_slot;
-    uint32_t cap = 1;  // largest power of two that fits the shared-memory budget
-    while (cap * 2 <= (uint32_t)jp.table_slots) cap <<= 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const unsigned n_units = *(volatile unsigned *)&P.ctr->unit_count;
-    const Tuple *ps = P.rel[1].out;
+    const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
     WarpOut w{0ull, 0ull};
-    uint32_t cur_p = 0xffffffffu, nr = 0;
+    OutCtx o{};
+    uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0;
     Unit un;
     while (next_unit(P, n_units, &s_slot, un)) {
-        if (un.p != cur_p) {
+        const JoinDev &J = P.join[un.join];
+        if (un.join != cur_j || un.p != cur_p) {
+            switch_join(P, un.join, cur_j, o, w);
             cur_p = un.p;
-            nr = min(P.rel[0].total[un.p], cap);
-            if (threadIdx.x == 0 && P.rel[0].total[un.p] > cap) atomicOr(&P.ctr->error, 1u);
+            uint32_t cap = 1;  // largest power of two that fits the shared-memory budget
+            while (cap * 2 <= (uint32_t)J.table_slots) cap <<= 1;
+            const RelDev &Rr = P.rel[2 * un.join];
+            nr = min(Rr.total[un.p], cap);
+            if (threadIdx.x == 0 && Rr.total[un.p] > cap) atomicOr(&J.ctr->error, 1u);
             uint32_t npad = 1;
             while (npad < nr) npad <<= 1;
-            const Tuple *pr = P.rel[0].out + P.rel[0].base[un.p];
+            const Tuple *pr = Rr.out + Rr.base[un.p];
             for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x)
                 sorted[i] = i < nr ? ((unsigned long long)pr[i].key << 32) | pr[i].pay : ~0ull;
             __syncthreads();
             for (uint32_t k = 2; k <= npad; k <<= 1) {
-                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
                     for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x) {
-                        const uint32_t ixj = i ^ j;
+                        const uint32_t ixj = i ^ jj;
                         if (ixj > i) {
                             const unsigned long long a = sorted[i], b = sorted[ixj];
                             if ((a > b) == ((i & k) == 0)) {
@@ -800,6 +952,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P, JoinPar
                 }
             }
         }
+        const Tuple *ps = P.rel[2 * un.join + 1].out;
         for (uint32_t base = un.s_begin + warp * 32; base < un.s_end; base += nwarps * 32) {
             const uint32_t idx = base + lane;
             const bool in = idx < un.s_end;
@@ -828,23 +981,36 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P, JoinPar
                     rp = (uint32_t)sorted[lo];
                 }
             }
-            warp_emit(P, w, mine, hit ? rp : t.key, t.pay);
+            warp_emit(o, w, mine, hit ? rp : t.key, t.pay);
         }
         __syncthreads();
     }
-    warp_close(P, w);
+    if (cur_j != 0xffffffffu) warp_close(o, w);
 }
 
 // ------------------------------------------- non-partitioned hash join (NPHJ) --
 // packetwise_no_partitioned_hash_join_build.c:88-160 / _probe.c:86-140 on B200:
-// one linear-probe table over all of R in HBM (2^k >= 2|R| slots, slot from
-// join_hash2 as in the reference), built with 64-bit global CAS, then probed by
-// a stream over S. No partitioning pass; the table's random reads are served by
-// L2 when R is small.
-__global__ void k_nphj_build(PlanDev P, uint32_t tmask) {
-    const Tuple *r = P.rel[0].in;
-    const uint32_t n = P.rel[0].n;
-    unsigned long long *table = P.gtable;
+// one linear-probe table per join over all of its R in HBM (2^k >= 2|R| slots,
+// slot from join_hash2 as in the reference), built with 64-bit global CAS, then
+// probed by a stream over S (units are raw S ranges). No partitioning pass; the
+// table's random reads are served by L2 when R is small.
+__global__ void k_nphj_clear(PlanDev P) {
+    const JoinDev &J = P.join[blockIdx.y];
+    if (J.alg != SPJ_ALG_NPHJ) return;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < J.gtable_slots;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        J.gtable[i] = 0ull;
+}
+
+__global__ void k_nphj_build(PlanDev P) {
+    const uint32_t j = blockIdx.y;
+    const JoinDev &J = P.join[j];
+    if (J.alg != SPJ_ALG_NPHJ) return;
+    const RelDev &Rr = P.rel[2 * j];
+    const Tuple *r = Rr.in;
+    const uint32_t n = Rr.n;
+    const uint32_t tmask = (uint32_t)(J.gtable_slots - 1);
+    unsigned long long *table = J.gtable;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const Tuple t = r[i];
         if (t.key == 0) continue;
@@ -854,63 +1020,71 @@ __global__ void k_nphj_build(PlanDev P, uint32_t tmask) {
             const unsigned long long prev = atomicCAS(&table[s], 0ull, ent);
             if (prev == 0ull || (uint32_t)prev == t.key) break;
             s = (s + 1) & tmask;
-            if (step == tmask) atomicOr(&P.ctr->error, 1u);
+            if (step == tmask) atomicOr(&J.ctr->error, 1u);
         }
     }
 }
 
-__global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P, uint32_t tmask) {
-    const Tuple *s = P.rel[1].in;
-    const uint32_t n = P.rel[1].n;
-    const unsigned long long *table = P.gtable;
-    const int lane = threadIdx.x & 31;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+__global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
+    __shared__ unsigned s_slot;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
     WarpOut w{0ull, 0ull};
-    constexpr int U = 4;
-    for (uint32_t base = gw * 32 * U; base < n; base += nw * 32 * U) {
-        Tuple t[U];
+    OutCtx o{};
+    uint32_t cur_j = 0xffffffffu;
+    Unit un;
+    while (next_unit(P, n_units, &s_slot, un)) {
+        switch_join(P, un.join, cur_j, o, w);
+        const JoinDev &J = P.join[un.join];
+        const unsigned long long *table = J.gtable;
+        const uint32_t tmask = (uint32_t)(J.gtable_slots - 1);
+        const Tuple *s = P.rel[2 * un.join + 1].in;
+        constexpr int U = 4;
+        for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
+            Tuple t[U];
 #pragma unroll
-        for (int k = 0; k < U; k++) {
-            const uint32_t idx = base + k * 32 + lane;
-            t[k] = idx < n ? s[idx] : Tuple{0u, 0u};
-        }
-        uint32_t sl[U];
-        unsigned long long e[U];
-#pragma unroll
-        for (int k = 0; k < U; k++) {
-            sl[k] = join_hash2(t[k].key) & tmask;
-            e[k] = t[k].key ? __ldg(&table[sl[k]]) : 0ull;
-        }
-#pragma unroll
-        for (int k = 0; k < U; k++) {
-            bool hit = false;
-            uint32_t rp = 0;
-            if (t[k].key) {
-                uint32_t sx = sl[k];
-                unsigned long long ex = e[k];
-                for (uint32_t step = 0; step <= tmask; step++) {
-                    if ((uint32_t)ex == t[k].key) {
-                        hit = true;
-                        rp = (uint32_t)(ex >> 32);
-                        break;
-                    }
-                    if ((uint32_t)ex == 0) break;
-                    sx = (sx + 1) & tmask;
-                    ex = __ldg(&table[sx]);
-                }
+            for (int k = 0; k < U; k++) {
+                const uint32_t idx = base + k * 32 + lane;
+                t[k] = idx < un.s_end ? s[idx] : Tuple{0u, 0u};
             }
-            warp_emit(P, w, hit, rp, t[k].pay);
+            uint32_t sl[U];
+            unsigned long long e[U];
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                sl[k] = join_hash2(t[k].key) & tmask;
+                e[k] = t[k].key ? __ldg(&table[sl[k]]) : 0ull;
+            }
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                bool hit = false;
+                uint32_t rp = 0;
+                if (t[k].key) {
+                    uint32_t sx = sl[k];
+                    unsigned long long ex = e[k];
+                    for (uint32_t step = 0; step <= tmask; step++) {
+                        if ((uint32_t)ex == t[k].key) {
+                            hit = true;
+                            rp = (uint32_t)(ex >> 32);
+                            break;
+                        }
+                        if ((uint32_t)ex == 0) break;
+                        sx = (sx + 1) & tmask;
+                        ex = __ldg(&table[sx]);
+                    }
+                }
+                warp_emit(o, w, hit, rp, t[k].pay);
+            }
         }
+        __syncthreads();
     }
-    warp_close(P, w);
+    if (cur_j != 0xffffffffu) warp_close(o, w);
 }
 
 // ------------------------------------------------------------------ fix-up --
-// Every reserved chunk is 1024-aligned and only a warp's last chunk can be
-// partly used, so the unused slots form at most one hole per warp at a chunk's
-// tail. With N = reserved - holes, the pairs stored at positions >= N outside
-// holes move into the holes below N.
+// Every reserved chunk is 1024-aligned and only a warp's last chunk of a join
+// can be partly used, so the unused slots form at most one hole per warp and
+// join, at a chunk's tail. With N = reserved - holes, the pairs stored at
+// positions >= N outside holes move into the holes below N. One CTA per join.
 // Exclusive scan in place of a[0..n) (n <= 12 * 1024) by a 1024-thread block;
 // returns the total. Each thread scans 12 consecutive entries.
 __device__ unsigned long long block_exclusive_scan(unsigned long long *a, unsigned n, unsigned long long *warp_tot) {
@@ -958,13 +1132,15 @@ __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
     extern __shared__ unsigned long long keys[];  // kHoleSortSlots sorted holes, then kMaxHoles scan slots
     __shared__ unsigned long long warp_tot[33];
     __shared__ unsigned s_nl, s_i0;
+    const JoinDev &J = P.join[blockIdx.x];
+    JoinCtr *ctr = J.ctr;
     unsigned long long *scan = keys + kHoleSortSlots;
-    const unsigned nh = min(P.ctr->hole_count, (unsigned)kMaxHoles);
+    const unsigned nh = min(ctr->hole_count, (unsigned)kMaxHoles);
     unsigned npow = 1;
     while (npow < nh) npow <<= 1;
     for (unsigned i = threadIdx.x; i < npow; i += blockDim.x) {
         if (i < nh) {
-            const Hole h = P.holes[i];
+            const Hole h = J.holes[i];
             keys[i] = (h.begin << 11) | (h.end - h.begin);
         } else {
             keys[i] = ~0ull;
@@ -994,7 +1170,7 @@ __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
     for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) scan[i] = keys[i] & 2047ull;
     __syncthreads();
     const unsigned long long H = block_exclusive_scan(scan, nh, warp_tot);
-    const unsigned long long total = P.ctr->out_reserved;
+    const unsigned long long total = ctr->out_reserved;
     const unsigned long long N = total - H;
     // parts of each hole below N (gaps to fill) and above N (skipped by the data)
     for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) {
@@ -1007,8 +1183,8 @@ __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
     const unsigned long long G = block_exclusive_scan(scan, nh, warp_tot);
     const unsigned nl = s_nl, i0 = s_i0;
     for (unsigned i = threadIdx.x; i < nl; i += blockDim.x) {
-        P.gaps[i].begin = keys[i] >> 11;
-        P.gap_off[i] = scan[i];
+        J.gaps[i].begin = keys[i] >> 11;
+        J.gap_off[i] = scan[i];
     }
     __syncthreads();
     for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) {
@@ -1021,15 +1197,15 @@ __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
         const unsigned long long b = keys[i] >> 11, e = b + (keys[i] & 2047ull);
         const unsigned long long ub = b > N ? b : N;
         // data elements stored before this hole, and holes' length up to and including it
-        P.datas[i - i0].begin = ub - N - scan[i];
-        P.data_off[i - i0] = scan[i] + (e - ub);
+        J.datas[i - i0].begin = ub - N - scan[i];
+        J.data_off[i - i0] = scan[i] + (e - ub);
     }
     if (threadIdx.x == 0) {
-        P.ctr->n_out = N;
-        if (P.n_out_user) *P.n_out_user = N;
-        P.ctr->gap_total = G;
-        P.ctr->n_gaps = nl;
-        P.ctr->n_data = nh - i0;
+        ctr->n_out = N;
+        if (J.n_out_user) *J.n_out_user = N;
+        ctr->gap_total = G;
+        ctr->n_gaps = nl;
+        ctr->n_data = nh - i0;
     }
 }
 
@@ -1047,29 +1223,31 @@ __device__ __forceinline__ unsigned upper_bound_u64(const unsigned long long *a,
 }
 
 __global__ void k_fixup_copy(PlanDev P) {
-    const unsigned long long G = P.ctr->gap_total;
-    if (G == 0 || (P.ctr->error & 8u)) return;  // holes were dropped: the count is unusable
-    const unsigned long long N = P.ctr->n_out;
-    const unsigned ng = P.ctr->n_gaps, nd = P.ctr->n_data;
-    uint2 *out = reinterpret_cast<uint2 *>(P.out);
+    const JoinDev &J = P.join[blockIdx.y];
+    JoinCtr *ctr = J.ctr;
+    const unsigned long long G = ctr->gap_total;
+    if (G == 0 || (ctr->error & 8u)) return;  // holes were dropped: the count is unusable
+    const unsigned long long N = ctr->n_out;
+    const unsigned ng = ctr->n_gaps, nd = ctr->n_data;
+    uint2 *out = reinterpret_cast<uint2 *>(J.out);
     for (unsigned long long x = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; x < G;
          x += (unsigned long long)gridDim.x * blockDim.x) {
         // destination: x-th slot of the holes below N
-        const unsigned gi = upper_bound_u64(P.gap_off, ng, x) - 1;
-        const unsigned long long dst = P.gaps[gi].begin + (x - P.gap_off[gi]);
+        const unsigned gi = upper_bound_u64(J.gap_off, ng, x) - 1;
+        const unsigned long long dst = J.gaps[gi].begin + (x - J.gap_off[gi]);
         // source: x-th stored pair at or above N (holes skipped)
         unsigned lo = 0, hi = nd;
         while (lo < hi) {
             const unsigned mid = (lo + hi) >> 1;
-            if (P.datas[mid].begin <= x)
+            if (J.datas[mid].begin <= x)
                 lo = mid + 1;
             else
                 hi = mid;
         }
-        const unsigned long long shift = lo > 0 ? P.data_off[lo - 1] : 0ull;
+        const unsigned long long shift = lo > 0 ? J.data_off[lo - 1] : 0ull;
         const unsigned long long src = N + x + shift;
-        if (src >= P.out_cap || dst >= N) {
-            atomicOr(&P.ctr->error, 16u);
+        if (src >= J.out_cap || dst >= N) {
+            atomicOr(&ctr->error, 16u);
             continue;
         }
         out[dst] = out[src];
@@ -1119,57 +1297,66 @@ __global__ void k_hist_single(const Tuple *t, uint64_t n, int bits, uint32_t *hi
 
 }  // namespace spj
 
-// Entry points used by spj_plan.cu (kept C++-linkage, internal).
+// Entry points used by spj_plan.cu and spj_noalloc.cu (C++ linkage, internal).
 namespace spj {
+
+cudaError_t init_single(spj_plan *pl, cudaStream_t st) {
+    const JoinHost &h = pl->joins[0];
+    const uint32_t f = 1u << h.dev.bits;
+    const uint32_t f1 = h.dev.fine_bits ? 1u << (h.dev.bits - h.dev.fine_bits) : 0u;
+    k_init_single<<<1, 32, 0, st>>>(pl->dev, h.rel[0], h.rel[1], h.dev, h.rel[0].nchunks, h.rel[1].nchunks, f, f1);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
     PlanDev &P = pl->dev;
-    const JoinParams &jp = pl->jp;
-    const int bits = jp.bits;
-    const unsigned F = 1u << bits;
-    const unsigned nchunks = P.rel[0].nchunks + P.rel[1].nchunks;
-    const size_t hsmem = (size_t)F * 4;
-    const int b2 = jp.fine_bits;
-    cudaEvent_t *ev = pl->have_events ? pl->ring[pl->ring_next] : nullptr;
+    // timing events are recorded on eager launches only (not while a graph is captured)
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cap);
+    cudaEvent_t *ev = (pl->have_events && cap == cudaStreamCaptureStatusNone) ? pl->ring[pl->ring_next] : nullptr;
     auto mark = [&](int i) {
         if (ev) cudaEventRecord(ev[i], st);
     };
+    const size_t jsm = (size_t)P.max_table_slots * 8;
+    const uint32_t J = P.njoin;
     mark(0);
-    if (jp.alg == SPJ_ALG_NPHJ) {
-        const uint32_t tmask = (uint32_t)(pl->gtable_slots - 1);
-        cudaMemsetAsync(P.gtable, 0, pl->gtable_slots * 8, st);
+    if (P.alg == SPJ_ALG_NPHJ) {
+        k_nphj_clear<<<dim3(pl->num_sms * 2, J), 256, 0, st>>>(P);
         mark(1);
         mark(2);
-        k_nphj_build<<<pl->num_sms * 8, 256, 0, st>>>(P, tmask);
+        k_nphj_build<<<dim3(pl->num_sms * 4, J), 256, 0, st>>>(P);
         mark(3);
+        k_units_count<<<(P.total_jparts + 255) / 256, 256, 0, st>>>(P);
+        k_units_scan<<<1, 1024, 0, st>>>(P);
+        k_units<<<(P.total_jparts * 32 + 255) / 256, 256, 0, st>>>(P);
         mark(4);
-        k_nphj_probe<<<pl->join_blocks, kJoinThreads, 0, st>>>(P, tmask);
+        k_nphj_probe<<<pl->join_blocks, kJoinThreads, 0, st>>>(P);
     } else {
-        k_hist<<<nchunks, kHistThreads, hsmem, st>>>(P, bits, b2);
+        k_hist<<<P.total_chunks, kHistThreads, (size_t)4 << P.max_bits, st>>>(P);
         mark(1);
-        k_colscan<<<dim3((F + 255) / 256, 2), 256, 0, st>>>(P, bits);
-        k_basescan<<<2, 1024, 0, st>>>(P, bits);
+        k_colscan<<<(P.total_parts + 255) / 256, 256, 0, st>>>(P);
+        k_basescan<<<P.nrel, 1024, 0, st>>>(P);
         mark(2);
-        k_scatter1<<<nchunks, kScatterThreads, sizeof(TileSmem), st>>>(P, bits, b2);
-        if (b2) {
-            const uint32_t f1 = 1u << (bits - b2);
-            k_items<<<(2 * f1 + 255) / 256, 256, 0, st>>>(P, bits, b2, pl->item_target);
-            k_scatter2<<<pl->num_sms * 2, kScatterThreads, sizeof(TileSmem), st>>>(P, bits, b2);
+        k_scatter1<<<P.total_chunks, kScatterThreads, sizeof(TileSmem), st>>>(P);
+        if (P.any_two_pass) {
+            if (P.total_coarse) k_items<<<(P.total_coarse + 255) / 256, 256, 0, st>>>(P);
+            k_scatter2<<<pl->num_sms * 2, kScatterThreads, sizeof(TileSmem), st>>>(P);
         }
         mark(3);
-        k_units<<<(F * 32 + 255) / 256, 256, 0, st>>>(P, bits, jp);
+        k_units_count<<<(P.total_jparts + 255) / 256, 256, 0, st>>>(P);
+        k_units_scan<<<1, 1024, 0, st>>>(P);
+        k_units<<<(P.total_jparts * 32 + 255) / 256, 256, 0, st>>>(P);
         mark(4);
-        const size_t jsm = (size_t)jp.table_slots * 8;
-        if (jp.alg == SPJ_ALG_SMJ)
-            k_join_smj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P, jp);
-        else if (jp.alg == SPJ_ALG_NL)
-            k_join_nl<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P, jp);
+        if (P.alg == SPJ_ALG_SMJ)
+            k_join_smj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
+        else if (P.alg == SPJ_ALG_NL)
+            k_join_nl<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
         else
-            k_join_phj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P, jp);
+            k_join_phj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
     }
     mark(5);
-    k_fixup_prep<<<1, 1024, (size_t)(kHoleSortSlots + kMaxHoles) * 8, st>>>(P);
-    k_fixup_copy<<<pl->num_sms * 2, 256, 0, st>>>(P);
+    k_fixup_prep<<<J, 1024, (size_t)(kHoleSortSlots + kMaxHoles) * 8, st>>>(P);
+    k_fixup_copy<<<dim3(pl->num_sms * 2, J), 256, 0, st>>>(P);
     mark(6);
     if (ev) {
         pl->ring_next = (pl->ring_next + 1) % spj_plan::kRing;
@@ -1177,9 +1364,6 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
     }
     return cudaGetLastError();
 }
-
-// Kernel launches of one execution (for launch accounting).
-int pipeline_launches(const spj_plan *pl) { return pl->jp.fine_bits ? 10 : 8; }
 
 cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm) {
     cudaError_t e;
@@ -1205,8 +1389,8 @@ cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm)
     e = cudaFuncSetAttribute(k_fixup_prep, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (kHoleSortSlots + kMaxHoles) * 8);
     if (e) return e;
-    const void *jk = alg == SPJ_ALG_SMJ ? (const void *)k_join_smj
-                     : alg == SPJ_ALG_NL  ? (const void *)k_join_nl
+    const void *jk = alg == SPJ_ALG_SMJ    ? (const void *)k_join_smj
+                     : alg == SPJ_ALG_NL   ? (const void *)k_join_nl
                      : alg == SPJ_ALG_NPHJ ? (const void *)k_nphj_probe
                                            : (const void *)k_join_phj;
     const size_t dyn = alg == SPJ_ALG_NPHJ ? 0 : (size_t)table_slots * 8;

@@ -1,6 +1,6 @@
-// spj_plan.cu -- host side of libspidjoin: the device-resident plan, the
-// JoinInstance-shaped handle of the C ABI, the synthetic-data generator and the
-// error reporting. No CPU join path exists: every join runs on the GPU.
+// spj_plan.cu -- host side of libspidjoin: plans (one join or a batch), their
+// device layout, the synthetic-data generator and the error reporting. No CPU
+// join path exists: every join runs on the GPU.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -15,8 +15,7 @@
 
 namespace spj {
 
-cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st);
-cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm);
+cudaError_t init_single(spj_plan *pl, cudaStream_t st);
 cudaError_t launch_checksum(const spj_kv_pair_t *pairs, const int64_t *n_dev, uint64_t *sum_dev, int sms,
                             cudaStream_t st);
 cudaError_t launch_generate(uint64_t seed, int64_t n_r, int64_t n_s, double zipf_s, spj_kv_pair_t *r,
@@ -36,9 +35,9 @@ int cuda_error(cudaError_t e, const char *what) {
                      std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define SPJ_CUDA(call)                                  \
-    do {                                                \
-        cudaError_t e_ = (call);                        \
+#define SPJ_CUDA(call)                                       \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
         if (e_ != cudaSuccess) return cuda_error(e_, #call); \
     } while (0)
 
@@ -71,6 +70,208 @@ static int device_sms(int *sms, int *dev_out) {
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+static int max_table_slots(int dev) {
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return ((max_smem - 4096) / 8) & ~1;
+}
+
+// Per-join tuning: the planner's choice for these sizes (size classes follow
+// from the formulas: fan-out from |R|, chunking from |R|+|S|).
+JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots) {
+    JoinShape sh;
+    int ts = d.table_slots > 0 ? std::min(d.table_slots, max_slots) : kDefaultTableSlots;
+    if (d.join_alg == SPJ_ALG_NPHJ) {
+        sh.bits = 0;
+        sh.fine_bits = 0;
+        sh.table_slots = 2;
+        unsigned long long slots = 1024;
+        while (slots < 2 * (unsigned long long)n_r) slots <<= 1;
+        sh.gtable_slots = slots;
+    } else {
+        if (d.radix_bits > 0) {
+            sh.bits = d.radix_bits;
+        } else {
+            // Mean R partition at a third of the table (short linear-probe runs), at
+            // least 8 partitions per SM for small joins, and at least 64 per rank.
+            const uint64_t target = std::max<uint64_t>(1, (uint64_t)ts / 3);
+            const int need = ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + target - 1) / target));
+            const int par = ceil_log2((uint64_t)8 * sms);
+            const int minb = ceil_log2((uint64_t)64 * d.rank_num);
+            sh.bits = std::min(std::max(std::max(need, par), minb), kMaxRadixBits);
+        }
+        if (d.table_slots <= 0) {
+            // shrink the table to three times a generous bound on the largest partition
+            const double mean = (double)n_r / (double)(1ull << sh.bits);
+            const double bound = mean + 6.0 * sqrt(mean) + 32.0;
+            const int want = (int)std::min<double>(max_slots, std::max(1024.0, 3.0 * bound));
+            ts = std::min(ts, (want + 255) / 256 * 256);
+            ts = std::max(ts, 1024);
+        }
+        sh.table_slots = ts & ~1;  // pairs of slots are probed together
+        sh.fine_bits = sh.bits > kMaxPassBits ? sh.bits - (sh.bits + 1) / 2 : 0;
+    }
+    // One chunk size for both relations so every pass-1 CTA does the same work;
+    // about one wave of 2 CTAs per SM.
+    int64_t c = std::max<int64_t>(4096, (n_r + n_s + 2 * sms - 3) / (2 * sms - 2));
+    c = (c + 1) & ~1ll;
+    const int64_t ns[2] = {n_r, n_s};
+    for (int r = 0; r < 2; r++) {
+        sh.nchunks[r] = (uint32_t)std::max<int64_t>(1, (ns[r] + c - 1) / c);
+        sh.chunk[r] = (uint32_t)c;
+    }
+    sh.item_target = (uint32_t)std::max<int64_t>(16384, (n_r + n_s) / (64 * sms));
+    // small joins reserve small output chunks, so a batch's output slack stays small
+    uint32_t oc = 32;
+    while (oc < (uint32_t)kOutChunk && (int64_t)oc * 8192 < n_s) oc <<= 1;
+    sh.out_chunk = oc;
+    return sh;
+}
+
+// Arena layout of a plan; with arena == nullptr only the size is computed.
+size_t layout_plan(spj_plan *pl, char *a, bool image) {
+    const uint32_t J = (uint32_t)pl->joins.size();
+    const spj_design_t &d = pl->design;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + std::max<size_t>(bytes, 1), 256);
+        return o;
+    };
+    const size_t o_ctr = take(sizeof(BatchCtr) + J * sizeof(JoinCtr));
+    const size_t o_rel = take(2 * J * sizeof(RelDev)), o_join = take(J * sizeof(JoinDev));
+    const size_t o_pref = take((3 * (2 * J + 1) + J + 1) * 4);
+    uint64_t max_units = 64, max_items = 1;
+    uint32_t tot_chunks = 0, tot_parts = 0, tot_coarse = 0, tot_jparts = 0;
+    int max_bits = 0, max_ts = 2, two = 0;
+    const uint32_t warps = (uint32_t)pl->join_blocks * (kJoinThreads / 32);
+    std::vector<uint32_t> chunk_pref(2 * J + 1), part_pref(2 * J + 1), coarse_pref(2 * J + 1), jpart_pref(J + 1);
+    for (uint32_t j = 0; j < J; j++) {
+        JoinHost &h = pl->joins[j];
+        const JoinShape &sh = pl->shapes[j];
+        const bool nphj = d.join_alg == SPJ_ALG_NPHJ;
+        const uint64_t F = nphj ? 1 : 1ull << sh.bits;
+        const uint64_t f1 = (!nphj && sh.fine_bits) ? 1ull << (sh.bits - sh.fine_bits) : 0;
+        JoinDev &jd = h.dev;
+        Tuple *const bound_out = jd.out;  // pointers bound by the caller survive a re-layout
+        unsigned long long *const bound_n = jd.n_out_user;
+        jd = JoinDev{};
+        jd.out = bound_out;
+        jd.n_out_user = bound_n;
+        jd.bits = sh.bits;
+        jd.fine_bits = nphj ? 0 : sh.fine_bits;
+        jd.table_slots = sh.table_slots;
+        jd.alg = d.join_alg;
+        jd.skew_mode = d.skew_mode;
+        jd.group = d.rank_set * d.bank_set;
+        jd.keep_unmatched = (d.join_alg == SPJ_ALG_SMJ || d.join_alg == SPJ_ALG_NL) ? 1 : 0;
+        jd.unit_tuples = d.unit_tuples > 0 ? (uint32_t)d.unit_tuples : (uint32_t)kDefaultUnitTuples;
+        jd.item_target = sh.item_target;
+        jd.out_chunk = sh.out_chunk;
+        jd.out_cap = (unsigned long long)h.n_s + (unsigned long long)warps * sh.out_chunk;
+        jd.gtable_slots = nphj ? sh.gtable_slots : 0;
+        const int64_t n[2] = {h.n_r, h.n_s};
+        for (int r = 0; r < 2; r++) {
+            RelDev &rd = h.rel[r];
+            const Tuple *const bound_in = rd.in;
+            rd = RelDev{};
+            rd.in = bound_in;
+            rd.n = (uint32_t)n[r];
+            rd.chunk = sh.chunk[r];
+            rd.nchunks = nphj ? 0 : sh.nchunks[r];
+            rd.join = j;
+            const size_t o_hist = take((size_t)rd.nchunks * F * 4);
+            const size_t o_chist = take((size_t)rd.nchunks * f1 * 4);
+            const size_t o_tot = take(F * 4), o_base = take(F * 4);
+            const size_t o_out = take(nphj ? 0 : (size_t)n[r] * 8 + 16);
+            const size_t o_tmp = take(f1 ? (size_t)n[r] * 8 + 16 : 0);
+            if (a) {
+                rd.hist = (uint32_t *)(a + o_hist);
+                rd.chist = f1 ? (uint32_t *)(a + o_chist) : nullptr;
+                rd.total = (uint32_t *)(a + o_tot);
+                rd.base = (uint32_t *)(a + o_base);
+                rd.out = nphj ? nullptr : (Tuple *)(a + o_out);
+                rd.tmp = f1 ? (Tuple *)(a + o_tmp) : nullptr;
+            }
+            chunk_pref[2 * j + r] = tot_chunks;
+            part_pref[2 * j + r] = tot_parts;
+            coarse_pref[2 * j + r] = tot_coarse;
+            tot_chunks += rd.nchunks;
+            tot_parts += nphj ? 0 : (uint32_t)F;
+            tot_coarse += (uint32_t)f1;
+        }
+        jpart_pref[j] = tot_jparts;
+        tot_jparts += nphj ? 1 : (uint32_t)F;
+        const size_t o_holes = take(kMaxHoles * sizeof(Hole)), o_gaps = take(kMaxHoles * sizeof(Hole));
+        const size_t o_datas = take(kMaxHoles * sizeof(Hole));
+        const size_t o_goff = take(kMaxHoles * 8), o_doff = take(kMaxHoles * 8);
+        const size_t o_gt = take(nphj ? jd.gtable_slots * 8 : 0);
+        if (a) {
+            jd.ctr = (JoinCtr *)(a + o_ctr + sizeof(BatchCtr)) + j;
+            jd.holes = (Hole *)(a + o_holes);
+            jd.gaps = (Hole *)(a + o_gaps);
+            jd.datas = (Hole *)(a + o_datas);
+            jd.gap_off = (unsigned long long *)(a + o_goff);
+            jd.data_off = (unsigned long long *)(a + o_doff);
+            jd.gtable = nphj ? (unsigned long long *)(a + o_gt) : nullptr;
+        }
+        max_units += nphj ? (uint64_t)h.n_s / jd.unit_tuples + 64
+                          : F * (uint64_t)std::max(jd.group, 1) + (uint64_t)h.n_s / jd.unit_tuples + F + 64;
+        if (f1) max_items += (uint64_t)(sh.nchunks[0] + sh.nchunks[1]) * f1 + 2 * f1;
+        max_bits = std::max(max_bits, nphj ? 0 : sh.bits);
+        max_ts = std::max(max_ts, sh.table_slots);
+        two |= f1 ? 1 : 0;
+    }
+    chunk_pref[2 * J] = tot_chunks;
+    part_pref[2 * J] = tot_parts;
+    coarse_pref[2 * J] = tot_coarse;
+    jpart_pref[J] = tot_jparts;
+    const size_t o_units = take(max_units * sizeof(Unit)), o_items = take(max_items * 16);
+    if (a) {
+        PlanDev &P = pl->dev;
+        P.rel = (RelDev *)(a + o_rel);
+        P.join = (JoinDev *)(a + o_join);
+        uint32_t *pref = (uint32_t *)(a + o_pref);
+        P.chunk_prefix = pref;
+        P.part_prefix = pref + (2 * J + 1);
+        P.coarse_prefix = pref + 2 * (2 * J + 1);
+        P.jpart_prefix = pref + 3 * (2 * J + 1);
+        P.nrel = 2 * J;
+        P.njoin = J;
+        P.total_chunks = tot_chunks;
+        P.total_parts = tot_parts;
+        P.total_coarse = tot_coarse;
+        P.total_jparts = tot_jparts;
+        P.max_bits = max_bits;
+        P.max_table_slots = max_ts;
+        P.alg = d.join_alg;
+        P.any_two_pass = two;
+        P.units = (Unit *)(a + o_units);
+        P.max_units = (uint32_t)std::min<uint64_t>(max_units, 0xFFFFFFFFull);
+        P.items = (uint4 *)(a + o_items);
+        P.max_items = (uint32_t)std::min<uint64_t>(max_items, 0xFFFFFFFFull);
+        P.bctr = (BatchCtr *)(a + o_ctr);
+        P.jctr = (JoinCtr *)(a + o_ctr + sizeof(BatchCtr));
+        pl->desc_offset = o_rel;
+    }
+    if (a && image) {  // host image of the descriptor region [o_rel, o_pref + prefixes)
+        const size_t dend = o_pref + (3 * (2 * J + 1) + J + 1) * 4;
+        pl->desc_host.assign(dend - o_rel, 0);
+        unsigned char *img = pl->desc_host.data();
+        for (uint32_t j = 0; j < J; j++) {
+            memcpy(img + (o_rel - o_rel) + (2 * j) * sizeof(RelDev), &pl->joins[j].rel[0], sizeof(RelDev));
+            memcpy(img + (2 * j + 1) * sizeof(RelDev), &pl->joins[j].rel[1], sizeof(RelDev));
+            memcpy(img + (o_join - o_rel) + j * sizeof(JoinDev), &pl->joins[j].dev, sizeof(JoinDev));
+        }
+        uint32_t *ip = (uint32_t *)(img + (o_pref - o_rel));
+        memcpy(ip, chunk_pref.data(), (2 * J + 1) * 4);
+        memcpy(ip + (2 * J + 1), part_pref.data(), (2 * J + 1) * 4);
+        memcpy(ip + 2 * (2 * J + 1), coarse_pref.data(), (2 * J + 1) * 4);
+        memcpy(ip + 3 * (2 * J + 1), jpart_pref.data(), (J + 1) * 4);
+    }
+    return off;
+}
+
 }  // namespace spj
 
 using namespace spj;
@@ -79,7 +280,7 @@ extern "C" {
 
 const char *spj_last_error(void) { return g_last_error.c_str(); }
 
-const char *spj_version(void) { return "spidjoin-b200 0.1 (sm_100a)"; }
+const char *spj_version(void) { return "spidjoin-b200 0.2 (sm_100a)"; }
 
 void spj_design_default(spj_design_t *d) {
     if (!d) return;
@@ -116,184 +317,120 @@ static int validate_design(const spj_design_t *d) {
     return SPJ_OK;
 }
 
-int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_plan_t **out) {
+// Creates a plan of J joins (shared by the plain and the batch entry points).
+static int create_plan(int J, const int64_t *n_r, const int64_t *n_s, const spj_design_t *design, spj_plan_t **out) {
     if (!out) return set_error(SPJ_E_ARG, "out is NULL");
     *out = nullptr;
     int rc = validate_design(design);
     if (rc) return rc;
-    if (n_r < 0 || n_s < 0 || n_r >= 0xFFFFFFFFll || n_s >= 0xFFFFFFFFll)
-        return set_error(SPJ_E_ARG, "relation sizes must be in [0, 2^32 - 1)");
+    if (J < 1 || J > 65535) return set_error(SPJ_E_ARG, "a batch holds 1 to 65535 joins");
+    for (int j = 0; j < J; j++)
+        if (n_r[j] < 0 || n_s[j] < 0 || n_r[j] >= 0xFFFFFFFFll || n_s[j] >= 0xFFFFFFFFll)
+            return set_error(SPJ_E_ARG, "relation sizes must be in [0, 2^32 - 1)");
     int sms = 0, dev = 0;
     if ((rc = device_sms(&sms, &dev))) return rc;
-
     spj_plan *pl = new spj_plan();
-    pl->n_r = n_r;
-    pl->n_s = n_s;
+    pl->n_r = n_r[0];
+    pl->n_s = n_s[0];
     pl->design = *design;
     pl->device = dev;
     pl->num_sms = sms;
-    JoinParams &jp = pl->jp;
-    const spj_design_t &d = *design;
-    int max_smem = 0;
-    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const int max_slots = (max_smem - 4096) / 8 & ~1;
-    int ts = d.table_slots > 0 ? std::min(d.table_slots, max_slots) : kDefaultTableSlots;
-    if (d.radix_bits > 0) {
-        jp.bits = d.radix_bits;
-    } else {
-        // Mean R partition at a third of the table (short linear-probe runs), at
-        // least 8 partitions per SM for small joins, and at least 64 per rank.
-        const uint64_t target = std::max<uint64_t>(1, (uint64_t)ts / 3);
-        const int need = ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + target - 1) / target));
-        const int par = ceil_log2((uint64_t)8 * sms);
-        const int minb = ceil_log2((uint64_t)64 * d.rank_num);
-        jp.bits = std::min(std::max(std::max(need, par), minb), kMaxRadixBits);
+    const int maxts = max_table_slots(dev);
+    pl->joins.resize(J);
+    pl->shapes.resize(J);
+    int ts_max = 2;
+    for (int j = 0; j < J; j++) {
+        pl->joins[j].n_r = n_r[j];
+        pl->joins[j].n_s = n_s[j];
+        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts);
+        ts_max = std::max(ts_max, pl->shapes[j].table_slots);
     }
-    if (d.table_slots <= 0) {
-        // shrink the table to three times a generous bound on the largest partition
-        const double mean = (double)n_r / (double)(1ull << jp.bits);
-        const double bound = mean + 6.0 * sqrt(mean) + 32.0;
-        const int want = (int)std::min<double>(max_slots, std::max(1024.0, 3.0 * bound));
-        ts = std::min(ts, (want + 255) / 256 * 256);
-        ts = std::max(ts, 1024);
-    }
-    jp.table_slots = ts & ~1;  // pairs of slots are probed together
-    jp.fine_bits = jp.bits > kMaxPassBits ? jp.bits - (jp.bits + 1) / 2 : 0;
-    jp.alg = d.join_alg;
-    jp.skew_mode = d.skew_mode;
-    jp.group = d.rank_set * d.bank_set;
-    jp.unit_tuples = d.unit_tuples > 0 ? (uint32_t)d.unit_tuples : (uint32_t)kDefaultUnitTuples;
-    jp.keep_unmatched = (d.join_alg == SPJ_ALG_SMJ || d.join_alg == SPJ_ALG_NL) ? 1 : 0;
-
     int per_sm = 0;
-    cudaError_t ce = configure_kernels(jp.table_slots, jp.alg, &per_sm);
+    cudaError_t ce = configure_kernels(ts_max, design->join_alg, &per_sm);
     if (ce != cudaSuccess || per_sm < 1) {
         delete pl;
         return ce != cudaSuccess ? cuda_error(ce, "configure kernels")
                                  : set_error(SPJ_E_ARG, "table_slots too large for one CTA");
     }
     pl->join_blocks = std::min(per_sm * sms, kMaxHoles / (kJoinThreads / 32));
-
-    const uint64_t F = 1ull << jp.bits;
-    const int64_t ns[2] = {n_r, n_s};
-    // One chunk size for both relations so every pass-1 CTA does the same work;
-    // about one wave of 3 CTAs per SM.
-    uint32_t nch[2], chunk[2];
-    {
-        const int64_t total = n_r + n_s;
-        int64_t c = std::max<int64_t>(4096, (total + 2 * sms - 3) / (2 * sms - 2));
-        c = (c + 1) & ~1ll;
-        for (int r = 0; r < 2; r++) {
-            nch[r] = (uint32_t)std::max<int64_t>(1, (ns[r] + c - 1) / c);
-            chunk[r] = (uint32_t)c;
-        }
-    }
-    // pass-2 work items of ~1/32 of a CTA's share of the tuples
-    const uint64_t f1 = 1ull << (jp.bits - jp.fine_bits);
-    pl->item_target = (uint32_t)std::max<int64_t>(16384, (n_r + n_s) / (64 * sms));
-    const uint64_t max_items = jp.fine_bits ? (uint64_t)(nch[0] + nch[1]) * f1 + 2 * f1 : 1;
-    const uint64_t max_units = F * (uint64_t)std::max(jp.group, 1) + (uint64_t)n_s / jp.unit_tuples + F + 64;
-    const uint64_t out_cap = (uint64_t)n_s + (uint64_t)pl->join_blocks * (kJoinThreads / 32) * kOutChunk;
-
-    // one arena for all scratch
-    size_t off = 0;
-    auto take = [&](size_t bytes) {
-        size_t o = off;
-        off = align_up(off + std::max<size_t>(bytes, 1), 256);
-        return o;
-    };
-    const size_t o_ctr = take(sizeof(Counters));
-    const size_t o_hist0 = take((size_t)nch[0] * F * 4), o_hist1 = take((size_t)nch[1] * F * 4);
-    const size_t o_ch0 = take((size_t)nch[0] * f1 * 4), o_ch1 = take((size_t)nch[1] * f1 * 4);
-    const size_t o_items = take(max_items * 16);
-    const size_t o_tot0 = take(F * 4), o_tot1 = take(F * 4), o_base0 = take(F * 4), o_base1 = take(F * 4);
-    const bool nphj = jp.alg == SPJ_ALG_NPHJ;
-    const size_t o_pr = take(nphj ? 0 : (size_t)n_r * 8 + 16), o_ps = take(nphj ? 0 : (size_t)n_s * 8 + 16);
-    if (nphj) {
-        uint64_t slots = 1024;
-        while (slots < 2 * (uint64_t)n_r) slots <<= 1;
-        pl->gtable_slots = slots;
-    }
-    const size_t o_gt = take(nphj ? pl->gtable_slots * 8 : 0);
-    const bool two = !nphj && jp.fine_bits > 0;
-    const size_t o_tr = two ? take((size_t)n_r * 8 + 16) : 0, o_ts = two ? take((size_t)n_s * 8 + 16) : 0;
-    const size_t o_units = take(max_units * sizeof(Unit));
-    const size_t o_holes = take(kMaxHoles * sizeof(Hole));
-    const size_t o_gaps = take(kMaxHoles * sizeof(Hole)), o_datas = take(kMaxHoles * sizeof(Hole));
-    const size_t o_goff = take(kMaxHoles * 8), o_doff = take(kMaxHoles * 8);
-    ce = cudaMalloc(&pl->arena, off);
+    const size_t bytes = layout_plan(pl, nullptr, false);
+    ce = cudaMalloc(&pl->arena, bytes);
     if (ce != cudaSuccess) {
         delete pl;
         return cuda_error(ce, "cudaMalloc(plan scratch)");
     }
-    pl->arena_bytes = off;
-    char *a = (char *)pl->arena;
-    PlanDev &P = pl->dev;
-    P.ctr = (Counters *)(a + o_ctr);
-    for (int r = 0; r < 2; r++) {
-        P.rel[r].in = nullptr;
-        P.rel[r].n = (uint32_t)ns[r];
-        P.rel[r].chunk = chunk[r];
-        P.rel[r].nchunks = nch[r];
+    pl->arena_bytes = bytes;
+    layout_plan(pl, (char *)pl->arena, true);
+    // descriptor arrays: uploaded once (a batch's pointers are bound later)
+    ce = cudaMemcpy((char *)pl->arena + pl->desc_offset, pl->desc_host.data(), pl->desc_host.size(),
+                    cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) {
+        cudaFree(pl->arena);
+        delete pl;
+        return cuda_error(ce, "descriptor upload");
     }
-    P.rel[0].hist = (uint32_t *)(a + o_hist0);
-    P.rel[1].hist = (uint32_t *)(a + o_hist1);
-    P.rel[0].chist = (uint32_t *)(a + o_ch0);
-    P.rel[1].chist = (uint32_t *)(a + o_ch1);
-    P.items = (uint4 *)(a + o_items);
-    P.max_items = (uint32_t)std::min<uint64_t>(max_items, 0xFFFFFFFFull);
-    P.rel[0].total = (uint32_t *)(a + o_tot0);
-    P.rel[1].total = (uint32_t *)(a + o_tot1);
-    P.rel[0].base = (uint32_t *)(a + o_base0);
-    P.rel[1].base = (uint32_t *)(a + o_base1);
-    P.rel[0].out = (Tuple *)(a + o_pr);
-    P.rel[1].out = (Tuple *)(a + o_ps);
-    P.rel[0].tmp = two ? (Tuple *)(a + o_tr) : nullptr;
-    P.rel[1].tmp = two ? (Tuple *)(a + o_ts) : nullptr;
-    P.units = (Unit *)(a + o_units);
-    P.max_units = (uint32_t)std::min<uint64_t>(max_units, 0xFFFFFFFFull);
-    P.holes = (Hole *)(a + o_holes);
-    P.gaps = (Hole *)(a + o_gaps);
-    P.datas = (Hole *)(a + o_datas);
-    P.gap_off = (unsigned long long *)(a + o_goff);
-    P.data_off = (unsigned long long *)(a + o_doff);
-    P.out = nullptr;
-    P.out_cap = out_cap;
-    P.gtable = nphj ? (unsigned long long *)(a + o_gt) : nullptr;
-    P.n_out_user = nullptr;
     pl->have_events = true;
     for (int i = 0; i < spj_plan::kRing && pl->have_events; i++)
-        for (int j = 0; j < spj_plan::kMarks; j++)
-            if (cudaEventCreate(&pl->ring[i][j]) != cudaSuccess) pl->have_events = false;
+        for (int k = 0; k < spj_plan::kMarks; k++)
+            if (cudaEventCreate(&pl->ring[i][k]) != cudaSuccess) pl->have_events = false;
     *out = pl;
     return SPJ_OK;
 }
 
-int64_t spj_plan_output_capacity(const spj_plan_t *plan) { return plan ? (int64_t)plan->dev.out_cap : 0; }
+int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_plan_t **out) {
+    return create_plan(1, &n_r, &n_s, design, out);
+}
+
+int64_t spj_plan_output_capacity(const spj_plan_t *plan) {
+    return plan ? (int64_t)plan->joins[0].dev.out_cap : 0;
+}
 
 int spj_plan_execute(spj_plan_t *pl, const spj_kv_pair_t *r, const spj_kv_pair_t *s, spj_kv_pair_t *out,
                      int64_t *n_out, void *stream) {
     if (!pl) return set_error(SPJ_E_ARG, "plan is NULL");
+    if (pl->joins.size() != 1) return set_error(SPJ_E_ARG, "a batch plan runs with spj_batch_execute");
     if ((pl->n_r && !r) || (pl->n_s && !s) || !out) return set_error(SPJ_E_ARG, "NULL column or output");
     if (((uintptr_t)r & 15) || ((uintptr_t)s & 15) || ((uintptr_t)out & 7))
         return set_error(SPJ_E_ARG, "columns must be 16-byte aligned and the output 8-byte aligned");
     cudaStream_t st = (cudaStream_t)stream;
-    PlanDev &P = pl->dev;
-    P.rel[0].in = reinterpret_cast<const Tuple *>(r);
-    P.rel[1].in = reinterpret_cast<const Tuple *>(s);
-    P.out = reinterpret_cast<Tuple *>(out);
-    P.n_out_user = reinterpret_cast<unsigned long long *>(n_out);
-    SPJ_CUDA(cudaMemsetAsync(P.ctr, 0, sizeof(Counters), st));
-    cudaError_t e = launch_pipeline(pl, st);
+    JoinHost &h = pl->joins[0];
+    // an empty relation still needs a readable, aligned column pointer
+    h.rel[0].in = r ? reinterpret_cast<const Tuple *>(r) : reinterpret_cast<const Tuple *>(out);
+    h.rel[1].in = s ? reinterpret_cast<const Tuple *>(s) : reinterpret_cast<const Tuple *>(out);
+    h.dev.out = reinterpret_cast<Tuple *>(out);
+    h.dev.n_out_user = reinterpret_cast<unsigned long long *>(n_out);
+    cudaError_t e = init_single(pl, st);
+    if (e != cudaSuccess) return cuda_error(e, "descriptor kernel");
+    SPJ_CUDA(cudaMemsetAsync(pl->dev.bctr, 0, sizeof(BatchCtr) + sizeof(JoinCtr), st));
+    e = launch_pipeline(pl, st);
     if (e != cudaSuccess) return cuda_error(e, "join kernels");
+    return SPJ_OK;
+}
+
+static void fill_stats(const spj_plan *pl, const JoinCtr &c, spj_stats_t *out) {
+    out->n_pairs = (int64_t)c.n_out;
+    out->units = c.units;
+    out->max_r_partition = c.max_r_part;
+    out->max_s_partition = c.max_s_part;
+    out->radix_bits = pl->shapes[0].bits;
+    out->table_slots = pl->shapes[0].table_slots;
+}
+
+static int ctr_error(const spj_plan *pl, unsigned err, unsigned max_r) {
+    if (err & 32u) return set_error(SPJ_E_TIMEOUT, "a bulk copy did not complete in time");
+    if (err & 1u)
+        return set_error(SPJ_E_OVERFLOW, "an R partition (" + std::to_string(max_r) +
+                                              " tuples) did not fit the shared-memory structure of its CTA");
+    if (err) return set_error(SPJ_E_OVERFLOW, "internal capacity exceeded (flags " + std::to_string(err) + ")");
+    (void)pl;
     return SPJ_OK;
 }
 
 int spj_plan_stats(spj_plan_t *pl, spj_stats_t *out) {
     if (!pl || !out) return set_error(SPJ_E_ARG, "NULL argument");
     memset(out, 0, sizeof(*out));
-    Counters c;
-    SPJ_CUDA(cudaMemcpy(&c, pl->dev.ctr, sizeof(c), cudaMemcpyDeviceToHost));
+    JoinCtr c;
+    SPJ_CUDA(cudaMemcpy(&c, pl->dev.jctr, sizeof(c), cudaMemcpyDeviceToHost));
     spj_kernel_times_t kt;
     if (pl->have_events && pl->ring_filled > 0 && spj_plan_kernel_times(pl, 0, &kt) == SPJ_OK) {
         out->partition_ms = kt.hist_ms + kt.scan_ms + kt.scatter_ms;
@@ -301,22 +438,8 @@ int spj_plan_stats(spj_plan_t *pl, spj_stats_t *out) {
         out->finish_ms = kt.fixup_ms;
         out->total_ms = kt.total_ms;
     }
-    out->n_pairs = (int64_t)c.n_out;
-    out->units = c.unit_count;
-    out->heavy_keys = c.heavy_keys;
-    out->heavy_tuples = (int64_t)c.heavy_tuples;
-    out->max_r_partition = c.max_r_part;
-    out->max_s_partition = c.max_s_part;
-    out->radix_bits = pl->jp.bits;
-    out->table_slots = pl->jp.table_slots;
-    if (c.error & 32u) return set_error(SPJ_E_TIMEOUT, "a bulk copy did not complete in time");
-    if (c.error & 1u)
-        return set_error(SPJ_E_OVERFLOW, "an R partition (" + std::to_string(c.max_r_part) +
-                                              " tuples) did not fit the shared-memory table of " +
-                                              std::to_string(pl->jp.table_slots) + " slots");
-    if (c.error)
-        return set_error(SPJ_E_OVERFLOW, "internal capacity exceeded (flags " + std::to_string(c.error) + ")");
-    return SPJ_OK;
+    fill_stats(pl, c, out);
+    return ctr_error(pl, c.error, c.max_r_part);
 }
 
 int spj_plan_kernel_times(spj_plan_t *pl, int back, spj_kernel_times_t *out) {
@@ -349,6 +472,59 @@ void spj_plan_destroy(spj_plan_t *pl) {
                 if (e) cudaEventDestroy(e);
     cudaFree(pl->arena);
     delete pl;
+}
+
+// ------------------------------------------------------------------ batches --
+
+int spj_batch_create(int n_joins, const int64_t *n_r, const int64_t *n_s, const spj_design_t *design,
+                     spj_plan_t **out) {
+    if (!n_r || !n_s) return set_error(SPJ_E_ARG, "NULL size arrays");
+    return create_plan(n_joins, n_r, n_s, design, out);
+}
+
+int64_t spj_batch_output_capacity(const spj_plan_t *plan, int j) {
+    if (!plan || j < 0 || j >= (int)plan->joins.size()) return 0;
+    return (int64_t)plan->joins[j].dev.out_cap;
+}
+
+int spj_batch_bind(spj_plan_t *pl, const spj_kv_pair_t *const *r, const spj_kv_pair_t *const *s,
+                   spj_kv_pair_t *const *out, int64_t *n_out) {
+    if (!pl || !r || !s || !out) return set_error(SPJ_E_ARG, "NULL pointer array");
+    const size_t J = pl->joins.size();
+    for (size_t j = 0; j < J; j++) {
+        JoinHost &h = pl->joins[j];
+        if ((h.n_r && !r[j]) || (h.n_s && !s[j]) || !out[j]) return set_error(SPJ_E_ARG, "NULL column or output");
+        if (((uintptr_t)r[j] & 15) || ((uintptr_t)s[j] & 15) || ((uintptr_t)out[j] & 7))
+            return set_error(SPJ_E_ARG, "columns must be 16-byte aligned and outputs 8-byte aligned");
+        h.rel[0].in = reinterpret_cast<const Tuple *>(r[j] ? r[j] : out[j]);
+        h.rel[1].in = reinterpret_cast<const Tuple *>(s[j] ? s[j] : out[j]);
+        h.dev.out = reinterpret_cast<Tuple *>(out[j]);
+        h.dev.n_out_user = n_out ? reinterpret_cast<unsigned long long *>(n_out + j) : nullptr;
+    }
+    layout_plan(pl, (char *)pl->arena, true);  // refreshes the host image with the bound pointers
+    SPJ_CUDA(cudaMemcpy((char *)pl->arena + pl->desc_offset, pl->desc_host.data(), pl->desc_host.size(),
+                        cudaMemcpyHostToDevice));
+    return SPJ_OK;
+}
+
+int spj_batch_execute(spj_plan_t *pl, void *stream) {
+    if (!pl) return set_error(SPJ_E_ARG, "plan is NULL");
+    cudaStream_t st = (cudaStream_t)stream;
+    SPJ_CUDA(cudaMemsetAsync(pl->dev.bctr, 0, sizeof(BatchCtr) + pl->joins.size() * sizeof(JoinCtr), st));
+    cudaError_t e = launch_pipeline(pl, st);
+    if (e != cudaSuccess) return cuda_error(e, "join kernels");
+    return SPJ_OK;
+}
+
+int spj_batch_stats(spj_plan_t *pl, int j, spj_stats_t *out) {
+    if (!pl || !out || j < 0 || j >= (int)pl->joins.size()) return set_error(SPJ_E_ARG, "bad argument");
+    memset(out, 0, sizeof(*out));
+    JoinCtr c;
+    SPJ_CUDA(cudaMemcpy(&c, pl->dev.jctr + j, sizeof(c), cudaMemcpyDeviceToHost));
+    fill_stats(pl, c, out);
+    out->radix_bits = pl->shapes[j].bits;
+    out->table_slots = pl->shapes[j].table_slots;
+    return ctr_error(pl, c.error, c.max_r_part);
 }
 
 int spj_partition_histogram(const spj_kv_pair_t *tuples, int64_t n, int bits, uint32_t *hist, void *stream) {

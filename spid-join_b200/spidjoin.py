@@ -31,6 +31,7 @@ EXPORTS = (
     "spj_start", "spj_finish", "spj_record_logs", "spj_destroy", "spj_plan_create", "spj_plan_output_capacity",
     "spj_plan_execute", "spj_plan_stats", "spj_plan_destroy", "spj_partition_histogram", "spj_checksum_device",
     "spj_generate_host", "spj_generate_device", "spj_plan_kernel_times", "spj_join_noalloc",
+    "spj_batch_create", "spj_batch_output_capacity", "spj_batch_bind", "spj_batch_execute", "spj_batch_stats",
 )
 
 
@@ -110,6 +111,12 @@ def lib():
                                         ctypes.POINTER(ctypes.c_uint64), i32]
         L.spj_generate_device.argtypes = [ctypes.c_uint64, i64, i64, ctypes.c_double, vp, vp, vp, vp]
         L.spj_join_noalloc.argtypes = [vp, i64, vp, i64, vp, i64, vp, vp]
+        L.spj_batch_create.argtypes = [i32, vp, vp, ctypes.POINTER(Design), ctypes.POINTER(vp)]
+        L.spj_batch_output_capacity.argtypes = [vp, i32]
+        L.spj_batch_output_capacity.restype = i64
+        L.spj_batch_bind.argtypes = [vp, vp, vp, vp, vp]
+        L.spj_batch_execute.argtypes = [vp, vp]
+        L.spj_batch_stats.argtypes = [vp, i32, ctypes.POINTER(Stats)]
         _lib = L
     return _lib
 
@@ -248,6 +255,46 @@ class Plan:
         kt = KernelTimes()
         check(lib().spj_plan_kernel_times(self._p, back, ctypes.byref(kt)))
         return kt.as_dict()
+
+    def close(self):
+        if self._p:
+            lib().spj_plan_destroy(self._p)
+            self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many joins in one launch sequence (spj_batch_*): create with the sizes,
+    bind device pointers once, execute many times (graph-capturable)."""
+
+    def __init__(self, n_r, n_s, design=None):
+        self.J = len(n_r)
+        design = design if design is not None else make_design()
+        self._nr = (ctypes.c_int64 * self.J)(*[int(x) for x in n_r])
+        self._ns = (ctypes.c_int64 * self.J)(*[int(x) for x in n_s])
+        self._p = ctypes.c_void_p()
+        check(lib().spj_batch_create(self.J, self._nr, self._ns, ctypes.byref(design), ctypes.byref(self._p)))
+
+    def output_capacity(self, j):
+        return lib().spj_batch_output_capacity(self._p, j)
+
+    def bind(self, r_ptrs, s_ptrs, out_ptrs, n_out_ptr=None):
+        arr = lambda xs: (ctypes.c_void_p * self.J)(*[int(x) for x in xs])
+        self._bound = (arr(r_ptrs), arr(s_ptrs), arr(out_ptrs))
+        check(lib().spj_batch_bind(self._p, self._bound[0], self._bound[1], self._bound[2], n_out_ptr))
+
+    def execute(self, stream=0):
+        check(lib().spj_batch_execute(self._p, stream))
+
+    def stats(self, j):
+        st = Stats()
+        check(lib().spj_batch_stats(self._p, j, ctypes.byref(st)))
+        return st.as_dict()
 
     def close(self):
         if self._p:
