@@ -388,6 +388,8 @@ def run_batched(args):
     clocks = sampler.stop()
     ms_batched = ev0.elapsed_time(ev1) / args.steps
     del graph
+    batch.execute(0)  # one eager run for the per-kernel split
+    kmean = batch.kernel_times(0)
     batch.close()
 
     # plain: one plan per join, its device time per execution, summed over joins
@@ -425,7 +427,7 @@ def run_batched(args):
         "batched_vs_plain": plain_ms / ms_batched,
         "pipeline_roofline": {"achieved": pipe_bytes / (ms_batched / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                               "frac": pipe_bytes / (ms_batched / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
-        "gpu_launches": 14 * args.steps, "clocks": clocks,
+        "gpu_launches": 14 * args.steps, "clocks": clocks, "kernels_ms_eager": kmean,
         "check": {"joins_checked": J, "all_exact": True},
     })
     return 0

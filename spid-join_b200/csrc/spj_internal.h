@@ -167,7 +167,7 @@ namespace spj {
 int set_error(int code, const std::string &msg);
 int cuda_error(cudaError_t e, const char *what);
 
-JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots);
+JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots, bool alone);
 // Computes the arena layout of pl->joins/pl->shapes (arena == nullptr: size only)
 // and fills pl->dev, the per-join descriptors and the host image of the
 // descriptor arrays.

@@ -315,10 +315,25 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
             }
         }
         __syncthreads();
+        // write phase, unrolled so all shared loads are in flight before the stores
         const uint32_t valid = S.valid;
-        for (uint32_t j = threadIdx.x; j < valid; j += kScatterThreads) {
-            const Tuple x = S.stage[j];
-            o2[S.wpos[S.bkt[j]] + j] = make_uint2(x.key, x.pay);
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t j = threadIdx.x + k * kScatterThreads;
+            if (j < valid) {
+                v[k] = S.stage[j];
+                br[k] = S.bkt[j];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t j = threadIdx.x + k * kScatterThreads;
+            if (j < valid) br[k] = S.wpos[br[k]] + j;
+        }
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t j = threadIdx.x + k * kScatterThreads;
+            if (j < valid) o2[br[k]] = make_uint2(v[k].key, v[k].pay);
         }
         // the next tile's rank phase may start: counts are zero, and its first
         // barrier orders these reads of stage/wpos before they are rewritten
@@ -1209,19 +1224,10 @@ __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
     }
 }
 
-__device__ __forceinline__ unsigned upper_bound_u64(const unsigned long long *a, unsigned n,
-                                                    unsigned long long x) {
-    unsigned lo = 0, hi = n;
-    while (lo < hi) {
-        const unsigned mid = (lo + hi) >> 1;
-        if (a[mid] <= x)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    return lo;
-}
-
+// One warp per gap (a hole below N): the gap's slots x in [gap_off, gap_off+len)
+// of the "x-space" are filled from the pairs stored above N, in order; between
+// consecutive upper holes the source is N + x + (length of the upper holes
+// before it), so the warp finds its first data segment once and copies runs.
 __global__ void k_fixup_copy(PlanDev P) {
     const JoinDev &J = P.join[blockIdx.y];
     JoinCtr *ctr = J.ctr;
@@ -1230,27 +1236,37 @@ __global__ void k_fixup_copy(PlanDev P) {
     const unsigned long long N = ctr->n_out;
     const unsigned ng = ctr->n_gaps, nd = ctr->n_data;
     uint2 *out = reinterpret_cast<uint2 *>(J.out);
-    for (unsigned long long x = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; x < G;
-         x += (unsigned long long)gridDim.x * blockDim.x) {
-        // destination: x-th slot of the holes below N
-        const unsigned gi = upper_bound_u64(J.gap_off, ng, x) - 1;
-        const unsigned long long dst = J.gaps[gi].begin + (x - J.gap_off[gi]);
-        // source: x-th stored pair at or above N (holes skipped)
+    const int lane = threadIdx.x & 31;
+    const unsigned wpb = blockDim.x >> 5;
+    for (unsigned gi = blockIdx.x * wpb + (threadIdx.x >> 5); gi < ng; gi += gridDim.x * wpb) {
+        const unsigned long long x0 = J.gap_off[gi];
+        const unsigned long long x1 = gi + 1 < ng ? J.gap_off[gi + 1] : G;
+        const unsigned long long d0 = J.gaps[gi].begin;
+        // k = number of upper holes whose data prefix is <= x0
         unsigned lo = 0, hi = nd;
         while (lo < hi) {
             const unsigned mid = (lo + hi) >> 1;
-            if (J.datas[mid].begin <= x)
+            if (J.datas[mid].begin <= x0)
                 lo = mid + 1;
             else
                 hi = mid;
         }
-        const unsigned long long shift = lo > 0 ? J.data_off[lo - 1] : 0ull;
-        const unsigned long long src = N + x + shift;
-        if (src >= J.out_cap || dst >= N) {
-            atomicOr(&ctr->error, 16u);
-            continue;
+        unsigned k = lo;
+        unsigned long long x = x0;
+        while (x < x1) {
+            const unsigned long long shift = k > 0 ? J.data_off[k - 1] : 0ull;
+            const unsigned long long brk = k < nd ? J.datas[k].begin : x1;
+            const unsigned long long run_end = brk < x1 ? brk : x1;
+            for (unsigned long long y = x + lane; y < run_end; y += 32) {
+                const unsigned long long src = N + y + shift, dst = d0 + (y - x0);
+                if (src >= J.out_cap || dst >= N)
+                    atomicOr(&ctr->error, 16u);
+                else
+                    out[dst] = out[src];
+            }
+            x = run_end;
+            k++;
         }
-        out[dst] = out[src];
     }
 }
 
@@ -1356,7 +1372,7 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
     }
     mark(5);
     k_fixup_prep<<<J, 1024, (size_t)(kHoleSortSlots + kMaxHoles) * 8, st>>>(P);
-    k_fixup_copy<<<dim3(pl->num_sms * 2, J), 256, 0, st>>>(P);
+    k_fixup_copy<<<dim3((kMaxHoles + 7) / 8, J), 256, 0, st>>>(P);
     mark(6);
     if (ev) {
         pl->ring_next = (pl->ring_next + 1) % spj_plan::kRing;

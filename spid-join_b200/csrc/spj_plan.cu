@@ -78,7 +78,7 @@ static int max_table_slots(int dev) {
 
 // Per-join tuning: the planner's choice for these sizes (size classes follow
 // from the formulas: fan-out from |R|, chunking from |R|+|S|).
-JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots) {
+JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots, bool alone) {
     JoinShape sh;
     int ts = d.table_slots > 0 ? std::min(d.table_slots, max_slots) : kDefaultTableSlots;
     if (d.join_alg == SPJ_ALG_NPHJ) {
@@ -93,10 +93,12 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
             sh.bits = d.radix_bits;
         } else {
             // Mean R partition at a third of the table (short linear-probe runs), at
-            // least 8 partitions per SM for small joins, and at least 64 per rank.
+            // least 64 partitions per rank, and -- for a join that runs alone --
+            // at least 8 partitions per SM so that a small join still fills the GPU
+            // (in a batch the other joins do).
             const uint64_t target = std::max<uint64_t>(1, (uint64_t)ts / 3);
             const int need = ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + target - 1) / target));
-            const int par = ceil_log2((uint64_t)8 * sms);
+            const int par = alone ? ceil_log2((uint64_t)8 * sms) : 0;
             const int minb = ceil_log2((uint64_t)64 * d.rank_num);
             sh.bits = std::min(std::max(std::max(need, par), minb), kMaxRadixBits);
         }
@@ -342,7 +344,7 @@ static int create_plan(int J, const int64_t *n_r, const int64_t *n_s, const spj_
     for (int j = 0; j < J; j++) {
         pl->joins[j].n_r = n_r[j];
         pl->joins[j].n_s = n_s[j];
-        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts);
+        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1);
         ts_max = std::max(ts_max, pl->shapes[j].table_slots);
     }
     int per_sm = 0;

@@ -296,6 +296,11 @@ class Batch:
         check(lib().spj_batch_stats(self._p, j, ctypes.byref(st)))
         return st.as_dict()
 
+    def kernel_times(self, back=0):
+        kt = KernelTimes()
+        check(lib().spj_plan_kernel_times(self._p, back, ctypes.byref(kt)))
+        return kt.as_dict()
+
     def close(self):
         if self._p:
             lib().spj_plan_destroy(self._p)
