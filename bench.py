@@ -82,17 +82,57 @@ def cpu_reference_run(wl, steps, warmup):
     return rates, sample, cores
 
 
+def cpu_reference_specs(specs, steps, warmup, budget_tuples=24 << 20):
+    """The reference pipeline restated in C on all host cores over a mix of
+    joins: each step joins the first joins of `specs` whose sizes add up to
+    about `budget_tuples` (every join in full), and the rate is their tuples
+    over the summed time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import spidjoin
+    take, tot = [], 0
+    for n_r, n_s, z in specs:
+        if tot + n_r + n_s > budget_tuples and take:
+            continue
+        take.append((n_r, n_s, z))
+        tot += n_r + n_s
+    data = [spidjoin.generate_host(n_r, n_s, z, seed=SEED + 77 + i) for i, (n_r, n_s, z) in enumerate(take)]
+    cores = os.cpu_count() or 1
+    rates = []
+    for it in range(warmup + steps):
+        el = 0.0
+        for (n_r, n_s, _), (R, S, expect) in zip(take, data):
+            t0 = time.perf_counter()
+            out = oracle.refpipe_join(R, S, ranks=1, rank_sets=1, bank_set=1, alg=0, nthreads=cores)
+            el += time.perf_counter() - t0
+            if it == 0:
+                assert out.shape[0] == n_s and oracle.checksum(out) == expect, "CPU restatement disagrees"
+        if it >= warmup:
+            rates.append(tot / el)
+    sample = (f"{len(take)} joins of the mix ({tot} tuples, each join in full), reference pipeline restated "
+              f"in C, {cores} threads")
+    return rates, sample, cores, tot
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    rates, sample, cores = cpu_reference_run(args.workload, args.steps, args.warmup)
+    if args.workload in ("c4", "c5"):
+        specs = c4_specs(scale=args.c4_scale) if args.workload == "c4" else c5_specs(args.c5_pool)
+        rates, sample, cores, tot = cpu_reference_specs(specs, args.steps, args.warmup)
+        desc = ("batched joins, |R| log-uniform [2^12, 2^24], R:S in {1,2,4,8}, Zipf s ~ U[0, 1.5]"
+                if args.workload == "c4" else
+                "served join stream, |R| log-uniform [2^10, 2^22], R:S in {1,2,4,8}, Zipf s ~ U[0, 1.5]")
+    else:
+        rates, sample, cores = cpu_reference_run(args.workload, args.steps, args.warmup)
+        n_r, n_s = WORKLOADS[args.workload][:2]
+        tot, desc = n_r + n_s, WORKLOADS[args.workload][4]
     v = statistics.median(rates)
-    n_r, n_s = WORKLOADS[args.workload][:2]
     emit({"impl": "reference", "metric": METRIC, "value": v, "unit": "tuples/s", "n_gpus": args.gpus,
-          "steps": args.steps, "warmup": args.warmup, "ms_per_step": (n_r + n_s) / v * 1e3,
+          "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / v * 1e3,
           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-          "config": {"workload": WORKLOADS[args.workload][4], "sample": sample},
+          "config": {"workload": desc, "sample": sample},
           "cpu_baseline": {"value": v, "unit": "tuples/s", "cores": cores, "kind": "port", "sample": sample},
           "e2e": {"value": v, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     return 0
@@ -433,12 +473,193 @@ def run_batched(args):
     return 0
 
 
+# ------------------------------------------------------------ served (c5) --
+def c5_specs(n_joins, seed=SEED + 5):
+    """Config 5's join mix: |R| log-uniform in [2^10, 2^22], R:S ratio from
+    {1,2,4,8}, Zipf s uniform in [0, 1.5] (numpy's PCG64)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(n_joins):
+        n_r = int(2.0 ** rng.uniform(10.0, 22.0))
+        ratio = int(rng.choice([1, 2, 4, 8]))
+        specs.append((n_r, n_r * ratio, float(rng.uniform(0.0, 1.5))))
+    return specs
+
+
+def serve_stream(spj, server, pool, R, S, outs, n_out, rate, seconds, max_outstanding, seed):
+    """Drives `server` with joins drawn round-robin from the pool: Poisson
+    arrivals at `rate` joins/s for `seconds` (rate = 0: closed loop with
+    `max_outstanding` requests in flight). A side-stream checksum and count of
+    every output are kept on the device for checking after the run. Returns a
+    dict of measurements."""
+    import threading
+    import numpy as np
+    import torch
+    P = len(pool)
+    lib = spj.lib()
+    rng = np.random.default_rng(seed)
+    cap_req = int((rate * 1.5 if rate > 0 else 50000) * seconds) + 16
+    sums = torch.zeros(cap_req, dtype=torch.int64, device="cuda")
+    counts = torch.full((cap_req,), -1, dtype=torch.int64, device="cuda")
+    side = torch.cuda.Stream()
+    free = [threading.Semaphore(1) for _ in range(P)]  # pool entry p: its output is not in use
+    checked = [torch.cuda.Event() for _ in range(P)]  # the side-stream check of entry p's last output
+    outstanding = threading.Semaphore(max_outstanding)
+    queue, qcv = [], threading.Condition(threading.Lock())
+    done_flag = [False]
+    lat, entries, late = [], [], []
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=cap_req)) if rate > 0 else None
+
+    def waiter():
+        k = 0
+        while True:
+            with qcv:
+                while k >= len(queue) and not done_flag[0]:
+                    qcv.wait(0.05)
+                if k >= len(queue):
+                    return
+                rid, p = queue[k]
+            lat.append(server.wait(rid, -1.0))
+            with torch.cuda.stream(side):
+                counts[k:k + 1].copy_(n_out[p:p + 1])
+                spj.check(lib.spj_checksum_device(outs[p].data_ptr(), n_out[p:p + 1].data_ptr(),
+                                                  sums[k:k + 1].data_ptr(), side.cuda_stream))
+                checked[p].record(side)
+            free[p].release()
+            outstanding.release()
+            k += 1
+
+    old_switch = sys.getswitchinterval()
+    sys.setswitchinterval(0.0002)
+    w = threading.Thread(target=waiter)
+    w.start()
+    t0 = time.perf_counter()
+    k = 0
+    while k < cap_req:
+        now = time.perf_counter() - t0
+        if now >= seconds:
+            break
+        if arrivals is not None and arrivals[k] > now:
+            time.sleep(arrivals[k] - now)
+            continue
+        p = k % P
+        outstanding.acquire()
+        free[p].acquire()
+        checked[p].synchronize()
+        if arrivals is not None:
+            late.append(time.perf_counter() - t0 - arrivals[k])
+        n_r, n_s, _ = pool[p]
+        rid = server.submit(R[p].data_ptr(), n_r, S[p].data_ptr(), n_s, outs[p].data_ptr(), outs[p].shape[0],
+                            n_out[p:p + 1].data_ptr())
+        with qcv:
+            queue.append((rid, p))
+            qcv.notify()
+        entries.append(p)
+        k += 1
+    with qcv:
+        done_flag[0] = True
+        qcv.notify()
+    w.join()
+    elapsed = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    sys.setswitchinterval(old_switch)
+    n = len(entries)
+    return {"requests": n, "elapsed_s": elapsed, "latencies_ms": lat, "entries": entries,
+            "sums": sums[:n], "counts": counts[:n], "late_s": late,
+            "tuples": sum(pool[p][0] + pool[p][1] for p in entries)}
+
+
+def run_served(args):
+    import numpy as np
+    import torch
+    import spidjoin as spj
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    lib = spj.lib()
+    P = args.c5_pool
+    pool = c5_specs(P)
+    design = spj.make_design(rank_num=1, join_alg=args.alg, skew_mode=args.skew)
+    budget = 120 << 30
+    server = spj.Server(hbm_budget_bytes=budget, max_batch=args.c5_max_batch, streams=args.c5_streams,
+                        design=design)
+    R, S, outs, exp = [], [], [], []
+    for i, (n_r, n_s, z) in enumerate(pool):
+        dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
+        dS = torch.empty((n_s, 2), dtype=torch.int32, device="cuda")
+        e = torch.zeros(1, dtype=torch.int64, device="cuda")
+        spj.check(lib.spj_generate_device(SEED + 5000 + i, n_r, n_s, z, dR.data_ptr(), dS.data_ptr(), e.data_ptr(),
+                                          None))
+        R.append(dR)
+        S.append(dS)
+        exp.append(e)
+        outs.append(torch.empty((server.output_capacity(n_r, n_s), 2), dtype=torch.int32, device="cuda"))
+    n_out = torch.zeros(P, dtype=torch.int64, device="cuda")
+    exp = torch.cat(exp)
+    n_s_t = torch.tensor([b for _, b, _ in pool], dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+
+    def wrong(run):
+        idx = torch.tensor(run["entries"], dtype=torch.int64, device="cuda")
+        return int(((run["sums"] != exp[idx]) | (run["counts"] != n_s_t[idx])).sum().item())
+
+    def summary(run, st):
+        lat = np.array(run["latencies_ms"])
+        return {"requests": run["requests"], "tuples_per_s": run["tuples"] / run["elapsed_s"],
+                "joins_per_s": run["requests"] / run["elapsed_s"], "elapsed_s": run["elapsed_s"],
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "max_ms": float(lat.max()), "batches": st["batches"], "mean_batch": st["mean_batch"],
+                "max_inflight_batches": st["max_inflight_batches"], "hbm_peak_gib": st["hbm_peak_bytes"] / 2**30,
+                "arrival_lag_p99_ms": float(np.percentile(run["late_s"], 99) * 1e3) if run["late_s"] else None,
+                "wrong_outputs": wrong(run)}
+
+    def leg(srv, rate, seconds, outstanding, seed):
+        srv.reset_stats()
+        run = serve_stream(spj, srv, pool, R, S, outs, n_out, rate, seconds, outstanding, seed)
+        return summary(run, srv.stats())
+
+    serve_stream(spj, server, pool, R, S, outs, n_out, 0, 1.0, 64, SEED)  # warm-up burst
+    sampler = ClockSampler()
+    served = leg(server, args.c5_rate, args.c5_seconds, 1 << 20, SEED + 1)
+    clocks = sampler.stop()
+    sat = leg(server, 0, args.c5_sat_seconds, 256, SEED + 2)
+    server.close()
+    # the plain per-request join: the same stream served one join at a time
+    plain_srv = spj.Server(hbm_budget_bytes=budget, max_batch=1, streams=1, design=design)
+    serve_stream(spj, plain_srv, pool, R, S, outs, n_out, 0, 0.5, 8, SEED)
+    plain = leg(plain_srv, args.c5_rate, args.c5_plain_seconds, 1 << 20, SEED + 1)
+    plain_sat = leg(plain_srv, 0, args.c5_sat_seconds, 256, SEED + 2)
+    plain_srv.close()
+    bad = served["wrong_outputs"] + sat["wrong_outputs"] + plain["wrong_outputs"] + plain_sat["wrong_outputs"]
+    if bad:
+        raise SystemExit(f"served join check failed for {bad} outputs")
+    emit({
+        "metric": METRIC, "value": served["tuples_per_s"], "unit": "tuples/s", "n_gpus": ws,
+        "steps": served["requests"], "warmup": 1, "ms_per_step": 1e3 * served["elapsed_s"] / served["requests"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"served join stream: Poisson arrivals at {args.c5_rate:g} joins/s for "
+                               f"{args.c5_seconds:g} s; joins drawn round-robin from a pool of {P} with |R| "
+                               f"log-uniform [2^10, 2^22], R:S in {{1,2,4,8}}, Zipf s ~ U[0, 1.5]; HBM budget "
+                               f"120 GiB", "pool_tuples": sum(a + b for a, b, _ in pool),
+                   "max_batch": args.c5_max_batch, "streams": args.c5_streams, "join_alg": args.alg},
+        "served": served, "saturated": sat, "plain": plain, "plain_saturated": plain_sat,
+        "served_vs_plain_saturated": sat["tuples_per_s"] / plain_sat["tuples_per_s"],
+        "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+        "gpu_launches": 14 * served["batches"], "clocks": clocks,
+        "check": {"outputs_checked": served["requests"] + sat["requests"] + plain["requests"] +
+                  plain_sat["requests"], "all_exact": True,
+                  "how": "count and 64-bit checksum of every output against the generator's"},
+    })
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--alg", type=int, default=0)
     ap.add_argument("--skew", type=int, default=0)
@@ -446,6 +667,13 @@ def main():
     ap.add_argument("--slots", type=int, default=0, help="table slots per CTA (0 = planner)")
     ap.add_argument("--unit", type=int, default=0, help="max S tuples per work unit (0 = planner)")
     ap.add_argument("--c4-scale", type=float, default=1.0, help="scale of the config-4 relation sizes")
+    ap.add_argument("--c5-rate", type=float, default=2000.0, help="served stream: arrivals per second")
+    ap.add_argument("--c5-seconds", type=float, default=60.0, help="served stream: duration")
+    ap.add_argument("--c5-plain-seconds", type=float, default=15.0, help="plain per-request stream: duration")
+    ap.add_argument("--c5-sat-seconds", type=float, default=8.0, help="closed-loop saturation runs: duration")
+    ap.add_argument("--c5-pool", type=int, default=256, help="served stream: distinct joins on the device")
+    ap.add_argument("--c5-max-batch", type=int, default=64)
+    ap.add_argument("--c5-streams", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -453,6 +681,8 @@ def main():
         return run_reference(args)
     if args.workload == "c4":
         return run_batched(args)
+    if args.workload == "c5":
+        return run_served(args)
     return run_ours(args)
 
 

@@ -196,6 +196,51 @@ int spj_batch_execute(spj_plan_t *plan, void *stream);
 /* Counters of join `join` after an execution (synchronises). */
 int spj_batch_stats(spj_plan_t *plan, int join, spj_stats_t *out);
 
+/* ------------------------------------------------------------ join server --
+ * A served stream of joins on one GPU with continuous batching. No counterpart
+ * in the reference, which runs one JoinInstance per join. A worker thread
+ * inside the server admits submitted joins in arrival order while their HBM
+ * footprint (columns + output + partition scratch, estimated at 16 bytes per
+ * input tuple) fits `hbm_budget_bytes`, forms one batch plan from everything
+ * admitted at that moment (at most `max_batch` joins) and launches it on one of
+ * `streams` streams, so batches overlap on the device. Scratch comes from a
+ * private stream-ordered memory pool; submit and the worker never synchronise
+ * the device. A join larger than the whole budget runs alone. Columns, output
+ * and count stay owned by the caller and must stay valid and unchanged until
+ * spj_server_wait returns for that id. Results equal those of the same join run
+ * alone through spj_plan_execute (as pair multisets). */
+typedef struct spj_server spj_server_t;
+typedef struct {
+    int64_t submitted, completed, failed, batches;
+    int32_t max_inflight_batches, reserved0;
+    double mean_batch;             /* joins per batch */
+    uint64_t hbm_peak_bytes;       /* the most that admission held at once */
+    uint64_t hbm_budget_bytes;
+    double p50_ms, p99_ms, max_ms; /* submit -> completion latency */
+} spj_server_stats_t;
+
+int spj_server_create(const spj_design_t *design, uint64_t hbm_budget_bytes, int max_batch, int streams,
+                      spj_server_t **out);
+/* Output capacity (pairs) a join of these sizes must be given. */
+int64_t spj_server_output_capacity(spj_server_t *server, int64_t n_r, int64_t n_s);
+/* r, s: device columns (16-byte aligned); out: device pairs (16-byte aligned);
+ * n_out: device int64 receiving the pair count; *id receives the request id. */
+int spj_server_submit(spj_server_t *server, const spj_kv_pair_t *r, int64_t n_r, const spj_kv_pair_t *s,
+                      int64_t n_s, spj_kv_pair_t *out, int64_t out_capacity, int64_t *n_out, int64_t *id);
+/* Waits for request `id` (timeout_ms < 0: no limit; on timeout returns
+ * SPJ_E_TIMEOUT and the id stays valid). On return the join's output and count
+ * are in device memory; latency_ms (may be NULL) receives submit -> completion. */
+int spj_server_wait(spj_server_t *server, int64_t id, double timeout_ms, double *latency_ms);
+int spj_server_stats(spj_server_t *server, spj_server_stats_t *out);
+/* hold != 0 pauses admission (submitted joins wait in the queue); hold = 0
+ * resumes it, and everything queued that fits is admitted as one batch. Lets a
+ * client hand over a group of joins that should run together. */
+int spj_server_hold(spj_server_t *server, int hold);
+/* Clears latencies and counters (e.g. after a warm-up phase). */
+int spj_server_reset_stats(spj_server_t *server);
+/* Finishes every queued and running join, then releases the server. */
+void spj_server_destroy(spj_server_t *server);
+
 /* The join for callers that cannot allocate device memory while they run it: a
  * runtime whose memory pool owns the whole GPU, code running under CUDA stream
  * capture (where cudaMalloc is not allowed), or a latency-bound loop that must

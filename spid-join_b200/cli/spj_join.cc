@@ -1,0 +1,121 @@
+// spj_join -- command-line driver of the join, with the knobs of the
+// reference's driver (test/join/main.cc:73-118):
+//   -s input_size (|R|)  -r rank_num  -z zipf_factor (Zipf exponent x 100)
+//   -t rs_ratio (|S|/|R|)  -R rank_set  -B bank_set
+// plus -a algorithm (phj|nphj|smj|nl), -n repetitions and -S seed. -h, -p and
+// -f take an argument and are ignored, as in the reference.
+//
+// With -z 0 the relations are the reference driver's (test/join/main.cc:33-43):
+// R[i] = (i+1, i+3) and S[i] = (i/ratio + 1, i/ratio + 3). With -z > 0 the
+// reference reads pre-generated files; here S keys are drawn Zipf(z/100) over
+// a seeded shuffle of R's keys by spj_generate_host. The output is checked by
+// count and by the order-independent 64-bit checksum; the exit status is 0
+// when it matches, 1 when it does not and 2 on an error.
+#include <getopt.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <string>
+#include <vector>
+
+#include "pidjoin.hpp"
+
+using namespace pidjoin;
+
+// the output checksum's digest: the splitmix64 finaliser of (lvalue << 32 | rvalue)
+static uint64_t splitmix64(uint64_t x) {
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+static uint64_t pair_sum(const kv_pair_t *p, int64_t n) {
+    uint64_t s = 0;
+    for (int64_t i = 0; i < n; i++) s += splitmix64((uint64_t)p[i].lvalue << 32 | p[i].rvalue);
+    return s;
+}
+
+int main(int argc, char **argv) {
+    join_design_t d;
+    d.primary_key = "order";
+    d.foreign_key = "l";
+    std::string alg = "phj";
+    int reps = 1;
+    uint64_t seed = 0x5EED5EEDull;
+    if (argc < 2) {
+        fprintf(stderr, "usage: %s -s |R| [-r ranks] [-z zipf*100] [-t |S|/|R|] [-R rank_set] [-B bank_set] "
+                        "[-a phj|nphj|smj|nl] [-n reps] [-S seed]\n", argv[0]);
+        return 0;
+    }
+    int opt;
+    while ((opt = getopt(argc, argv, "s:r:z:t:R:B:h:p:f:a:n:S:")) != -1) {
+        switch (opt) {
+            case 's': d.input_size = atoll(optarg); break;
+            case 'r': d.rank_num = atoi(optarg); break;
+            case 'z': d.zipf_factor = atoi(optarg); break;
+            case 't': d.rs_ratio = atoi(optarg); break;
+            case 'R': d.rank_set = atoi(optarg); break;
+            case 'B': d.bank_set = atoi(optarg); break;
+            case 'a': alg = optarg; break;
+            case 'n': reps = atoi(optarg); break;
+            case 'S': seed = strtoull(optarg, nullptr, 0); break;
+            default: break;
+        }
+    }
+    if (alg == "phj") d.join_alg = JOIN_DESIGN_JOIN_ALGORITHM_PHJ;
+    else if (alg == "nphj") d.join_alg = JOIN_DESIGN_JOIN_ALGORITHM_NPHJ;
+    else if (alg == "smj") d.join_alg = JOIN_DESIGN_JOIN_ALGORITHM_SMJ;
+    else if (alg == "nl") d.join_alg = JOIN_DESIGN_JOIN_ALGORITHM_NL;
+    else {
+        fprintf(stderr, "unknown algorithm %s\n", alg.c_str());
+        return 2;
+    }
+    const int64_t n_r = d.input_size, n_s = d.input_size * (int64_t)d.rs_ratio;
+    if (n_r <= 0 || d.rs_ratio <= 0 || d.rank_num <= 0 || d.rank_set <= 0 || d.rank_num % d.rank_set) {
+        fprintf(stderr, "bad sizes or rank layout\n");
+        return 2;
+    }
+    std::vector<kv_pair_t> R(n_r), S(n_s);
+    uint64_t expect = 0;
+    if (d.zipf_factor == 0) {
+        for (int64_t i = 0; i < n_r; i++) R[i] = {(uint32_t)(i + 1), (uint32_t)(i + 3)};
+        for (int64_t i = 0; i < n_s; i++) {
+            const uint32_t k = (uint32_t)(i / d.rs_ratio);
+            S[i] = {k + 1, k + 3};
+            expect += splitmix64((uint64_t)(k + 3) << 32 | (k + 3));
+        }
+    } else if (spj_generate_host(seed, n_r, n_s, d.zipf_factor / 100.0, R.data(), S.data(), &expect, 0) != SPJ_OK) {
+        fprintf(stderr, "generator: %s\n", spj_last_error());
+        return 2;
+    }
+    try {
+        JoinInstance join_instance(d.rank_num, d.rank_set, d.rank_num / d.rank_set);
+        join_instance.LoadColumn(R.data(), n_r, "left");
+        join_instance.LoadColumn(S.data(), n_s, "right");
+        join_instance.PrepareJoin(d);
+        int bad = 0;
+        for (int it = 0; it < reps; it++) {
+            struct timespec start;
+            clock_gettime(CLOCK_MONOTONIC, &start);
+            join_instance.StartJoin(d);
+            ResultBuffers_t res = join_instance.FinishJoin();
+            join_instance.RecordLogs(start, 0);
+            int64_t n = 0;
+            uint64_t sum = 0;
+            for (size_t r = 0; r < res.first.size(); r++) {
+                n += res.second[r] / 8;
+                sum += pair_sum(res.first[r], res.second[r] / 8);
+            }
+            const bool ok = n == n_s && sum == expect;
+            printf("check: %s pairs=%lld expected=%lld checksum=%016llx expected=%016llx\n", ok ? "ok" : "MISMATCH",
+                   (long long)n, (long long)n_s, (unsigned long long)sum, (unsigned long long)expect);
+            bad += !ok;
+        }
+        return bad ? 1 : 0;
+    } catch (const Error &e) {
+        fprintf(stderr, "%s\n", e.what());
+        return 2;
+    }
+}

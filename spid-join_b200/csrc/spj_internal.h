@@ -175,4 +175,11 @@ size_t layout_plan(spj_plan *pl, char *arena, bool image);
 cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st);
 cudaError_t init_single(spj_plan *pl, cudaStream_t st);
 cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm);
+int create_plan_stream(int J, const int64_t *n_r, const int64_t *n_s, const spj_design_t *design,
+                       const spj_kv_pair_t *const *r, const spj_kv_pair_t *const *s, spj_kv_pair_t *const *out,
+                       int64_t *const *n_out, cudaMemPool_t pool, cudaStream_t st, spj_plan_t **pout,
+                       size_t *bytes);
+void destroy_plan_stream(spj_plan_t *pl, cudaStream_t st);
+int64_t join_output_capacity(int64_t n_r, int64_t n_s, const spj_design_t &d, bool alone);
+int join_ctr_status(unsigned err, unsigned max_r_part);
 }  // namespace spj

@@ -50,6 +50,8 @@ static int ceil_log2(uint64_t v) {
 static bool is_pow2(int64_t v) { return v > 0 && (v & (v - 1)) == 0; }
 
 // Checks that a usable sm_100 device is current and returns its SM count.
+// Attribute queries only (cudaGetDeviceProperties costs milliseconds, and this
+// runs on every plan creation and every served request).
 static int device_sms(int *sms, int *dev_out) {
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
@@ -57,13 +59,15 @@ static int device_sms(int *sms, int *dev_out) {
         cudaGetLastError();
         return set_error(SPJ_E_NODEVICE, "no CUDA device available; libspidjoin has no CPU path");
     }
-    int dev = 0;
+    int dev = 0, major = 0;
     SPJ_CUDA(cudaGetDevice(&dev));
-    cudaDeviceProp prop;
-    SPJ_CUDA(cudaGetDeviceProperties(&prop, dev));
-    if (prop.major != 10)
+    SPJ_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10) {
+        cudaDeviceProp prop;
+        SPJ_CUDA(cudaGetDeviceProperties(&prop, dev));
         return set_error(SPJ_E_NODEVICE, std::string("libspidjoin is built for sm_100a; device is ") + prop.name);
-    *sms = prop.multiProcessorCount;
+    }
+    SPJ_CUDA(cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev));
     if (dev_out) *dev_out = dev;
     return SPJ_OK;
 }
@@ -379,6 +383,97 @@ static int create_plan(int J, const int64_t *n_r, const int64_t *n_s, const spj_
     return SPJ_OK;
 }
 
+}  // extern "C"
+
+namespace spj {
+
+// Builds a batch plan whose scratch is allocated stream-ordered on `st` (from
+// `pool`, or the device's default pool when it is null), with its column,
+// output and per-join count pointers bound and its descriptors uploaded
+// asynchronously; no timing events. Used by the join server, whose batches must
+// not synchronise the device. *bytes receives the scratch size. Release with
+// destroy_plan_stream on the same stream.
+int create_plan_stream(int J, const int64_t *n_r, const int64_t *n_s, const spj_design_t *design,
+                       const spj_kv_pair_t *const *r, const spj_kv_pair_t *const *s, spj_kv_pair_t *const *out,
+                       int64_t *const *n_out, cudaMemPool_t pool, cudaStream_t st, spj_plan_t **pout,
+                       size_t *bytes) {
+    *pout = nullptr;
+    int rc = validate_design(design);
+    if (rc) return rc;
+    if (J < 1 || J > 65535) return set_error(SPJ_E_ARG, "a batch holds 1 to 65535 joins");
+    int sms = 0, dev = 0;
+    if ((rc = device_sms(&sms, &dev))) return rc;
+    spj_plan *pl = new spj_plan();
+    pl->n_r = n_r[0];
+    pl->n_s = n_s[0];
+    pl->design = *design;
+    pl->device = dev;
+    pl->num_sms = sms;
+    pl->have_events = false;
+    const int maxts = max_table_slots(dev);
+    pl->joins.resize(J);
+    pl->shapes.resize(J);
+    int ts_max = 2;
+    for (int j = 0; j < J; j++) {
+        JoinHost &h = pl->joins[j];
+        h.n_r = n_r[j];
+        h.n_s = n_s[j];
+        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1);
+        ts_max = std::max(ts_max, pl->shapes[j].table_slots);
+        h.rel[0].in = reinterpret_cast<const Tuple *>(r[j] ? r[j] : out[j]);
+        h.rel[1].in = reinterpret_cast<const Tuple *>(s[j] ? s[j] : out[j]);
+        h.dev.out = reinterpret_cast<Tuple *>(out[j]);
+        h.dev.n_out_user = reinterpret_cast<unsigned long long *>(n_out[j]);
+    }
+    int per_sm = 0;
+    cudaError_t ce = configure_kernels(ts_max, design->join_alg, &per_sm);
+    if (ce != cudaSuccess || per_sm < 1) {
+        delete pl;
+        return ce != cudaSuccess ? cuda_error(ce, "configure kernels") : set_error(SPJ_E_ARG, "table too large");
+    }
+    pl->join_blocks = std::min(per_sm * sms, kMaxHoles / (kJoinThreads / 32));
+    const size_t b = layout_plan(pl, nullptr, false);
+    ce = pool ? cudaMallocFromPoolAsync(&pl->arena, b, pool, st) : cudaMallocAsync(&pl->arena, b, st);
+    if (ce != cudaSuccess) {
+        delete pl;
+        return cuda_error(ce, "stream-ordered allocation of batch scratch");
+    }
+    pl->arena_bytes = b;
+    layout_plan(pl, (char *)pl->arena, true);
+    ce = cudaMemcpyAsync((char *)pl->arena + pl->desc_offset, pl->desc_host.data(), pl->desc_host.size(),
+                         cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) {
+        cudaFreeAsync(pl->arena, st);
+        delete pl;
+        return cuda_error(ce, "descriptor upload");
+    }
+    *pout = pl;
+    *bytes = b;
+    return SPJ_OK;
+}
+
+void destroy_plan_stream(spj_plan_t *pl, cudaStream_t st) {
+    if (!pl) return;
+    cudaFreeAsync(pl->arena, st);
+    delete pl;
+}
+
+// Output capacity (pairs) a join of these sizes needs inside any plan: |S| plus
+// one output chunk per join warp, counting the most join CTAs an SM can hold
+// (2048 threads), so no kernel attribute query is needed.
+int64_t join_output_capacity(int64_t n_r, int64_t n_s, const spj_design_t &d, bool alone) {
+    int sms = 0, dev = 0;
+    if (device_sms(&sms, &dev)) return -1;
+    const JoinShape sh = plan_shape(n_r, n_s, d, sms, max_table_slots(dev), alone);
+    const int per_sm = 2048 / kJoinThreads;
+    const int blocks = std::min(per_sm * sms, kMaxHoles / (kJoinThreads / 32));
+    return n_s + (int64_t)blocks * (kJoinThreads / 32) * sh.out_chunk;
+}
+
+}  // namespace spj
+
+extern "C" {
+
 int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_plan_t **out) {
     return create_plan(1, &n_r, &n_s, design, out);
 }
@@ -597,3 +692,9 @@ int spj_generate_host(uint64_t seed, int64_t n_r, int64_t n_s, double zipf_s, sp
 }
 
 }  // extern "C"
+
+namespace spj {
+// The status a finished join's counter error bits map to (the message goes to
+// the calling thread's last error).
+int join_ctr_status(unsigned err, unsigned max_r_part) { return ctr_error(nullptr, err, max_r_part); }
+}  // namespace spj

@@ -32,6 +32,8 @@ EXPORTS = (
     "spj_plan_execute", "spj_plan_stats", "spj_plan_destroy", "spj_partition_histogram", "spj_checksum_device",
     "spj_generate_host", "spj_generate_device", "spj_plan_kernel_times", "spj_join_noalloc",
     "spj_batch_create", "spj_batch_output_capacity", "spj_batch_bind", "spj_batch_execute", "spj_batch_stats",
+    "spj_server_create", "spj_server_output_capacity", "spj_server_submit", "spj_server_wait", "spj_server_stats",
+    "spj_server_reset_stats", "spj_server_destroy", "spj_server_hold",
 )
 
 
@@ -64,6 +66,17 @@ class Stats(ctypes.Structure):
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("batches", ctypes.c_int64), ("max_inflight_batches", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("mean_batch", ctypes.c_double), ("hbm_peak_bytes", ctypes.c_uint64),
+                ("hbm_budget_bytes", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f[0]: getattr(self, f[0]) for f in self._fields_ if f[0] != "reserved0"}
 
 
 class KernelTimes(ctypes.Structure):
@@ -117,6 +130,16 @@ def lib():
         L.spj_batch_bind.argtypes = [vp, vp, vp, vp, vp]
         L.spj_batch_execute.argtypes = [vp, vp]
         L.spj_batch_stats.argtypes = [vp, i32, ctypes.POINTER(Stats)]
+        L.spj_server_create.argtypes = [ctypes.POINTER(Design), ctypes.c_uint64, i32, i32, ctypes.POINTER(vp)]
+        L.spj_server_output_capacity.argtypes = [vp, i64, i64]
+        L.spj_server_output_capacity.restype = i64
+        L.spj_server_submit.argtypes = [vp, vp, i64, vp, i64, vp, i64, vp, ctypes.POINTER(i64)]
+        L.spj_server_wait.argtypes = [vp, i64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+        L.spj_server_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+        L.spj_server_reset_stats.argtypes = [vp]
+        L.spj_server_hold.argtypes = [vp, i32]
+        L.spj_server_destroy.argtypes = [vp]
+        L.spj_server_destroy.restype = None
         _lib = L
     return _lib
 
@@ -304,6 +327,59 @@ class Batch:
     def close(self):
         if self._p:
             lib().spj_plan_destroy(self._p)
+            self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The served join stream (spj_server_*): submit joins over device columns,
+    a worker thread in the library batches whatever has arrived and fits the
+    HBM budget, and wait() returns once a join's output is in device memory."""
+
+    def __init__(self, hbm_budget_bytes=120 << 30, max_batch=64, streams=4, design=None):
+        design = design if design is not None else make_design()
+        self._p = ctypes.c_void_p()
+        check(lib().spj_server_create(ctypes.byref(design), int(hbm_budget_bytes), max_batch, streams,
+                                      ctypes.byref(self._p)))
+
+    def output_capacity(self, n_r, n_s):
+        c = lib().spj_server_output_capacity(self._p, n_r, n_s)
+        if c < 0:
+            check(-1)
+        return c
+
+    def submit(self, r_ptr, n_r, s_ptr, n_s, out_ptr, out_capacity, n_out_ptr):
+        i = ctypes.c_int64()
+        check(lib().spj_server_submit(self._p, r_ptr, n_r, s_ptr, n_s, out_ptr, out_capacity, n_out_ptr,
+                                      ctypes.byref(i)))
+        return i.value
+
+    def wait(self, req_id, timeout_ms=-1.0):
+        """Returns the request's submit-to-completion latency in milliseconds."""
+        lat = ctypes.c_double()
+        check(lib().spj_server_wait(self._p, req_id, timeout_ms, ctypes.byref(lat)))
+        return lat.value
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().spj_server_stats(self._p, ctypes.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        check(lib().spj_server_reset_stats(self._p))
+
+    def hold(self, on=True):
+        """Pauses (or resumes) admission; joins submitted meanwhile queue up."""
+        check(lib().spj_server_hold(self._p, 1 if on else 0))
+
+    def close(self):
+        if self._p:
+            lib().spj_server_destroy(self._p)
             self._p = ctypes.c_void_p()
 
     def __del__(self):

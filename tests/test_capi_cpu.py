@@ -41,9 +41,13 @@ def test_no_gpu_fails_loudly(spj):
         spj.JoinInstance(1, 1, 1)
     with pytest.raises(spj.SpjError, match="NODEVICE"):
         spj.Plan(100, 100)
+    with pytest.raises(spj.SpjError, match="NODEVICE"):
+        spj.Server(1 << 30)
 
 
 def test_bad_arguments(spj):
+    with pytest.raises(spj.SpjError, match="ARG"):
+        spj.Server(1 << 30, max_batch=0)
     with pytest.raises(spj.SpjError, match="ARG"):
         spj.JoinInstance(4, 3, 1)  # ranks must equal groups x per group
 
@@ -71,3 +75,15 @@ def test_generator_zipf_head(spj, s):
     top = counts.max() / m
     h = sum(1.0 / k ** s for k in range(1, n + 1))
     assert abs(top - 1.0 / h) < 0.01, (top, 1.0 / h)
+
+
+def test_cli_without_gpu_fails_loudly():
+    import os
+    import subprocess
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    cli = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "spid-join_b200", "spj_join")
+    p = subprocess.run([cli, "-s", "1024", "-t", "2", "-z", "0", "-r", "1", "-R", "1", "-B", "1"],
+                       capture_output=True, text=True, timeout=60)
+    assert p.returncode == 2 and "no CUDA device" in p.stderr

@@ -1,0 +1,24 @@
+"""The command-line driver spj_join, run with the reference driver's knobs
+(test/join/main.cc:73-118: -s -r -z -t -R -B): it joins through the pidjoin.hpp
+facade and checks its output's count and checksum itself (exit status 0)."""
+import os
+import subprocess
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CLI = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "spid-join_b200", "spj_join")
+
+
+@pytest.mark.parametrize("args", [
+    "-s 1048576 -t 2 -z 0 -r 1 -R 1 -B 1",          # the reference's small configuration
+    "-s 262144 -t 4 -z 100 -r 4 -R 4 -B 1",          # Zipf 1.0, replication groups of 4
+    "-s 65536 -t 8 -z 150 -r 4 -R 1 -B 16 -a smj",
+    "-s 65536 -t 2 -z 50 -r 2 -R 2 -B 1 -a nl",
+    "-s 100000 -t 3 -z 0 -r 1 -R 1 -B 1 -a nphj -n 2",
+])
+def test_cli_joins_and_verifies(args):
+    p = subprocess.run([CLI] + args.split(), capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert "check: ok" in p.stdout and "MISMATCH" not in p.stdout
