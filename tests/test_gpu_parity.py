@@ -219,3 +219,25 @@ def test_algorithms_edge_sizes(spj, oracle, alg, nr, ns):
     S = np.stack([rng.integers(1, nr + 3, ns), np.arange(ns)], 1).astype(np.uint32).reshape(ns, 2)
     out = run_instance(spj, R, S, join_alg=alg)[0].pairs()
     assert same_multiset(oracle, out, oracle.simple_join(R, S, keep_unmatched=alg in ("smj", "nl")))
+
+
+@pytest.mark.parametrize("alg", [0, 2])
+def test_host_columns_joined_in_overlapped_slices(spj, oracle, alg):
+    # |S| above 2^26 host tuples: the instance joins S in slices (copy-in,
+    # join and copy-out of different slices overlap); the last slice is
+    # shorter. The union of the slices must be the whole join, twice in a row.
+    n_r, n_s = 1 << 22, (1 << 26) + (1 << 20) + 7
+    R, S, expect = spj.generate_host(n_r, n_s, 1.0, seed=77)
+    inst = spj.JoinInstance(4, 4, 1)
+    inst.LoadColumn(R, n_r, "left")
+    inst.LoadColumn(S, n_s, "right")
+    d = spj.make_design(rank_num=4, rank_set=4, join_alg=alg)
+    inst.PrepareJoin(d)
+    for _ in range(2):
+        inst.StartJoin(d)
+        out = inst.FinishJoin().pairs()
+        assert out.shape == (n_s, 2)
+        assert oracle.checksum(out) == expect
+    logs = inst.RecordLogs()
+    inst.close()
+    assert logs["n_pairs"] == n_s
