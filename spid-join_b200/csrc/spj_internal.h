@@ -19,6 +19,7 @@ namespace spj {
 
 constexpr int kHistThreads = 1024;
 constexpr int kScatterThreads = 512;
+constexpr int kScatterBlocksPerSM = 2;  // resident scatter CTAs per SM (shared memory and registers)
 constexpr int kJoinThreads = 1024;
 constexpr int kOutChunk = 1024;       // output pairs reserved per warp at a time
 constexpr int kMaxHoles = 12288;      // per join: warps of the emitting kernels (one hole each)

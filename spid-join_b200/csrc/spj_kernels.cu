@@ -352,7 +352,7 @@ __device__ __forceinline__ void tile_init(TileSmem &S) {
 
 // Pass 1: one CTA per chunk. Coarse bucket P = p >> b2; the write cursor of
 // (chunk c, bucket P) is base[P << b2] + sum_q off[c][(P << b2) + q].
-__global__ void __launch_bounds__(kScatterThreads, 2) k_scatter1(PlanDev P) {
+__global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatter1(PlanDev P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
     const uint32_t r = find_slot(P.chunk_prefix, P.nrel, blockIdx.x);
@@ -415,7 +415,7 @@ __global__ void k_items(PlanDev P) {
 
 // Pass 2: persistent CTAs over the work list; each item scatters one run of a
 // coarse region to the final fine positions.
-__global__ void __launch_bounds__(kScatterThreads, 2) k_scatter2(PlanDev P) {
+__global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatter2(PlanDev P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
     tile_init(S);
@@ -645,11 +645,15 @@ __device__ __forceinline__ void warp_close(const OutCtx &o, WarpOut &w) {
     w.cur = w.end = 0ull;
 }
 
-// Table slot of a key: the hash bits above the partition bits, scaled to the
-// table size (multiply-shift range reduction).
-__device__ __forceinline__ uint32_t slot_of(uint32_t key, uint32_t bits, uint32_t ts) {
-    const uint32_t hi = glb_partition_hash(key) >> bits;
-    return (uint32_t)(((unsigned long long)hi * ts) >> (32 - bits));
+// Table slot of a key: Fibonacci (multiplicative) hashing -- the key times
+// 2^32 / golden ratio, whose high bits are scaled to the table size
+// (multiply-shift range reduction). Two multiplies; independent of the
+// partition hash, so the keys of one partition spread over the whole table.
+// (The reference's build hashes with its tabulation join_hash,
+// a2a_srj_build.c:202-246; the slot function changes no result.)
+__device__ __forceinline__ uint32_t slot_of(uint32_t key, uint32_t ts) {
+    const uint32_t h = key * 0x9E3779B1u;
+    return (uint32_t)(((unsigned long long)h * ts) >> 32);
 }
 
 // Clears the table and inserts the R partition. Linear probing, key 0 = empty
@@ -659,8 +663,7 @@ __device__ __forceinline__ uint32_t slot_of(uint32_t key, uint32_t bits, uint32_
 __device__ __forceinline__ void build_table(const PlanDev &P, const JoinDev &J, uint32_t j, uint32_t p,
                                             unsigned long long *table) {
     const uint32_t ts = J.table_slots;
-    const uint32_t bits = J.bits;
-    for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) table[i] = 0ull;
+        for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) table[i] = 0ull;
     __syncthreads();
     const RelDev &Rr = P.rel[2 * j];
     const uint32_t nr = Rr.total[p];
@@ -677,7 +680,7 @@ __device__ __forceinline__ void build_table(const PlanDev &P, const JoinDev &J, 
         for (int k = 0; k < B; k++) {
             if (t[k].key == 0) continue;
             const unsigned long long ent = ((unsigned long long)t[k].pay << 32) | t[k].key;
-            uint32_t s = slot_of(t[k].key, bits, ts);
+            uint32_t s = slot_of(t[k].key, ts);
             for (uint32_t step = 0;; step++) {
                 const unsigned long long prev = atomicCAS(&table[s], 0ull, ent);
                 if (prev == 0ull || (uint32_t)prev == t[k].key) break;
@@ -697,9 +700,9 @@ __device__ __forceinline__ void build_table(const PlanDev &P, const JoinDev &J, 
 // halves the steps of the linear scan; when the home slot s is odd, slot s-1 of
 // the first pair lies before the probe sequence and is ignored. The scan is
 // bounded by the table size.
-__device__ __forceinline__ bool probe_table(const unsigned long long *table, uint32_t ts, uint32_t bits,
+__device__ __forceinline__ bool probe_table(const unsigned long long *table, uint32_t ts,
                                             uint32_t key, uint32_t &rpay) {
-    const uint32_t s = slot_of(key, bits, ts);
+    const uint32_t s = slot_of(key, ts);
     const ulonglong2 *t2 = reinterpret_cast<const ulonglong2 *>(table);
     uint32_t p = s & ~1u;
     {
@@ -774,7 +777,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
             build_table(P, J, un.join, un.p, table);
             cur_p = un.p;
         }
-        const uint32_t ts = J.table_slots, bits = J.bits;
+        const uint32_t ts = J.table_slots;
         const Tuple *ps = P.rel[2 * un.join + 1].out;
         constexpr int U = 4;
         for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
@@ -787,7 +790,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
 #pragma unroll
             for (int k = 0; k < U; k++) {
                 uint32_t rp = 0;
-                const bool hit = t[k].key != 0 && probe_table(table, ts, bits, t[k].key, rp);
+                const bool hit = t[k].key != 0 && probe_table(table, ts, t[k].key, rp);
                 warp_emit(o, w, hit, rp, t[k].pay);
             }
         }
@@ -1356,7 +1359,7 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
         k_scatter1<<<P.total_chunks, kScatterThreads, sizeof(TileSmem), st>>>(P);
         if (P.any_two_pass) {
             if (P.total_coarse) k_items<<<(P.total_coarse + 255) / 256, 256, 0, st>>>(P);
-            k_scatter2<<<pl->num_sms * 2, kScatterThreads, sizeof(TileSmem), st>>>(P);
+            k_scatter2<<<pl->num_sms * kScatterBlocksPerSM, kScatterThreads, sizeof(TileSmem), st>>>(P);
         }
         mark(3);
         k_units_count<<<(P.total_jparts + 255) / 256, 256, 0, st>>>(P);

@@ -118,8 +118,9 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
         sh.fine_bits = sh.bits > kMaxPassBits ? sh.bits - (sh.bits + 1) / 2 : 0;
     }
     // One chunk size for both relations so every pass-1 CTA does the same work;
-    // about one wave of 2 CTAs per SM.
-    int64_t c = std::max<int64_t>(4096, (n_r + n_s + 2 * sms - 3) / (2 * sms - 2));
+    // about one wave of resident scatter CTAs.
+    const int64_t wave = (int64_t)kScatterBlocksPerSM * sms - 2;
+    int64_t c = std::max<int64_t>(4096, (n_r + n_s + wave - 1) / wave);
     c = (c + 1) & ~1ll;
     const int64_t ns[2] = {n_r, n_s};
     for (int r = 0; r < 2; r++) {
