@@ -23,7 +23,7 @@ constexpr int kScatterBlocksPerSM = 2;  // resident scatter CTAs per SM (shared 
 constexpr int kJoinThreads = 1024;
 constexpr int kOutChunk = 1024;       // output pairs reserved per warp at a time
 constexpr int kMaxHoles = 12288;      // per join: warps of the emitting kernels (one hole each)
-constexpr int kHoleSortSlots = 16384; // power of two >= kMaxHoles
+constexpr int kUpSlots = kMaxHoles + 2;  // chunks that the output's tail [N, reserved) can span
 constexpr int kMaxRadixBits = 15;
 constexpr int kMaxPassBits = 8;       // buckets per scatter pass <= 256
 constexpr int kTile = 4096;           // tuples sorted per tile in shared memory
@@ -168,7 +168,9 @@ namespace spj {
 int set_error(int code, const std::string &msg);
 int cuda_error(cudaError_t e, const char *what);
 
-JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots, bool alone);
+// batch_tuples: all tuples of the plan's joins when the join is one of many (0 alone)
+JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots, bool alone,
+                     int64_t batch_tuples);
 // Computes the arena layout of pl->joins/pl->shapes (arena == nullptr: size only)
 // and fills pl->dev, the per-join descriptors and the host image of the
 // descriptor arrays.

@@ -1103,10 +1103,10 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
 // can be partly used, so the unused slots form at most one hole per warp and
 // join, at a chunk's tail. With N = reserved - holes, the pairs stored at
 // positions >= N outside holes move into the holes below N. One CTA per join.
-// Exclusive scan in place of a[0..n) (n <= 12 * 1024) by a 1024-thread block;
-// returns the total. Each thread scans 12 consecutive entries.
+// Exclusive scan in place of a[0..n) (n <= 13 * 1024) by a 1024-thread block;
+// returns the total. Each thread scans 13 consecutive entries.
 __device__ unsigned long long block_exclusive_scan(unsigned long long *a, unsigned n, unsigned long long *warp_tot) {
-    constexpr int PER = 12;
+    constexpr int PER = 13;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned beg = threadIdx.x * PER;
     unsigned long long v[PER], sum = 0;
@@ -1146,84 +1146,69 @@ __device__ unsigned long long block_exclusive_scan(unsigned long long *a, unsign
     return total;
 }
 
+// Holes need no sort: each lies in its own chunk (a chunk's tail), so the holes
+// at or above N are put in position order by indexing a slot array with their
+// chunk number relative to N's chunk, and the gaps below N may be filled in
+// any order (the output is a multiset). Three block scans per join.
 __global__ void __launch_bounds__(1024) k_fixup_prep(PlanDev P) {
-    extern __shared__ unsigned long long keys[];  // kHoleSortSlots sorted holes, then kMaxHoles scan slots
+    extern __shared__ unsigned long long sm[];  // kUpSlots upper-hole slots, then kUpSlots scan slots
+    unsigned long long *up = sm;                // (begin << 11) | length of the part above N, 0 = none
+    unsigned long long *scan = sm + kUpSlots;
     __shared__ unsigned long long warp_tot[33];
-    __shared__ unsigned s_nl, s_i0;
     const JoinDev &J = P.join[blockIdx.x];
     JoinCtr *ctr = J.ctr;
-    unsigned long long *scan = keys + kHoleSortSlots;
     const unsigned nh = min(ctr->hole_count, (unsigned)kMaxHoles);
-    unsigned npow = 1;
-    while (npow < nh) npow <<= 1;
-    for (unsigned i = threadIdx.x; i < npow; i += blockDim.x) {
-        if (i < nh) {
-            const Hole h = J.holes[i];
-            keys[i] = (h.begin << 11) | (h.end - h.begin);
-        } else {
-            keys[i] = ~0ull;
-        }
-    }
-    if (threadIdx.x == 0) {
-        s_nl = 0;
-        s_i0 = nh;
-    }
-    __syncthreads();
-    for (unsigned k = 2; k <= npow; k <<= 1) {
-        for (unsigned j = k >> 1; j > 0; j >>= 1) {
-            for (unsigned i = threadIdx.x; i < npow; i += blockDim.x) {
-                const unsigned ixj = i ^ j;
-                if (ixj > i) {
-                    const unsigned long long a = keys[i], b = keys[ixj];
-                    if ((a > b) == ((i & k) == 0)) {
-                        keys[i] = b;
-                        keys[ixj] = a;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-    // total hole length -> N
-    for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) scan[i] = keys[i] & 2047ull;
+    const unsigned long long chunk = J.out_chunk;
+    for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) scan[i] = J.holes[i].end - J.holes[i].begin;
     __syncthreads();
     const unsigned long long H = block_exclusive_scan(scan, nh, warp_tot);
     const unsigned long long total = ctr->out_reserved;
     const unsigned long long N = total - H;
-    // parts of each hole below N (gaps to fill) and above N (skipped by the data)
+    const unsigned long long c0 = N / chunk;
+    const unsigned long long ncu = total > N ? (total - 1) / chunk - c0 + 1 : 0;
+    if (ncu > (unsigned long long)kUpSlots) {  // cannot happen while holes are chunk tails
+        if (threadIdx.x == 0) atomicOr(&ctr->error, 8u);
+        return;
+    }
+    for (unsigned k = threadIdx.x; k < ncu; k += blockDim.x) up[k] = 0ull;
+    __syncthreads();
+    // gap part (below N) of every hole, in hole order; upper part into its chunk's slot
     for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) {
-        const unsigned long long b = keys[i] >> 11, e = b + (keys[i] & 2047ull);
+        const unsigned long long b = J.holes[i].begin, e = J.holes[i].end;
         scan[i] = b < N ? (e < N ? e : N) - b : 0ull;
-        if (b < N && (i + 1 == nh || (keys[i + 1] >> 11) >= N)) s_nl = i + 1;       // holes below N: a prefix
-        if (e > N && (i == 0 || (keys[i - 1] >> 11) + (keys[i - 1] & 2047ull) <= N)) s_i0 = i;  // above: a suffix
+        J.gaps[i].begin = b;
+        if (e > N) {
+            const unsigned long long ub = b > N ? b : N;
+            up[ub / chunk - c0] = (ub << 11) | (e - ub);
+        }
     }
     __syncthreads();
     const unsigned long long G = block_exclusive_scan(scan, nh, warp_tot);
-    const unsigned nl = s_nl, i0 = s_i0;
-    for (unsigned i = threadIdx.x; i < nl; i += blockDim.x) {
-        J.gaps[i].begin = keys[i] >> 11;
-        J.gap_off[i] = scan[i];
-    }
+    for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) J.gap_off[i] = scan[i];
     __syncthreads();
-    for (unsigned i = threadIdx.x; i < nh; i += blockDim.x) {
-        const unsigned long long b = keys[i] >> 11, e = b + (keys[i] & 2047ull);
-        scan[i] = e > N ? e - (b > N ? b : N) : 0ull;
-    }
+    // upper holes in position order: their ranks, then the hole length before each
+    for (unsigned k = threadIdx.x; k < ncu; k += blockDim.x) scan[k] = up[k] ? 1ull : 0ull;
     __syncthreads();
-    block_exclusive_scan(scan, nh, warp_tot);
-    for (unsigned i = i0 + threadIdx.x; i < nh; i += blockDim.x) {
-        const unsigned long long b = keys[i] >> 11, e = b + (keys[i] & 2047ull);
-        const unsigned long long ub = b > N ? b : N;
+    const unsigned long long nd = block_exclusive_scan(scan, (unsigned)ncu, warp_tot);
+    for (unsigned k = threadIdx.x; k < ncu; k += blockDim.x)
+        if (up[k]) J.datas[scan[k]].end = k;  // slot of the rank-th upper hole
+    __syncthreads();
+    for (unsigned d = threadIdx.x; d < nd; d += blockDim.x) scan[d] = up[J.datas[d].end] & 2047ull;
+    __syncthreads();
+    block_exclusive_scan(scan, (unsigned)nd, warp_tot);
+    for (unsigned d = threadIdx.x; d < nd; d += blockDim.x) {
+        const unsigned long long u = up[J.datas[d].end];
+        const unsigned long long ub = u >> 11;
         // data elements stored before this hole, and holes' length up to and including it
-        J.datas[i - i0].begin = ub - N - scan[i];
-        J.data_off[i - i0] = scan[i] + (e - ub);
+        J.datas[d].begin = ub - N - scan[d];
+        J.data_off[d] = scan[d] + (u & 2047ull);
     }
     if (threadIdx.x == 0) {
         ctr->n_out = N;
         if (J.n_out_user) *J.n_out_user = N;
         ctr->gap_total = G;
-        ctr->n_gaps = nl;
-        ctr->n_data = nh - i0;
+        ctr->n_gaps = nh;
+        ctr->n_data = (unsigned)nd;
     }
 }
 
@@ -1374,8 +1359,9 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
             k_join_phj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
     }
     mark(5);
-    k_fixup_prep<<<J, 1024, (size_t)(kHoleSortSlots + kMaxHoles) * 8, st>>>(P);
-    k_fixup_copy<<<dim3((kMaxHoles + 7) / 8, J), 256, 0, st>>>(P);
+    k_fixup_prep<<<J, 1024, (size_t)kUpSlots * 2 * 8, st>>>(P);
+    // gaps are spread over all warps of a join's blocks; a batch gives each join fewer blocks
+    k_fixup_copy<<<dim3(std::max<uint32_t>(16, (kMaxHoles + 7) / 8 / J), J), 256, 0, st>>>(P);
     mark(6);
     if (ev) {
         pl->ring_next = (pl->ring_next + 1) % spj_plan::kRing;
@@ -1406,7 +1392,7 @@ cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm)
                                       cudaSharedmemCarveoutMaxShared)))
             return e;
     e = cudaFuncSetAttribute(k_fixup_prep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (kHoleSortSlots + kMaxHoles) * 8);
+                             kUpSlots * 2 * 8);
     if (e) return e;
     const void *jk = alg == SPJ_ALG_SMJ    ? (const void *)k_join_smj
                      : alg == SPJ_ALG_NL   ? (const void *)k_join_nl

@@ -82,7 +82,8 @@ static int max_table_slots(int dev) {
 
 // Per-join tuning: the planner's choice for these sizes (size classes follow
 // from the formulas: fan-out from |R|, chunking from |R|+|S|).
-JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots, bool alone) {
+JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots, bool alone,
+                     int64_t batch_tuples) {
     JoinShape sh;
     int ts = d.table_slots > 0 ? std::min(d.table_slots, max_slots) : kDefaultTableSlots;
     if (d.join_alg == SPJ_ALG_NPHJ) {
@@ -117,10 +118,14 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
         sh.table_slots = ts & ~1;  // pairs of slots are probed together
         sh.fine_bits = sh.bits > kMaxPassBits ? sh.bits - (sh.bits + 1) / 2 : 0;
     }
-    // One chunk size for both relations so every pass-1 CTA does the same work;
-    // about one wave of resident scatter CTAs.
+    // One chunk size for both relations so every pass-1 CTA does the same work:
+    // about one wave of resident scatter CTAs over this join; when the join is
+    // one of many, chunks are at least 1/8 wave of the whole batch, so a batch
+    // has about eight waves of chunks in all (fine enough to balance the
+    // pass-1 CTAs, coarse enough to keep the per-chunk histograms small).
     const int64_t wave = (int64_t)kScatterBlocksPerSM * sms - 2;
-    int64_t c = std::max<int64_t>(4096, (n_r + n_s + wave - 1) / wave);
+    const int64_t spread = std::max<int64_t>(n_r + n_s, batch_tuples / 8);
+    int64_t c = std::max<int64_t>(4096, (spread + wave - 1) / wave);
     c = (c + 1) & ~1ll;
     const int64_t ns[2] = {n_r, n_s};
     for (int r = 0; r < 2; r++) {
@@ -346,10 +351,13 @@ static int create_plan(int J, const int64_t *n_r, const int64_t *n_s, const spj_
     pl->joins.resize(J);
     pl->shapes.resize(J);
     int ts_max = 2;
+    int64_t batch_tuples = 0;
+    if (J > 1)
+        for (int j = 0; j < J; j++) batch_tuples += n_r[j] + n_s[j];
     for (int j = 0; j < J; j++) {
         pl->joins[j].n_r = n_r[j];
         pl->joins[j].n_s = n_s[j];
-        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1);
+        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1, batch_tuples);
         ts_max = std::max(ts_max, pl->shapes[j].table_slots);
     }
     int per_sm = 0;
@@ -415,11 +423,14 @@ int create_plan_stream(int J, const int64_t *n_r, const int64_t *n_s, const spj_
     pl->joins.resize(J);
     pl->shapes.resize(J);
     int ts_max = 2;
+    int64_t batch_tuples = 0;
+    if (J > 1)
+        for (int j = 0; j < J; j++) batch_tuples += n_r[j] + n_s[j];
     for (int j = 0; j < J; j++) {
         JoinHost &h = pl->joins[j];
         h.n_r = n_r[j];
         h.n_s = n_s[j];
-        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1);
+        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1, batch_tuples);
         ts_max = std::max(ts_max, pl->shapes[j].table_slots);
         h.rel[0].in = reinterpret_cast<const Tuple *>(r[j] ? r[j] : out[j]);
         h.rel[1].in = reinterpret_cast<const Tuple *>(s[j] ? s[j] : out[j]);
@@ -465,7 +476,7 @@ void destroy_plan_stream(spj_plan_t *pl, cudaStream_t st) {
 int64_t join_output_capacity(int64_t n_r, int64_t n_s, const spj_design_t &d, bool alone) {
     int sms = 0, dev = 0;
     if (device_sms(&sms, &dev)) return -1;
-    const JoinShape sh = plan_shape(n_r, n_s, d, sms, max_table_slots(dev), alone);
+    const JoinShape sh = plan_shape(n_r, n_s, d, sms, max_table_slots(dev), alone, 0);
     const int per_sm = 2048 / kJoinThreads;
     const int blocks = std::min(per_sm * sms, kMaxHoles / (kJoinThreads / 32));
     return n_s + (int64_t)blocks * (kJoinThreads / 32) * sh.out_chunk;
