@@ -384,32 +384,57 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
 }
 
 // Work list of pass 2: for every (relation, coarse bucket), runs of consecutive
-// chunks holding at least `item_target` tuples. Within a coarse region the
-// chunks' segments follow each other in chunk order, as do the fine offsets, so
-// cursors set from a run's first chunk stay exact. A heavy single segment is its
-// own item.
+// chunks. A run ends at each chunk where the bucket's running tuple count
+// crosses a multiple of `item_target` (and at the last chunk, if tuples remain),
+// so runs hold about item_target tuples and a heavy single segment is its own
+// run. Within a coarse region the chunks' segments follow each other in chunk
+// order, as do the fine offsets, so cursors set from a run's first chunk stay
+// exact. One warp per (relation, coarse bucket), 32 chunks per step.
 __global__ void k_items(PlanDev P) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= P.total_coarse) return;
+    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= P.total_coarse) return;  // whole warps leave together
     const uint32_t r = find_slot(P.coarse_prefix, P.nrel, t);
     const uint32_t cb = t - P.coarse_prefix[r];
     const RelDev R = P.rel[r];
     const JoinDev &J = P.join[R.join];
     const uint32_t f1 = 1u << (J.bits - J.fine_bits);
-    uint32_t acc = 0, c0 = 0;
-    for (uint32_t c = 0; c < R.nchunks; c++) {
-        acc += R.chist[(size_t)c * f1 + cb];
-        if (acc >= J.item_target || c + 1 == R.nchunks) {
-            if (acc) {
-                const unsigned i = atomicAdd(&P.bctr->item_count, 1u);
-                if (i < P.max_items)
-                    P.items[i] = make_uint4(r, cb, c0, c + 1);
-                else
-                    atomicOr(&J.ctr->error, 4u);
-            }
-            acc = 0;
-            c0 = c + 1;
+    const unsigned long long T = J.item_target;
+    const uint32_t nch = R.nchunks;
+    unsigned long long carry = 0, cum_last_b = 0;  // count before this step; count at the last run end
+    int last_b = -1;                                 // chunk of the last run end
+    for (uint32_t base = 0; base < nch; base += 32) {
+        const uint32_t c = base + lane;
+        const unsigned long long cnt = c < nch ? R.chist[(size_t)c * f1 + cb] : 0u;
+        unsigned long long incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long x = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += x;
         }
+        const unsigned long long cum = carry + incl, prev = cum - cnt;
+        const bool cross = c < nch && cum / T != prev / T;
+        // the run ending here starts after the previous run end (this step or earlier)
+        const unsigned below = __ballot_sync(0xffffffffu, cross) & ((1u << lane) - 1u);
+        const int pl = below ? 31 - __clz(below) : -1;
+        const unsigned long long cum_pl = __shfl_sync(0xffffffffu, cum, pl < 0 ? 0 : pl);
+        const int start_b = pl >= 0 ? (int)base + pl : last_b;
+        const unsigned long long cum_start = pl >= 0 ? cum_pl : cum_last_b;
+        const bool tail = c + 1 == nch && !cross && cum > cum_start;
+        if (cross || tail) {
+            const unsigned i = atomicAdd(&P.bctr->item_count, 1u);
+            if (i < P.max_items)
+                P.items[i] = make_uint4(r, cb, (uint32_t)(start_b + 1), c + 1);
+            else
+                atomicOr(&J.ctr->error, 4u);
+        }
+        const unsigned all = __ballot_sync(0xffffffffu, cross);
+        if (all) {
+            const int hb = 31 - __clz(all);
+            cum_last_b = __shfl_sync(0xffffffffu, cum, hb);
+            last_b = (int)base + hb;
+        }
+        carry = __shfl_sync(0xffffffffu, cum, 31);
     }
 }
 
@@ -1343,7 +1368,7 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
         mark(2);
         k_scatter1<<<P.total_chunks, kScatterThreads, sizeof(TileSmem), st>>>(P);
         if (P.any_two_pass) {
-            if (P.total_coarse) k_items<<<(P.total_coarse + 255) / 256, 256, 0, st>>>(P);
+            if (P.total_coarse) k_items<<<(P.total_coarse + 7) / 8, 256, 0, st>>>(P);
             k_scatter2<<<pl->num_sms * kScatterBlocksPerSM, kScatterThreads, sizeof(TileSmem), st>>>(P);
         }
         mark(3);
