@@ -130,11 +130,21 @@ __global__ void k_colscan(PlanDev P) {
     const RelDev R = P.rel[r];
     const uint32_t F = 1u << P.join[R.join].bits;
     const uint32_t p = t - P.part_prefix[r];
-    uint32_t run = 0;
-    for (uint32_t c = 0; c < R.nchunks; c++) {
-        uint32_t *cell = R.hist + (size_t)c * F + p;
-        const uint32_t v = *cell;
-        *cell = run;
+    uint32_t run = 0, c = 0;
+    uint32_t *col = R.hist + p;
+    for (; c + 8 <= R.nchunks; c += 8) {  // eight loads in flight before the stores
+        uint32_t v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = col[(size_t)(c + k) * F];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            col[(size_t)(c + k) * F] = run;
+            run += v[k];
+        }
+    }
+    for (; c < R.nchunks; c++) {
+        const uint32_t v = col[(size_t)c * F];
+        col[(size_t)c * F] = run;
         run += v;
     }
     R.total[p] = run;
