@@ -6,8 +6,10 @@ fraction of the HBM roofline, on the seeded synthetic relations.
 
 One step = one plain join (partition, build, probe, compaction) of the workload
 with R and S resident in HBM. Rank 0 prints one JSON line. Under torchrun with
-N > 1 every rank joins its own relations (replicas, weak scaling; the
-multi-GPU hash exchange is not built yet) and the time is the max over ranks.
+N > 1 the step is one join sharded over the N GPUs (each rank holds the
+workload's |R| and |S|: weak scaling): split by destination rank, NCCL
+all-to-all of R and S, local join; the time is the max over ranks
+(`--replicas`: N independent joins instead).
 `--impl reference` times the reference's algorithm restated on the host cores
 (the oracle's pipeline restatement; the UPMEM original cannot run here).
 """
@@ -354,6 +356,122 @@ def run_ours(args):
     return 0
 
 
+# ------------------------------------------------------- sharded (N > 1) --
+def run_distributed(args):
+    """One join over N GPUs: every rank holds a shard of R and of S (the
+    workload's sizes per rank: weak scaling; rank i's keys are its generator's
+    keys + i*|R|, so the global R has unique keys), splits both by destination
+    rank, exchanges them with NCCL all-to-all and joins what it received. The
+    timed step is the whole distributed join; time = max over ranks."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import spidjoin as spj
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if "MASTER_ADDR" not in os.environ:  # one process without torchrun (--sharded)
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(sk.getsockname()[1]), RANK="0",
+                              WORLD_SIZE="1")
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    n_r, n_s, zipf, (ranks, rsets, bset), desc = WORKLOADS[args.workload]
+    design = spj.make_design(rank_num=ranks, rank_set=rsets, bank_set=bset, join_alg=args.alg,
+                             skew_mode=args.skew, input_size=n_r, rs_ratio=max(n_s // n_r, 1),
+                             zipf_factor=int(round(zipf * 100)), radix_bits=args.bits,
+                             table_slots=args.slots, unit_tuples=args.unit)
+    lib = spj.lib()
+    stream = torch.cuda.current_stream()
+    dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
+    dS = torch.empty((n_s, 2), dtype=torch.int32, device="cuda")
+    expect = torch.zeros(1, dtype=torch.int64, device="cuda")
+    spj.check(lib.spj_generate_device(SEED + rank, n_r, n_s, zipf, dR.data_ptr(), dS.data_ptr(),
+                                      expect.data_ptr(), stream.cuda_stream))
+    dR[:, 0] += rank * n_r
+    dS[:, 0] += rank * n_r
+    dj = spj.DistributedJoin(design=design)
+    csum = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for _ in range(args.warmup):
+        pairs, n = dj.run(dR, dS)
+    spj.check(lib.spj_checksum_device(pairs.data_ptr(), n.data_ptr(), csum.data_ptr(), stream.cuda_stream))
+    tot = torch.stack([csum[0], expect[0], n[0]])
+    dist.all_reduce(tot)
+    if int(tot[0].item()) != int(tot[1].item()) or int(tot[2].item()) != ws * n_s:
+        raise SystemExit("distributed join result check failed")
+    del pairs
+    sampler = ClockSampler() if rank == 0 else None
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        pairs, n = dj.run(dR, dS)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = sampler.stop() if sampler else None
+    t = torch.tensor([ev0.elapsed_time(ev1) / args.steps], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step = float(t.item())
+    local_out = torch.tensor([float(n.item())], dtype=torch.float64, device="cuda")
+    dist.all_reduce(local_out, op=dist.ReduceOp.MAX)
+    del pairs
+    # end to end: shards from pinned host memory, the distributed join, pairs back to pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        hR = torch.empty((n_r, 2), dtype=torch.int32, pin_memory=True)
+        hS = torch.empty((n_s, 2), dtype=torch.int32, pin_memory=True)
+        hR.copy_(dR)
+        hS.copy_(dS)
+        hout = torch.empty((int(local_out.item()) + (1 << 20), 2), dtype=torch.int32, pin_memory=True)
+        ke, got, el = 2, 0, 0.0
+        for i in range(ke + 1):
+            dist.barrier()
+            t0 = time.perf_counter()
+            dR.copy_(hR, non_blocking=True)
+            dS.copy_(hS, non_blocking=True)
+            pairs, n = dj.run(dR, dS)
+            k = int(n.item())
+            if k > hout.shape[0]:
+                hout = torch.empty((k, 2), dtype=torch.int32, pin_memory=True)
+            hout[:k].copy_(pairs[:k], non_blocking=True)
+            torch.cuda.synchronize()
+            if i > 0:
+                el += time.perf_counter() - t0
+                got += k
+            del pairs
+        te = torch.tensor([el], dtype=torch.float64, device="cuda")
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": ws * (n_r + n_s) * ke / float(te.item()), "unit": "tuples/s", "steps": ke,
+               "h2d_bytes_per_step": 8 * (n_r + n_s), "d2h_bytes_per_step": 8 * got // ke,
+               "ms_per_step": float(te.item()) / ke * 1e3, "per": "rank 0's copies; time max over ranks"}
+        del hR, hS, hout
+    dj.close()
+    peak, peak_kind = peaks()
+    pipe_bytes = ws * (24 * (n_r + n_s) + 8 * n_s)
+    if rank == 0:
+        emit({
+            "metric": METRIC, "value": ws * (n_r + n_s) / (ms_step / 1e3), "unit": "tuples/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": desc + f"; per rank, sharded over {ws} GPUs (rank i keys + i*|R|)",
+                       "n_r_per_rank": n_r, "n_s_per_rank": n_s, "zipf": zipf, "join_alg": args.alg,
+                       "parallelism": f"hash exchange over {ws} ranks (split, NCCL all-to-all, local join)",
+                       "l2": "inputs larger than L2; no flush", "seed": SEED},
+            "pipeline_roofline": {"achieved": pipe_bytes / ws / (ms_step / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                  "frac": pipe_bytes / ws / (ms_step / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
+                                  "formula": "per rank: 24*(|R|+|S|) + 8*|out|, exchange not counted"},
+            "max_local_pairs": local_out.item(),
+            "e2e": e2e, "cpu_baseline": None, "gpu_launches": 24 * args.steps, "clocks": clocks,
+            "check": {"global_checksum_ok": True, "pairs": int(tot[2].item())},
+        })
+    dist.destroy_process_group()
+    return 0
+
+
 # ----------------------------------------------------------- batched (c4) --
 def c4_specs(n_joins=256, seed=SEED + 4, scale=1.0):
     """Config 4: |R| log-uniform in [2^12, 2^24], R:S ratio from {1,2,4,8}, Zipf s
@@ -674,6 +792,8 @@ def main():
     ap.add_argument("--c5-pool", type=int, default=256, help="served stream: distinct joins on the device")
     ap.add_argument("--c5-max-batch", type=int, default=64)
     ap.add_argument("--c5-streams", type=int, default=4)
+    ap.add_argument("--replicas", action="store_true", help="N > 1: independent joins instead of one sharded join")
+    ap.add_argument("--sharded", action="store_true", help="the sharded join even on one GPU (exchange with itself)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -683,6 +803,8 @@ def main():
         return run_batched(args)
     if args.workload == "c5":
         return run_served(args)
+    if (dist_env()[0] > 1 and not args.replicas) or args.sharded:
+        return run_distributed(args)
     return run_ours(args)
 
 

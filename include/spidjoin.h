@@ -261,6 +261,19 @@ void spj_server_destroy(spj_server_t *server);
 int spj_join_noalloc(const spj_kv_pair_t *r, int64_t n_r, const spj_kv_pair_t *s, int64_t n_s, spj_kv_pair_t *out,
                      int64_t out_capacity, int64_t *n_out, void *stream);
 
+/* The split before the rank-to-rank exchange of a join sharded over `world`
+ * GPUs: the B200 form of the reference's global partition scatter into
+ * per-rank packets ahead of its rotate-and-stream shuffle
+ * (src/dpu/src/join/glb_partition_packet.c:420-464, src/queryHostFunc.cc:481-777).
+ * The destination of a tuple is (glb_partition_hash(key) * world) >> 32. out
+ * (device, n pairs) receives the non-padding tuples grouped by destination:
+ * destination d's are out[off_d, off_d + counts[d]) with off the exclusive
+ * prefix of counts (the order inside a group is unspecified). counts: device
+ * int64[2 * world]; the first `world` entries receive the group sizes, the rest
+ * is workspace. Allocates nothing, does not synchronise. */
+int spj_exchange_split(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv_pair_t *out, int64_t *counts,
+                       void *stream);
+
 /* Histogram of glb_partition_hash(key) & (2^bits - 1) over a device column (key-0
  * tuples skipped): the B200 form of the global partition count kernel
  * (src/dpu/src/join/glb_partition_count.c:119-371, partition_type 0). hist is a

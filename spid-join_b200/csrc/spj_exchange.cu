@@ -1,0 +1,127 @@
+// spj_exchange.cu -- the split that precedes the rank-to-rank exchange of a
+// join sharded over several GPUs.
+//
+// The reference shuffles every relation between its DPU ranks through the host
+// (the rotate-and-stream all-to-all, src/queryHostFunc.cc:481-777, with
+// destinations from the global partition hash, glb_partition_packet.c:420-464).
+// Over NVLink the exchange is one all-to-all per relation; before it, each GPU
+// groups its shard by destination rank so that every destination's tuples are
+// one contiguous segment. The destination of a key is glb_partition_hash(key)
+// scaled to the number of ranks (multiply-shift), which leaves its low bits --
+// the local partitions of the join that follows -- evenly spread on every rank.
+#include <cuda_runtime.h>
+
+#include "spj_internal.h"
+
+using namespace spj;
+
+namespace {
+
+constexpr int kSplitThreads = 512;
+constexpr int kSplitTile = 4096;  // tuples per block step
+constexpr int kMaxWorld = 1024;
+
+__device__ __forceinline__ uint32_t dest_of(uint32_t key, uint32_t world) {
+    return (uint32_t)(((unsigned long long)glb_partition_hash(key) * world) >> 32);
+}
+
+// counts[d] += tuples of destination d (key-0 padding is dropped).
+__global__ void __launch_bounds__(kSplitThreads) k_split_count(const Tuple *in, unsigned long long n, uint32_t world,
+                                                               unsigned long long *counts) {
+    __shared__ uint32_t cnt[kMaxWorld];
+    for (uint32_t d = threadIdx.x; d < world; d += blockDim.x) cnt[d] = 0;
+    __syncthreads();
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const Tuple t = in[i];
+        if (t.key) atomicAdd(&cnt[dest_of(t.key, world)], 1u);
+    }
+    __syncthreads();
+    for (uint32_t d = threadIdx.x; d < world; d += blockDim.x)
+        if (cnt[d]) atomicAdd(&counts[d], (unsigned long long)cnt[d]);
+}
+
+// cursor[d] = exclusive prefix of counts (one warp; world <= 1024).
+__global__ void k_split_offsets(const unsigned long long *counts, uint32_t world, unsigned long long *cursor) {
+    const int lane = threadIdx.x;
+    unsigned long long carry = 0;
+    for (uint32_t base = 0; base < world; base += 32) {
+        const uint32_t d = base + lane;
+        const unsigned long long v = d < world ? counts[d] : 0ull;
+        unsigned long long incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long x = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += x;
+        }
+        if (d < world) cursor[d] = carry + incl - v;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+}
+
+// Each block step takes a tile, counts it per destination, reserves one range
+// per destination with one atomic each and writes its tuples there, so a
+// destination's tuples from one tile leave as one run.
+__global__ void __launch_bounds__(kSplitThreads) k_split_scatter(const Tuple *in, unsigned long long n, uint32_t world,
+                                                                 unsigned long long *cursor, Tuple *out) {
+    __shared__ uint32_t cnt[kMaxWorld];
+    __shared__ unsigned long long base[kMaxWorld];
+    constexpr int PER = kSplitTile / kSplitThreads;
+    for (unsigned long long t0 = (unsigned long long)blockIdx.x * kSplitTile; t0 < n;
+         t0 += (unsigned long long)gridDim.x * kSplitTile) {
+        for (uint32_t d = threadIdx.x; d < world; d += blockDim.x) cnt[d] = 0;
+        __syncthreads();
+        Tuple v[PER];
+        uint32_t dr[PER];  // destination << 16 | rank in the tile; 0xffffffff = none
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const unsigned long long i = t0 + threadIdx.x + (unsigned long long)k * kSplitThreads;
+            v[k] = i < n ? in[i] : Tuple{0u, 0u};
+            dr[k] = 0xffffffffu;
+            if (v[k].key) {
+                const uint32_t d = dest_of(v[k].key, world);
+                dr[k] = (d << 16) | atomicAdd(&cnt[d], 1u);
+            }
+        }
+        __syncthreads();
+        for (uint32_t d = threadIdx.x; d < world; d += blockDim.x)
+            base[d] = cnt[d] ? atomicAdd(&cursor[d], (unsigned long long)cnt[d]) : 0ull;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PER; k++)
+            if (dr[k] != 0xffffffffu) out[base[dr[k] >> 16] + (dr[k] & 0xffffu)] = v[k];
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int spj_exchange_split(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv_pair_t *out, int64_t *counts,
+                       void *stream) {
+    if (world < 1 || world > kMaxWorld) return set_error(SPJ_E_ARG, "world must be in [1, 1024]");
+    if (n < 0 || (n > 0 && (!tuples || !out)) || !counts) return set_error(SPJ_E_ARG, "bad split arguments");
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(SPJ_E_NODEVICE, "no CUDA device available; libspidjoin has no CPU path");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(counts);
+    unsigned long long *cursor = cnt + world;
+    e = cudaMemsetAsync(cnt, 0, (size_t)world * 8, st);
+    if (e != cudaSuccess) return cuda_error(e, "split counters");
+    const Tuple *in = reinterpret_cast<const Tuple *>(tuples);
+    if (n > 0) k_split_count<<<sms * 4, kSplitThreads, 0, st>>>(in, (unsigned long long)n, world, cnt);
+    k_split_offsets<<<1, 32, 0, st>>>(cnt, world, cursor);
+    if (n > 0)
+        k_split_scatter<<<sms * 4, kSplitThreads, 0, st>>>(in, (unsigned long long)n, world, cursor,
+                                                            reinterpret_cast<Tuple *>(out));
+    e = cudaGetLastError();
+    return e ? cuda_error(e, "split kernels") : SPJ_OK;
+}
+
+}  // extern "C"

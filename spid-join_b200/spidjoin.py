@@ -33,7 +33,7 @@ EXPORTS = (
     "spj_generate_host", "spj_generate_device", "spj_plan_kernel_times", "spj_join_noalloc",
     "spj_batch_create", "spj_batch_output_capacity", "spj_batch_bind", "spj_batch_execute", "spj_batch_stats",
     "spj_server_create", "spj_server_output_capacity", "spj_server_submit", "spj_server_wait", "spj_server_stats",
-    "spj_server_reset_stats", "spj_server_destroy", "spj_server_hold",
+    "spj_server_reset_stats", "spj_server_destroy", "spj_server_hold", "spj_exchange_split",
 )
 
 
@@ -140,6 +140,7 @@ def lib():
         L.spj_server_hold.argtypes = [vp, i32]
         L.spj_server_destroy.argtypes = [vp]
         L.spj_server_destroy.restype = None
+        L.spj_exchange_split.argtypes = [vp, i64, i32, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -387,3 +388,77 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class DistributedJoin:
+    """A join of R and S sharded over the ranks of a torch.distributed process
+    group, one GPU per rank: the multi-GPU form of the reference's rank-to-rank
+    shuffle (src/queryHostFunc.cc:481-777). Every rank splits its shards by
+    destination rank (spj_exchange_split: (glb_partition_hash(key) * world) >> 32),
+    exchanges the per-destination counts and then the tuples of each relation
+    with one all-to-all each (NCCL over NVLink), and joins what it received with
+    its own plan. Rank d's output holds the pairs of the keys whose destination
+    is d; the union over the ranks is the join of the union of the shards.
+
+    `split(T) -> (grouped, counts)` and `join(R, S) -> (pairs, n)` replace the
+    device split and the local join; the CPU tests of the exchange protocol pass
+    host versions of both and run gloo ranks."""
+
+    def __init__(self, group=None, design=None, split=None, join=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+        self.world = dist.get_world_size(group)
+        self.design = design if design is not None else make_design()
+        self._split = split if split is not None else self._device_split
+        self._join = join if join is not None else self._device_join
+        self._plans = {}
+
+    def _device_split(self, T):
+        import torch
+        out = torch.empty_like(T)
+        cnt = torch.empty(2 * self.world, dtype=torch.int64, device=T.device)
+        check(lib().spj_exchange_split(T.data_ptr(), T.shape[0], self.world, out.data_ptr(), cnt.data_ptr(),
+                                       torch.cuda.current_stream().cuda_stream))
+        return out, cnt[:self.world]
+
+    def _device_join(self, R, S):
+        import torch
+        key = (R.shape[0], S.shape[0])
+        if key not in self._plans:
+            for p in self._plans.values():
+                p.close()
+            self._plans = {key: Plan(key[0], key[1], self.design)}
+        plan = self._plans[key]
+        out = torch.empty((plan.output_capacity, 2), dtype=torch.int32, device=R.device)
+        n = torch.zeros(1, dtype=torch.int64, device=R.device)
+        pad = torch.zeros((1, 2), dtype=torch.int32, device=R.device)
+        r = R if R.shape[0] else pad
+        s = S if S.shape[0] else pad
+        plan.execute(r.data_ptr(), s.data_ptr(), out.data_ptr(), n.data_ptr(),
+                     torch.cuda.current_stream().cuda_stream)
+        return out, n
+
+    def exchange(self, T):
+        """Splits the (n, 2) int32 tuples T by destination rank and exchanges
+        them; returns the tuples this rank receives."""
+        import torch
+        grouped, cnt = self._split(T)
+        recv_cnt = torch.empty_like(cnt)
+        self.dist.all_to_all_single(recv_cnt, cnt, group=self.group)
+        send, recv = [int(x) for x in cnt.tolist()], [int(x) for x in recv_cnt.tolist()]
+        got = torch.empty((sum(recv), 2), dtype=T.dtype, device=T.device)
+        src = grouped[:sum(send)].contiguous().view(torch.int64).view(-1)
+        self.dist.all_to_all_single(got.view(torch.int64).view(-1), src, output_split_sizes=recv,
+                                    input_split_sizes=send, group=self.group)
+        return got
+
+    def run(self, R, S):
+        """R, S: this rank's shards, (n, 2) int32 tensors (key, payload) on this
+        rank's device. Returns (pairs, n): this rank's part of the join."""
+        return self._join(self.exchange(R), self.exchange(S))
+
+    def close(self):
+        for p in self._plans.values():
+            p.close()
+        self._plans = {}

@@ -1,0 +1,101 @@
+"""The multi-GPU join's exchange protocol on CPU: two and three gloo ranks run
+spidjoin.DistributedJoin with host stand-ins for the device split and the local
+join (the oracle's hash and join -- test scaffolding only), and the union of the
+ranks' outputs must equal the join of the union of the shards. Every rank must
+receive exactly the keys whose destination it is."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _dest(keys, world):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    h = oracle.glb_partition_hash_np(keys).astype(np.uint64)
+    return ((h * np.uint64(world)) >> np.uint64(32)).astype(np.int64)
+
+
+def _dataset(seed, n_r, n_s, world):
+    rng = np.random.default_rng(seed)
+    keys = rng.permutation(n_r).astype(np.uint32) + 1
+    R = np.stack([keys, np.arange(n_r, dtype=np.uint32)], axis=1)
+    sk = keys[rng.integers(0, n_r, n_s)]
+    sk[rng.random(n_s) < 0.05] = 0                       # padding
+    miss = rng.random(n_s) < 0.05
+    sk[miss] = (n_r + 1 + rng.integers(0, 1000, int(miss.sum()))).astype(np.uint32)  # no partner
+    S = np.stack([sk, np.arange(n_s, dtype=np.uint32)], axis=1)
+    return R, S
+
+
+def _rank_main(rank, world, port, seed, out_q):
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(ROOT, "spid-join_b200"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import spidjoin
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        R, S = _dataset(seed, 5000, 20000, world)
+        # uneven shards: rank i holds a contiguous slice of each relation
+        rb = np.linspace(0, R.shape[0], world + 1).astype(int)
+        sb = (np.linspace(0, 1, world + 1) ** 1.5 * S.shape[0]).astype(int)
+        myR, myS = R[rb[rank]:rb[rank + 1]], S[sb[rank]:sb[rank + 1]]
+
+        def split(T):
+            a = T.numpy().view(np.uint32).reshape(-1, 2)
+            a = a[a[:, 0] != 0]
+            d = _dest(a[:, 0], world)
+            order = np.argsort(d, kind="stable")
+            counts = np.bincount(d, minlength=world).astype(np.int64)
+            return torch.from_numpy(a[order].view(np.int32).copy()), torch.from_numpy(counts)
+
+        received = {}
+
+        def join(Rr, Sr):
+            received["R"], received["S"] = Rr.numpy().view(np.uint32), Sr.numpy().view(np.uint32)
+            out = oracle.simple_join(received["R"], received["S"])
+            return torch.from_numpy(out.view(np.int32).copy()), torch.tensor([out.shape[0]])
+
+        dj = spidjoin.DistributedJoin(split=split, join=join)
+        pairs, n = dj.run(torch.from_numpy(myR.view(np.int32).copy()), torch.from_numpy(myS.view(np.int32).copy()))
+        ok_dest = all(bool(np.all(_dest(received[x][:, 0], world) == rank)) for x in ("R", "S"))
+        out_q.put((rank, pairs[:int(n[0])].numpy().view(np.uint32).copy(), ok_dest,
+                   received["R"].shape[0], received["S"].shape[0]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_exchange_then_local_joins_equal_global_join(oracle, world):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, 7, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=240) for _ in range(world)]
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    R, S = _dataset(7, 5000, 20000, world)
+    want = oracle.sort_pairs(oracle.simple_join(R, S))
+    got = oracle.sort_pairs(np.concatenate([r[1] for r in res]))
+    assert np.array_equal(got, want)
+    assert all(r[2] for r in res), "a rank received keys of another destination"
+    assert sum(r[3] for r in res) == int((R[:, 0] != 0).sum())
+    assert sum(r[4] for r in res) == int((S[:, 0] != 0).sum())

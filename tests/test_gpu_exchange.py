@@ -1,0 +1,62 @@
+"""GPU tests of the multi-GPU join's pieces that one GPU can run: the device
+split by destination rank (spj_exchange_split) against the oracle's hash, and
+DistributedJoin end to end on a one-rank NCCL group."""
+import socket
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _dest(oracle, keys, world):
+    h = oracle.glb_partition_hash_np(keys).astype(np.uint64)
+    return ((h * np.uint64(world)) >> np.uint64(32)).astype(np.int64)
+
+
+@pytest.mark.parametrize("world", [1, 2, 5, 8, 1024])
+def test_exchange_split_groups_by_destination(spj, oracle, world):
+    import torch
+    n_r, n_s = 1 << 16, (1 << 20) + 3
+    R, S, _ = spj.generate_host(n_r, n_s, 1.2, seed=5)
+    S = S.copy()
+    S[::97, 0] = 0  # padding is dropped
+    dS = torch.from_numpy(S.view(np.int32)).cuda()
+    out = torch.empty_like(dS)
+    cnt = torch.empty(2 * world, dtype=torch.int64, device="cuda")
+    spj.check(spj.lib().spj_exchange_split(dS.data_ptr(), n_s, world, out.data_ptr(), cnt.data_ptr(), None))
+    torch.cuda.synchronize()
+    counts = cnt[:world].cpu().numpy()
+    keep = S[S[:, 0] != 0]
+    d = _dest(oracle, keep[:, 0], world)
+    assert np.array_equal(counts, np.bincount(d, minlength=world))
+    got = out.cpu().numpy().view(np.uint32)[:keep.shape[0]]
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for r in range(world):
+        seg = got[off[r]:off[r + 1]]
+        assert np.all(_dest(oracle, seg[:, 0], world) == r)
+        assert np.array_equal(oracle.sort_pairs(seg), oracle.sort_pairs(keep[d == r]))
+
+
+def test_distributed_join_one_rank(spj, oracle):
+    import torch
+    import torch.distributed as dist
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        n_r, n_s = 1 << 18, 1 << 20
+        R, S, expect = spj.generate_host(n_r, n_s, 1.0, seed=9)
+        dj = spj.DistributedJoin(design=spj.make_design(rank_num=1))
+        dR = torch.from_numpy(R.view(np.int32)).cuda()
+        dS = torch.from_numpy(S.view(np.int32)).cuda()
+        for _ in range(2):
+            pairs, n = dj.run(dR, dS)
+            torch.cuda.synchronize()
+            got = pairs[:int(n.item())].cpu().numpy().view(np.uint32)
+            assert got.shape == (n_s, 2)
+            assert oracle.checksum(got) == expect
+        dj.close()
+    finally:
+        dist.destroy_process_group()
