@@ -33,12 +33,24 @@ WORKLOADS = {
            "plain equi-join |R|=2^27 |S|=2^29 Zipf 1.0, replication groups of 4 (-r 4 -R 4 -B 1)"),
     "c3": (1 << 26, 1 << 29, 1.5, (4, 4, 1), "plain equi-join |R|=2^26 |S|=2^29 Zipf 1.5, groups of 4"),
     "c2u": (1 << 27, 1 << 29, 0.0, (4, 4, 1), "plain equi-join |R|=2^27 |S|=2^29 uniform, groups of 4"),
+    "c2z": (1 << 27, 1 << 29, 1.5, (4, 4, 1), "plain equi-join |R|=2^27 |S|=2^29 Zipf 1.5, groups of 4"),
+    "c3u": (1 << 26, 1 << 29, 0.0, (4, 4, 1), "plain equi-join |R|=2^26 |S|=2^29 uniform, groups of 4"),
     # 1/8 of C2 (same Zipf and layout): the small case for ncu captures
     "c2s": (1 << 24, 1 << 26, 1.0, (4, 4, 1), "plain equi-join |R|=2^24 |S|=2^26 Zipf 1.0, groups of 4"),
 }
 SEED = 0x5EED5EED
 METRIC = "join tuples/s (|R|+|S|)"
 CPU_SAMPLE_DIV = 32   # the CPU legs run |R|/32, |S|/32 of the same workload
+
+
+def launches_per_join(alg, radix_bits, single=True):
+    """Kernels of this library one plan execution launches (see launch_pipeline):
+    k_init_single for a single-join plan; the non-partitioned join has no
+    partitioning passes; a second scatter pass (and its work list) above 8 radix bits."""
+    n = 1 if single else 0
+    if alg == 1:
+        return n + 8
+    return n + 10 + (2 if radix_bits > 8 else 0)
 
 
 def peaks():
@@ -346,7 +358,7 @@ def run_ours(args):
                                   "algorithmic_bytes": pipe_bytes, "formula": "24*(|R|+|S|) + 8*|out|"},
             "kernels_ms": kmean,
             "e2e": e2e, "cpu_baseline": cpu,
-            "gpu_launches": 8 * args.steps,
+            "gpu_launches": launches_per_join(args.alg, st["radix_bits"]) * args.steps,
             "clocks": clocks,
             "check": {"n_pairs": n_pairs, "checksum_ok": ok, "max_s_partition": st["max_s_partition"],
                       "units": st["units"]},
@@ -465,7 +477,8 @@ def run_distributed(args):
                                   "frac": pipe_bytes / ws / (ms_step / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
                                   "formula": "per rank: 24*(|R|+|S|) + 8*|out|, exchange not counted"},
             "max_local_pairs": local_out.item(),
-            "e2e": e2e, "cpu_baseline": None, "gpu_launches": 24 * args.steps, "clocks": clocks,
+            "e2e": e2e, "cpu_baseline": None, "gpu_launches": (6 + launches_per_join(args.alg, 15)) * args.steps,
+            "clocks": clocks,
             "check": {"global_checksum_ok": True, "pairs": int(tot[2].item())},
         })
     dist.destroy_process_group()
@@ -585,7 +598,8 @@ def run_batched(args):
         "batched_vs_plain": plain_ms / ms_batched,
         "pipeline_roofline": {"achieved": pipe_bytes / (ms_batched / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                               "frac": pipe_bytes / (ms_batched / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
-        "gpu_launches": 14 * args.steps, "clocks": clocks, "kernels_ms_eager": kmean,
+        "gpu_launches": launches_per_join(args.alg, 15, single=False) * args.steps, "clocks": clocks,
+        "kernels_ms_eager": kmean,
         "check": {"joins_checked": J, "all_exact": True},
     })
     return 0
@@ -764,7 +778,7 @@ def run_served(args):
         "served": served, "saturated": sat, "plain": plain, "plain_saturated": plain_sat,
         "served_vs_plain_saturated": sat["tuples_per_s"] / plain_sat["tuples_per_s"],
         "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
-        "gpu_launches": 14 * served["batches"], "clocks": clocks,
+        "gpu_launches": launches_per_join(args.alg, 15, single=False) * served["batches"], "clocks": clocks,
         "check": {"outputs_checked": served["requests"] + sat["requests"] + plain["requests"] +
                   plain_sat["requests"], "all_exact": True,
                   "how": "count and 64-bit checksum of every output against the generator's"},
@@ -796,7 +810,14 @@ def main():
     ap.add_argument("--sharded", action="store_true", help="the sharded join even on one GPU (exchange with itself)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--nr", type=int, default=0, help="custom workload: |R| (with --ns, --zipf)")
+    ap.add_argument("--ns", type=int, default=0)
+    ap.add_argument("--zipf", type=float, default=0.0)
     args = ap.parse_args()
+    if args.nr > 0:
+        WORKLOADS["custom"] = (args.nr, args.ns, args.zipf, (1, 1, 1),
+                               f"plain equi-join |R|={args.nr} |S|={args.ns} Zipf {args.zipf:g}")
+        args.workload = "custom"
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "c4":
