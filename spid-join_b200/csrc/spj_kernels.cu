@@ -226,7 +226,7 @@ struct __align__(128) TileSmem {
 // flight while this one is sorted and written. A tuple at an odd boundary index
 // is moved with an ordinary load (bulk copies need 16-byte alignment).
 // Returns false (the same value in every thread) when a bulk copy timed out.
-template <typename BucketFn>
+template <bool kHot, typename BucketFn>
 __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint32_t b, uint32_t e,
                                               Tuple *__restrict__ out, TileSmem &S, int nb, BucketFn bucket_of,
                                               uint32_t (&uses)[2], unsigned int *err) {
@@ -274,15 +274,25 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
         }
         Tuple v[PER];
         uint32_t br[PER];  // bucket << 16 | rank inside the tile; 0xffff0000 = no tuple
+        // Rank. In a hot run (kHot: a pass-2 segment of one heavy chunk, where a
+        // hot key puts most tuples in one bucket) a warp whose 32 tuples share a
+        // bucket takes its 32 ranks with one counter increment instead of 32
+        // serialised ones; elsewhere the check would only cost time.
 #pragma unroll
         for (int k = 0; k < PER; k++) {
             const uint32_t idx = threadIdx.x + k * kScatterThreads;
-            br[k] = 0xffff0000u;
             v[k] = idx < nt ? S.inbuf[buf][idx] : Tuple{0u, 0u};
-            if (v[k].key) {
-                const uint32_t bk = (uint32_t)bucket_of(v[k].key);
-                br[k] = (bk << 16) | atomicAdd(&S.cnt[bk], 1u);
+            const uint32_t bk = v[k].key ? (uint32_t)bucket_of(v[k].key) : 0xffffu;
+            if (kHot) {
+                const uint32_t b0 = __shfl_sync(0xffffffffu, bk, 0);
+                if (__all_sync(0xffffffffu, bk == b0) && b0 != 0xffffu) {
+                    uint32_t base = 0;
+                    if ((threadIdx.x & 31) == 0) base = atomicAdd(&S.cnt[b0], 32u);
+                    br[k] = (b0 << 16) | (__shfl_sync(0xffffffffu, base, 0) + (threadIdx.x & 31));
+                    continue;
+                }
             }
+            br[k] = bk != 0xffffu ? (bk << 16) | atomicAdd(&S.cnt[bk], 1u) : 0xffff0000u;
         }
         __syncthreads();
         if (threadIdx.x < 32) {  // exclusive scan of the <= 256 bucket counts
@@ -388,7 +398,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
     const uint32_t e0 = min(R.n, b0 + R.chunk);
     Tuple *dst = b2 ? R.tmp : R.out;
     uint32_t uses[2] = {0, 0};
-    scatter_range(R.in, b0, e0, dst, S, nb,
+    scatter_range<false>(R.in, b0, e0, dst, S, nb,
                   [=](uint32_t key) { return (int)((glb_partition_hash(key) & mask) >> b2); }, uses,
                   &J.ctr->error);
 }
@@ -433,8 +443,10 @@ __global__ void k_items(PlanDev P) {
         const bool tail = c + 1 == nch && !cross && cum > cum_start;
         if (cross || tail) {
             const unsigned i = atomicAdd(&P.bctr->item_count, 1u);
+            // a run of one chunk holding a whole item's worth is a hot key's segment
+            const bool hot = start_b + 1 == (int)c && cnt >= T;
             if (i < P.max_items)
-                P.items[i] = make_uint4(r, cb, (uint32_t)(start_b + 1), c + 1);
+                P.items[i] = make_uint4(r | (hot ? 0x80000000u : 0u), cb, (uint32_t)(start_b + 1), c + 1);
             else
                 atomicOr(&J.ctr->error, 4u);
         }
@@ -466,7 +478,8 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
         const unsigned it = S.item;
         if (it >= n_items) break;
         const uint4 item = P.items[it];
-        const RelDev R = P.rel[item.x];
+        const bool hot = (item.x >> 31) != 0;
+        const RelDev R = P.rel[item.x & 0x7fffffffu];
         const JoinDev &J = P.join[R.join];
         const int b2 = J.fine_bits;
         const uint32_t F = 1u << J.bits;
@@ -487,9 +500,9 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
         if (mine_cnt) atomicAdd(&S.seg_len, mine_cnt);
         __syncthreads();
         const uint32_t beg = R.base[cb << b2] + S.seg_begin;
-        const bool ok = scatter_range(R.tmp, beg, beg + S.seg_len, R.out, S, nb,
-                                      [=](uint32_t key) { return (int)(glb_partition_hash(key) & qmask); }, uses,
-                                      &J.ctr->error);
+        auto fine = [=](uint32_t key) { return (int)(glb_partition_hash(key) & qmask); };
+        const bool ok = hot ? scatter_range<true>(R.tmp, beg, beg + S.seg_len, R.out, S, nb, fine, uses, &J.ctr->error)
+                            : scatter_range<false>(R.tmp, beg, beg + S.seg_len, R.out, S, nb, fine, uses, &J.ctr->error);
         __syncthreads();
         if (!ok) break;
     }
