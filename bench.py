@@ -510,6 +510,10 @@ def run_batched(args):
     tot = sum(a + b for a, b, _ in specs)
     lib = spj.lib()
     design = spj.make_design(rank_num=1, join_alg=args.alg, skew_mode=args.skew)
+    tuning = None
+    if args.tuning and os.path.exists(args.tuning):
+        spj.load_tuning(args.tuning)  # the autotuner's per-class table (spid-join_b200/autotune.py)
+        tuning = os.path.relpath(args.tuning, ROOT)
     R, S, exp = [], [], []
     for i, (n_r, n_s, z) in enumerate(specs):
         dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
@@ -591,7 +595,7 @@ def run_batched(args):
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": f"batched: {J} joins, |R| log-uniform [2^12, 2^24], R:S in {{1,2,4,8}}, "
                                f"Zipf s ~ U[0, 1.5], one seed; one CUDA graph per step",
-                   "joins": J, "tuples": tot, "join_alg": args.alg, "scale": args.c4_scale,
+                   "joins": J, "tuples": tot, "join_alg": args.alg, "scale": args.c4_scale, "tuning": tuning,
                    "l2": "inputs larger than L2; no flush"},
         "plain": {"value": tot / (plain_ms / 1e3), "ms_per_step": plain_ms,
                   "how": "one pre-created plan per join, CUDA-event device time per execution, summed"},
@@ -799,6 +803,8 @@ def main():
     ap.add_argument("--slots", type=int, default=0, help="table slots per CTA (0 = planner)")
     ap.add_argument("--unit", type=int, default=0, help="max S tuples per work unit (0 = planner)")
     ap.add_argument("--c4-scale", type=float, default=1.0, help="scale of the config-4 relation sizes")
+    ap.add_argument("--tuning", default=os.path.join(ROOT, "spid-join_b200", "tuning_b200.json"),
+                    help="batched workload: autotuner table to install ('' = the planner alone)")
     ap.add_argument("--c5-rate", type=float, default=2000.0, help="served stream: arrivals per second")
     ap.add_argument("--c5-seconds", type=float, default=60.0, help="served stream: duration")
     ap.add_argument("--c5-plain-seconds", type=float, default=15.0, help="plain per-request stream: duration")

@@ -14,6 +14,8 @@
 #define PIDJOIN_HPP
 
 #include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
 #include <time.h>
 
 #include <stdexcept>
@@ -142,13 +144,25 @@ public:
         check(spj_start(h_, &d), "StartJoin");
     }
 
-    // Per-rank pair buffers (host memory owned by the instance) and byte sizes.
-    ResultBuffers_t FinishJoin() {
+    // Per-rank pair buffers and their byte sizes. By default the buffers are
+    // slices of host memory owned by the instance (valid until the next
+    // StartJoin). With caller_owned, each rank's pairs are copied into its own
+    // aligned_alloc'd buffer that the caller releases with free(), as the
+    // reference hands out its result buffers (src/queryHostFunc.cc:1089).
+    ResultBuffers_t FinishJoin(bool caller_owned = false) {
         check(spj_finish(h_, &last_), "FinishJoin");
         ResultBuffers_t out;
         for (int r = 0; r < last_.num_rank; r++) {
-            out.first.push_back(const_cast<kv_pair_t *>(last_.pairs) + last_.rank_offsets[r]);
-            out.second.push_back(8 * (last_.rank_offsets[r + 1] - last_.rank_offsets[r]));
+            const int64_t bytes = 8 * (last_.rank_offsets[r + 1] - last_.rank_offsets[r]);
+            kv_pair_t *src = const_cast<kv_pair_t *>(last_.pairs) + last_.rank_offsets[r];
+            if (caller_owned) {
+                kv_pair_t *dst = (kv_pair_t *)aligned_alloc(64, (size_t)((bytes + 63) / 64 * 64 + 64));
+                if (!dst) throw Error(SPJ_E_NOMEM, "FinishJoin: result buffer allocation failed");
+                memcpy(dst, src, (size_t)bytes);
+                src = dst;
+            }
+            out.first.push_back(src);
+            out.second.push_back(bytes);
         }
         return out;
     }

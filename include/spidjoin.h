@@ -177,6 +177,28 @@ int spj_plan_kernel_times(spj_plan_t *plan, int back, spj_kernel_times_t *out);
 
 void spj_plan_destroy(spj_plan_t *plan);
 
+/* -------------------------------------------------------------- autotuning --
+ * A per-size-class tuning table that the planner applies to the knobs a design
+ * leaves at 0 (automatic) for the joins of a batch (a plan of two or more joins,
+ * including the server's batches); a join planned alone keeps the planner's
+ * choice. No counterpart in the reference, whose partition counts follow fixed
+ * formulas.
+ * A class is (floor(log2 |R|), floor(log2(|S| / |R|)) clamped to [0, 6]);
+ * radix_bits_delta offsets the planner's fan-out, table_slots and unit_tuples
+ * replace its choices when non-zero. The table is filled by the autotuner
+ * (spidjoin.autotune, which times candidates per class on the device) and is
+ * process-wide; spj_tuning_set replaces it (n = 0 clears it). */
+typedef struct {
+    int log2_r, log2_ratio;
+    int radix_bits_delta; /* -4..4 */
+    int table_slots;      /* 0 = planner */
+    int unit_tuples;      /* 0 = planner */
+    int reserved[3];
+} spj_tuning_t;
+int spj_tuning_set(const spj_tuning_t *entries, int n);
+/* Copies up to `capacity` entries; returns the table's size. */
+int spj_tuning_get(spj_tuning_t *entries, int capacity);
+
 /* ------------------------------------------------------------------ batches --
  * Many joins of uneven sizes and skew in one launch sequence: the kernels of a
  * batch plan cover every join, and one persistent work queue of

@@ -43,14 +43,15 @@ int main(int argc, char **argv) {
     d.foreign_key = "l";
     std::string alg = "phj";
     int reps = 1;
+    bool owned = false;  // -o: result buffers owned by the caller, as the reference hands them out
     uint64_t seed = 0x5EED5EEDull;
     if (argc < 2) {
         fprintf(stderr, "usage: %s -s |R| [-r ranks] [-z zipf*100] [-t |S|/|R|] [-R rank_set] [-B bank_set] "
-                        "[-a phj|nphj|smj|nl] [-n reps] [-S seed]\n", argv[0]);
+                        "[-a phj|nphj|smj|nl] [-n reps] [-S seed] [-o]\n", argv[0]);
         return 0;
     }
     int opt;
-    while ((opt = getopt(argc, argv, "s:r:z:t:R:B:h:p:f:a:n:S:")) != -1) {
+    while ((opt = getopt(argc, argv, "s:r:z:t:R:B:h:p:f:a:n:S:o")) != -1) {
         switch (opt) {
             case 's': d.input_size = atoll(optarg); break;
             case 'r': d.rank_num = atoi(optarg); break;
@@ -61,6 +62,7 @@ int main(int argc, char **argv) {
             case 'a': alg = optarg; break;
             case 'n': reps = atoi(optarg); break;
             case 'S': seed = strtoull(optarg, nullptr, 0); break;
+            case 'o': owned = true; break;
             default: break;
         }
     }
@@ -100,7 +102,7 @@ int main(int argc, char **argv) {
             struct timespec start;
             clock_gettime(CLOCK_MONOTONIC, &start);
             join_instance.StartJoin(d);
-            ResultBuffers_t res = join_instance.FinishJoin();
+            ResultBuffers_t res = join_instance.FinishJoin(owned);
             join_instance.RecordLogs(start, 0);
             int64_t n = 0;
             uint64_t sum = 0;
@@ -112,6 +114,8 @@ int main(int argc, char **argv) {
             printf("check: %s pairs=%lld expected=%lld checksum=%016llx expected=%016llx\n", ok ? "ok" : "MISMATCH",
                    (long long)n, (long long)n_s, (unsigned long long)sum, (unsigned long long)expect);
             bad += !ok;
+            if (owned)
+                for (auto *p : res.first) free(p);
         }
         return bad ? 1 : 0;
     } catch (const Error &e) {

@@ -137,6 +137,7 @@ struct JoinShape {
     uint32_t nchunks[2] = {1, 1}, chunk[2] = {2, 2};
     uint32_t item_target = 0;
     uint32_t out_chunk = kOutChunk;
+    uint32_t unit_tuples = kDefaultUnitTuples;
     unsigned long long gtable_slots = 0;
 };
 
@@ -169,8 +170,10 @@ int set_error(int code, const std::string &msg);
 int cuda_error(cudaError_t e, const char *what);
 
 // batch_tuples: all tuples of the plan's joins when the join is one of many (0 alone)
+// tune: the autotuner's entry for this size class, or null
 JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots, bool alone,
-                     int64_t batch_tuples);
+                     int64_t batch_tuples, const spj_tuning_t *tune);
+const spj_tuning_t *find_tuning(int64_t n_r, int64_t n_s, spj_tuning_t *out);
 // Computes the arena layout of pl->joins/pl->shapes (arena == nullptr: size only)
 // and fills pl->dev, the per-join descriptors and the host image of the
 // descriptor arrays.

@@ -125,7 +125,7 @@ extern "C" int spj_join_noalloc(const spj_kv_pair_t *r, int64_t n_r, const spj_k
     pl.shapes.resize(1);
     pl.joins[0].n_r = n_r;
     pl.joins[0].n_s = n_s;
-    JoinShape sh = plan_shape(n_r, n_s, pl.design, ds->sms, ds->table_slots_max, true, 0);
+    JoinShape sh = plan_shape(n_r, n_s, pl.design, ds->sms, ds->table_slots_max, true, 0, nullptr);
     sh.bits = std::min(std::max(ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + 4095) / 4096)), 6), kMaxPassBits);
     sh.fine_bits = 0;
     {

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -80,12 +81,42 @@ static int max_table_slots(int dev) {
     return ((max_smem - 4096) / 8) & ~1;
 }
 
+// ------------------------------------------------------------------ tuning --
+// The autotuner's per-size-class table (spj_tuning_set): a class is
+// (floor(log2 |R|), floor(log2(|S| / |R|)) clamped to [0, 6]).
+static std::mutex g_tuning_mu;
+static std::vector<spj_tuning_t> g_tuning;
+
+static int log2_floor(uint64_t v) {
+    int b = 0;
+    while (v > 1) {
+        v >>= 1;
+        b++;
+    }
+    return b;
+}
+
+const spj_tuning_t *find_tuning(int64_t n_r, int64_t n_s, spj_tuning_t *out) {
+    const int lr = log2_floor((uint64_t)std::max<int64_t>(1, n_r));
+    const int lt = std::min(6, log2_floor((uint64_t)std::max<int64_t>(1, n_s / std::max<int64_t>(1, n_r))));
+    std::lock_guard<std::mutex> lk(g_tuning_mu);
+    for (const auto &t : g_tuning)
+        if (t.log2_r == lr && t.log2_ratio == lt) {
+            *out = t;
+            return out;
+        }
+    return nullptr;
+}
+
 // Per-join tuning: the planner's choice for these sizes (size classes follow
 // from the formulas: fan-out from |R|, chunking from |R|+|S|).
 JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots, bool alone,
-                     int64_t batch_tuples) {
+                     int64_t batch_tuples, const spj_tuning_t *tune) {
     JoinShape sh;
-    int ts = d.table_slots > 0 ? std::min(d.table_slots, max_slots) : kDefaultTableSlots;
+    const bool tuned_ts = d.table_slots <= 0 && tune && tune->table_slots > 0;
+    int ts = d.table_slots > 0 ? std::min(d.table_slots, max_slots)
+             : tuned_ts        ? std::min(tune->table_slots, max_slots)
+                               : kDefaultTableSlots;
     if (d.join_alg == SPJ_ALG_NPHJ) {
         sh.bits = 0;
         sh.fine_bits = 0;
@@ -105,9 +136,10 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
             const int need = ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + target - 1) / target));
             const int par = alone ? ceil_log2((uint64_t)8 * sms) : 0;
             const int minb = ceil_log2((uint64_t)64 * d.rank_num);
-            sh.bits = std::min(std::max(std::max(need, par), minb), kMaxRadixBits);
+            const int delta = tune ? tune->radix_bits_delta : 0;  // the autotuner's offset for this size class
+            sh.bits = std::min(std::max(std::max(std::max(need, par), minb) + delta, 1), kMaxRadixBits);
         }
-        if (d.table_slots <= 0) {
+        if (d.table_slots <= 0 && !tuned_ts) {
             // shrink the table to three times a generous bound on the largest partition
             const double mean = (double)n_r / (double)(1ull << sh.bits);
             const double bound = mean + 6.0 * sqrt(mean) + 32.0;
@@ -137,6 +169,9 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     uint32_t oc = 32;
     while (oc < (uint32_t)kOutChunk && (int64_t)oc * 8192 < n_s) oc <<= 1;
     sh.out_chunk = oc;
+    sh.unit_tuples = d.unit_tuples > 0                ? (uint32_t)d.unit_tuples
+                     : (tune && tune->unit_tuples > 0) ? (uint32_t)tune->unit_tuples
+                                                       : (uint32_t)kDefaultUnitTuples;
     return sh;
 }
 
@@ -177,7 +212,7 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
         jd.skew_mode = d.skew_mode;
         jd.group = d.rank_set * d.bank_set;
         jd.keep_unmatched = (d.join_alg == SPJ_ALG_SMJ || d.join_alg == SPJ_ALG_NL) ? 1 : 0;
-        jd.unit_tuples = d.unit_tuples > 0 ? (uint32_t)d.unit_tuples : (uint32_t)kDefaultUnitTuples;
+        jd.unit_tuples = sh.unit_tuples;
         jd.item_target = sh.item_target;
         jd.out_chunk = sh.out_chunk;
         jd.out_cap = (unsigned long long)h.n_s + (unsigned long long)warps * sh.out_chunk;
@@ -357,7 +392,9 @@ static int create_plan(int J, const int64_t *n_r, const int64_t *n_s, const spj_
     for (int j = 0; j < J; j++) {
         pl->joins[j].n_r = n_r[j];
         pl->joins[j].n_s = n_s[j];
-        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1, batch_tuples);
+        spj_tuning_t tn;
+        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1, batch_tuples,
+                                   J > 1 ? find_tuning(n_r[j], n_s[j], &tn) : nullptr);
         ts_max = std::max(ts_max, pl->shapes[j].table_slots);
     }
     int per_sm = 0;
@@ -430,7 +467,9 @@ int create_plan_stream(int J, const int64_t *n_r, const int64_t *n_s, const spj_
         JoinHost &h = pl->joins[j];
         h.n_r = n_r[j];
         h.n_s = n_s[j];
-        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1, batch_tuples);
+        spj_tuning_t tn;
+        pl->shapes[j] = plan_shape(n_r[j], n_s[j], *design, sms, maxts, J == 1, batch_tuples,
+                                   J > 1 ? find_tuning(n_r[j], n_s[j], &tn) : nullptr);
         ts_max = std::max(ts_max, pl->shapes[j].table_slots);
         h.rel[0].in = reinterpret_cast<const Tuple *>(r[j] ? r[j] : out[j]);
         h.rel[1].in = reinterpret_cast<const Tuple *>(s[j] ? s[j] : out[j]);
@@ -476,7 +515,9 @@ void destroy_plan_stream(spj_plan_t *pl, cudaStream_t st) {
 int64_t join_output_capacity(int64_t n_r, int64_t n_s, const spj_design_t &d, bool alone) {
     int sms = 0, dev = 0;
     if (device_sms(&sms, &dev)) return -1;
-    const JoinShape sh = plan_shape(n_r, n_s, d, sms, max_table_slots(dev), alone, 0);
+    spj_tuning_t tn;
+    const JoinShape sh = plan_shape(n_r, n_s, d, sms, max_table_slots(dev), alone, 0,
+                                    alone ? nullptr : find_tuning(n_r, n_s, &tn));
     const int per_sm = 2048 / kJoinThreads;
     const int blocks = std::min(per_sm * sms, kMaxHoles / (kJoinThreads / 32));
     return n_s + (int64_t)blocks * (kJoinThreads / 32) * sh.out_chunk;
@@ -710,3 +751,28 @@ namespace spj {
 // the calling thread's last error).
 int join_ctr_status(unsigned err, unsigned max_r_part) { return ctr_error(nullptr, err, max_r_part); }
 }  // namespace spj
+
+extern "C" {
+
+int spj_tuning_set(const spj_tuning_t *entries, int n) {
+    if (n < 0 || (n > 0 && !entries)) return set_error(SPJ_E_ARG, "bad tuning table");
+    for (int i = 0; i < n; i++) {
+        const spj_tuning_t &t = entries[i];
+        if (t.log2_r < 0 || t.log2_r > 32 || t.log2_ratio < 0 || t.log2_ratio > 6 || t.radix_bits_delta < -4 ||
+            t.radix_bits_delta > 4 || t.table_slots < 0 || t.unit_tuples < 0)
+            return set_error(SPJ_E_ARG, "tuning entry " + std::to_string(i) + " out of range");
+    }
+    std::lock_guard<std::mutex> lk(g_tuning_mu);
+    g_tuning.assign(entries, entries + n);
+    return SPJ_OK;
+}
+
+int spj_tuning_get(spj_tuning_t *entries, int capacity) {
+    std::lock_guard<std::mutex> lk(g_tuning_mu);
+    const int n = (int)g_tuning.size();
+    if (entries)
+        for (int i = 0; i < n && i < capacity; i++) entries[i] = g_tuning[i];
+    return n;
+}
+
+}  // extern "C"

@@ -34,6 +34,7 @@ EXPORTS = (
     "spj_batch_create", "spj_batch_output_capacity", "spj_batch_bind", "spj_batch_execute", "spj_batch_stats",
     "spj_server_create", "spj_server_output_capacity", "spj_server_submit", "spj_server_wait", "spj_server_stats",
     "spj_server_reset_stats", "spj_server_destroy", "spj_server_hold", "spj_exchange_split",
+    "spj_tuning_set", "spj_tuning_get",
 )
 
 
@@ -66,6 +67,11 @@ class Stats(ctypes.Structure):
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("log2_r", ctypes.c_int), ("log2_ratio", ctypes.c_int), ("radix_bits_delta", ctypes.c_int),
+                ("table_slots", ctypes.c_int), ("unit_tuples", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
 class ServerStats(ctypes.Structure):
@@ -141,6 +147,8 @@ def lib():
         L.spj_server_destroy.argtypes = [vp]
         L.spj_server_destroy.restype = None
         L.spj_exchange_split.argtypes = [vp, i64, i32, vp, vp, vp]
+        L.spj_tuning_set.argtypes = [ctypes.POINTER(Tuning), i32]
+        L.spj_tuning_get.argtypes = [ctypes.POINTER(Tuning), i32]
         _lib = L
     return _lib
 
@@ -462,3 +470,120 @@ class DistributedJoin:
         for p in self._plans.values():
             p.close()
         self._plans = {}
+
+
+# ------------------------------------------------------------- autotuning --
+TUNING_KEYS = ("log2_r", "log2_ratio", "radix_bits_delta", "table_slots", "unit_tuples")
+
+
+def set_tuning(entries):
+    """Installs the process-wide per-size-class tuning table (list of dicts with
+    TUNING_KEYS; [] clears it). Applies to joins planned in batches."""
+    arr = (Tuning * max(1, len(entries)))()
+    for i, e in enumerate(entries):
+        for k in TUNING_KEYS:
+            setattr(arr[i], k, int(e.get(k, 0)))
+    check(lib().spj_tuning_set(arr, len(entries)))
+
+
+def get_tuning():
+    n = lib().spj_tuning_get(None, 0)
+    arr = (Tuning * max(1, n))()
+    lib().spj_tuning_get(arr, n)
+    return [{k: getattr(arr[i], k) for k in TUNING_KEYS} for i in range(n)]
+
+
+def load_tuning(path):
+    import json
+    with open(path) as f:
+        t = json.load(f)
+    set_tuning(t["entries"])
+    return t
+
+
+def autotune(classes, zipf=1.0, reps=3, batch_tuples=1 << 26, max_joins=256, candidates=None, log=None):
+    """Autotuner of the batch planner: for every size class (log2|R|, log2(|S|/|R|))
+    it builds a batch of joins of that class (about `batch_tuples` tuples, from the
+    seeded device generator), times every candidate setting of the fan-out offset,
+    table size and work-unit size with CUDA events (a warm-up, then `reps` runs),
+    checks every join's count and checksum, and keeps the fastest. Returns the
+    table (the fields of spj_tuning_t plus the measured times); set_tuning()
+    installs it. Needs a GPU."""
+    import torch
+    set_tuning([])  # measure against the planner's own choices
+    if candidates is None:
+        # table sizes stay the planner's: in a mixed batch the largest table sets
+        # the shared memory (and so the CTAs per SM) of every join
+        candidates = [(dl, 0, ut) for dl in (0, -1, -2, 1) for ut in (0, 32768, 131072)]
+    table = []
+    for lr, lt in classes:
+        n_r = 1 << lr
+        n_s = n_r << lt
+        J = int(max(2, min(max_joins, batch_tuples // (n_r + n_s))))
+        R, S, exp = [], [], []
+        for j in range(J):
+            dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
+            dS = torch.empty((n_s, 2), dtype=torch.int32, device="cuda")
+            e = torch.zeros(1, dtype=torch.int64, device="cuda")
+            check(lib().spj_generate_device(0x7E57 + 7919 * j + 104729 * lr + 31 * lt, n_r, n_s, zipf,
+                                            dR.data_ptr(), dS.data_ptr(), e.data_ptr(), None))
+            R.append(dR)
+            S.append(dS)
+            exp.append(e)
+        exp = torch.cat(exp)
+        # planner's fan-out for this class (offset 0, automatic table and units)
+        probe = Batch([n_r] * J, [n_s] * J, make_design(rank_num=1))
+        outs = [torch.empty((probe.output_capacity(j), 2), dtype=torch.int32, device="cuda") for j in range(J)]
+        n_out = torch.zeros(J, dtype=torch.int64, device="cuda")
+        probe.bind([t.data_ptr() for t in R], [t.data_ptr() for t in S], [o.data_ptr() for o in outs],
+                   n_out.data_ptr())
+        probe.execute(0)
+        torch.cuda.synchronize()
+        base_bits = probe.stats(0)["radix_bits"]
+        probe.close()
+        del outs
+        sums = torch.zeros(J, dtype=torch.int64, device="cuda")
+        best, default_ms = None, None
+        for dl, ts, ut in candidates:
+            bits = base_bits + dl
+            if bits < 1 or bits > 15:
+                continue
+            design = make_design(rank_num=1, radix_bits=bits if dl else 0, table_slots=ts, unit_tuples=ut)
+            try:
+                b = Batch([n_r] * J, [n_s] * J, design)
+                outs = [torch.empty((b.output_capacity(j), 2), dtype=torch.int32, device="cuda") for j in range(J)]
+                n_out.zero_()
+                b.bind([t.data_ptr() for t in R], [t.data_ptr() for t in S], [o.data_ptr() for o in outs],
+                       n_out.data_ptr())
+                b.execute(0)
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record()
+                for _ in range(reps):
+                    b.execute(0)
+                ev1.record()
+                torch.cuda.synchronize()
+                ms = ev0.elapsed_time(ev1) / reps
+                for j in range(J):
+                    check(lib().spj_checksum_device(outs[j].data_ptr(), n_out[j:j + 1].data_ptr(),
+                                                    sums[j:j + 1].data_ptr(), None))
+                ok = bool(((sums == exp) & (n_out == n_s)).all().item())
+                for j in range(J):
+                    b.stats(j)  # raises on a capacity error
+                b.close()
+                del outs
+            except SpjError:
+                continue
+            if not ok:
+                raise SpjError(-5, f"autotune candidate {(dl, ts, ut)} gave a wrong result for class {(lr, lt)}")
+            if (dl, ts, ut) == (0, 0, 0):
+                default_ms = ms
+            if best is None or ms < best[0]:
+                best = (ms, dl, ts, ut)
+        entry = {"log2_r": lr, "log2_ratio": lt, "radix_bits_delta": best[1], "table_slots": best[2],
+                 "unit_tuples": best[3], "joins": J, "ms": best[0], "planner_ms": default_ms}
+        if log:
+            log(entry)
+        table.append(entry)
+        del R, S
+        torch.cuda.empty_cache()
+    return table

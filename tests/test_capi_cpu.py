@@ -87,3 +87,17 @@ def test_cli_without_gpu_fails_loudly():
     p = subprocess.run([cli, "-s", "1024", "-t", "2", "-z", "0", "-r", "1", "-R", "1", "-B", "1"],
                        capture_output=True, text=True, timeout=60)
     assert p.returncode == 2 and "no CUDA device" in p.stderr
+
+
+def test_tuning_table_roundtrip(spj):
+    entries = [{"log2_r": 20, "log2_ratio": 1, "radix_bits_delta": -1, "table_slots": 8192, "unit_tuples": 0},
+               {"log2_r": 14, "log2_ratio": 3, "radix_bits_delta": 1, "table_slots": 0, "unit_tuples": 32768}]
+    spj.set_tuning(entries)
+    try:
+        assert spj.get_tuning() == entries
+        with pytest.raises(spj.SpjError, match="ARG"):
+            spj.set_tuning([{"log2_r": 20, "log2_ratio": 9}])
+        assert spj.get_tuning() == entries  # a rejected table leaves the old one
+    finally:
+        spj.set_tuning([])
+    assert spj.get_tuning() == []

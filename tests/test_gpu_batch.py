@@ -120,3 +120,19 @@ def test_batch_matches_plain_plans(spj, oracle):
         plain = out[:int(n.item())].cpu().numpy().view(np.uint32)
         plan.close()
         assert np.array_equal(oracle.sort_pairs(plain), oracle.sort_pairs(results[0][j]))
+
+
+def test_autotuned_batch_stays_exact(spj, oracle):
+    table = spj.autotune([(12, 1), (14, 0)], zipf=1.0, reps=1, batch_tuples=1 << 20, max_joins=8,
+                         candidates=[(0, 0, 0), (1, 0, 0), (-1, 0, 32768)])
+    assert len(table) == 2 and all(e["ms"] > 0 for e in table)
+    spj.set_tuning(table)
+    try:
+        specs = [(1 << 12, 1 << 13, 1.0), (1 << 14, 1 << 14, 0.5), (5000, 9000, 1.2)] * 2
+        R, S, exp = make_batch_inputs(spj, specs, seed0=900)
+        results, _ = run_batch(spj, specs, spj.make_design(rank_num=1), R, S, repeats=1)
+        for j, (n_r, n_s, _) in enumerate(specs):
+            assert results[0][j].shape == (n_s, 2)
+            assert oracle.checksum(results[0][j]) == exp[j] & (2**64 - 1)
+    finally:
+        spj.set_tuning([])

@@ -17,6 +17,7 @@ CLI = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 
     "-s 65536 -t 8 -z 150 -r 4 -R 1 -B 16 -a smj",
     "-s 65536 -t 2 -z 50 -r 2 -R 2 -B 1 -a nl",
     "-s 100000 -t 3 -z 0 -r 1 -R 1 -B 1 -a nphj -n 2",
+    "-s 200000 -t 2 -z 120 -r 4 -R 2 -B 1 -n 2 -o",  # result buffers owned (and freed) by the caller
 ])
 def test_cli_joins_and_verifies(args):
     p = subprocess.run([CLI] + args.split(), capture_output=True, text=True, timeout=300)
