@@ -296,6 +296,20 @@ int spj_join_noalloc(const spj_kv_pair_t *r, int64_t n_r, const spj_kv_pair_t *s
 int spj_exchange_split(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv_pair_t *out, int64_t *counts,
                        void *stream);
 
+/* The same exchange with the split fused into the send: spj_exchange_count gives
+ * the per-destination sizes (counts: device int64[world]); once every rank knows
+ * the size matrix, spj_exchange_scatter writes each non-padding tuple straight
+ * into its destination's receive buffer. dest_bufs: device array of `world`
+ * pointers to the ranks' receive buffers (peer memory mapped into this process,
+ * e.g. symmetric memory, written over NVLink); dest_offsets: device
+ * int64[world], where this rank's segment starts in each destination buffer;
+ * cursor: device int64[world] workspace. Allocates nothing, does not
+ * synchronise; the caller orders the receivers' reads after every sender's
+ * kernel (a cross-GPU barrier). */
+int spj_exchange_count(const spj_kv_pair_t *tuples, int64_t n, int world, int64_t *counts, void *stream);
+int spj_exchange_scatter(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv_pair_t *const *dest_bufs,
+                         const int64_t *dest_offsets, int64_t *cursor, void *stream);
+
 /* Histogram of glb_partition_hash(key) & (2^bits - 1) over a device column (key-0
  * tuples skipped): the B200 form of the global partition count kernel
  * (src/dpu/src/join/glb_partition_count.c:119-371, partition_type 0). hist is a

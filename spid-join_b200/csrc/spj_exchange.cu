@@ -4,9 +4,12 @@
 // The reference shuffles every relation between its DPU ranks through the host
 // (the rotate-and-stream all-to-all, src/queryHostFunc.cc:481-777, with
 // destinations from the global partition hash, glb_partition_packet.c:420-464).
-// Over NVLink the exchange is one all-to-all per relation; before it, each GPU
-// groups its shard by destination rank so that every destination's tuples are
-// one contiguous segment. The destination of a key is glb_partition_hash(key)
+// Over NVLink the exchange is either one all-to-all per relation after each GPU
+// has grouped its shard by destination rank (spj_exchange_split), or the split
+// itself writing every tuple straight into its destination GPU's receive buffer
+// through peer pointers (spj_exchange_scatter after spj_exchange_count): one
+// kernel that partitions and sends, with no staging copy and no separate
+// collective for the tuples. The destination of a key is glb_partition_hash(key)
 // scaled to the number of ranks (multiply-shift), which leaves its low bits --
 // the local partitions of the join that follows -- evenly spread on every rank.
 #include <cuda_runtime.h>
@@ -61,9 +64,13 @@ __global__ void k_split_offsets(const unsigned long long *counts, uint32_t world
 
 // Each block step takes a tile, counts it per destination, reserves one range
 // per destination with one atomic each and writes its tuples there, so a
-// destination's tuples from one tile leave as one run.
+// destination's tuples from one tile leave as one run. kPeers: destination d's
+// tuples go to dests[d] (another GPU's receive buffer, written over NVLink);
+// otherwise all go to `out`.
+template <bool kPeers>
 __global__ void __launch_bounds__(kSplitThreads) k_split_scatter(const Tuple *in, unsigned long long n, uint32_t world,
-                                                                 unsigned long long *cursor, Tuple *out) {
+                                                                 unsigned long long *cursor, Tuple *out,
+                                                                 Tuple *const *dests) {
     __shared__ uint32_t cnt[kMaxWorld];
     __shared__ unsigned long long base[kMaxWorld];
     constexpr int PER = kSplitTile / kSplitThreads;
@@ -89,7 +96,11 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_scatter(const Tuple *in
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < PER; k++)
-            if (dr[k] != 0xffffffffu) out[base[dr[k] >> 16] + (dr[k] & 0xffffu)] = v[k];
+            if (dr[k] != 0xffffffffu) {
+                const uint32_t d = dr[k] >> 16;
+                Tuple *dst = kPeers ? dests[d] : out;
+                dst[base[d] + (dr[k] & 0xffffu)] = v[k];
+            }
         __syncthreads();
     }
 }
@@ -118,10 +129,53 @@ int spj_exchange_split(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv
     if (n > 0) k_split_count<<<sms * 4, kSplitThreads, 0, st>>>(in, (unsigned long long)n, world, cnt);
     k_split_offsets<<<1, 32, 0, st>>>(cnt, world, cursor);
     if (n > 0)
-        k_split_scatter<<<sms * 4, kSplitThreads, 0, st>>>(in, (unsigned long long)n, world, cursor,
-                                                            reinterpret_cast<Tuple *>(out));
+        k_split_scatter<false><<<sms * 4, kSplitThreads, 0, st>>>(in, (unsigned long long)n, world, cursor,
+                                                                   reinterpret_cast<Tuple *>(out), nullptr);
     e = cudaGetLastError();
     return e ? cuda_error(e, "split kernels") : SPJ_OK;
+}
+
+static int exchange_device(int *sms) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(SPJ_E_NODEVICE, "no CUDA device available; libspidjoin has no CPU path");
+    }
+    return SPJ_OK;
+}
+
+int spj_exchange_count(const spj_kv_pair_t *tuples, int64_t n, int world, int64_t *counts, void *stream) {
+    if (world < 1 || world > kMaxWorld) return set_error(SPJ_E_ARG, "world must be in [1, 1024]");
+    if (n < 0 || (n > 0 && !tuples) || !counts) return set_error(SPJ_E_ARG, "bad count arguments");
+    int sms = 0, rc = exchange_device(&sms);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(counts, 0, (size_t)world * 8, st);
+    if (e == cudaSuccess && n > 0)
+        k_split_count<<<sms * 4, kSplitThreads, 0, st>>>(reinterpret_cast<const Tuple *>(tuples),
+                                                         (unsigned long long)n, world,
+                                                         reinterpret_cast<unsigned long long *>(counts));
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e ? cuda_error(e, "count kernel") : SPJ_OK;
+}
+
+int spj_exchange_scatter(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv_pair_t *const *dest_bufs,
+                         const int64_t *dest_offsets, int64_t *cursor, void *stream) {
+    if (world < 1 || world > kMaxWorld) return set_error(SPJ_E_ARG, "world must be in [1, 1024]");
+    if (n < 0 || (n > 0 && !tuples) || !dest_bufs || !dest_offsets || !cursor)
+        return set_error(SPJ_E_ARG, "bad scatter arguments");
+    int sms = 0, rc = exchange_device(&sms);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(cursor, dest_offsets, (size_t)world * 8, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && n > 0)
+        k_split_scatter<true><<<sms * 4, kSplitThreads, 0, st>>>(
+            reinterpret_cast<const Tuple *>(tuples), (unsigned long long)n, world,
+            reinterpret_cast<unsigned long long *>(cursor), nullptr, reinterpret_cast<Tuple *const *>(dest_bufs));
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e ? cuda_error(e, "exchange scatter kernel") : SPJ_OK;
 }
 
 }  // extern "C"

@@ -30,7 +30,7 @@ using namespace spj;
 namespace {
 constexpr int kMaxSlices = 16;
 constexpr int64_t kSliceMin = 1ll << 24;     // host S below this is joined in one piece
-constexpr int64_t kSliceTuples = 1ll << 26;  // target S tuples per slice
+constexpr int64_t kSliceTuples = 1ll << 25;  // target S tuples per slice
 }  // namespace
 
 struct spj_handle {

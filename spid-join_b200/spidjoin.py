@@ -34,7 +34,7 @@ EXPORTS = (
     "spj_batch_create", "spj_batch_output_capacity", "spj_batch_bind", "spj_batch_execute", "spj_batch_stats",
     "spj_server_create", "spj_server_output_capacity", "spj_server_submit", "spj_server_wait", "spj_server_stats",
     "spj_server_reset_stats", "spj_server_destroy", "spj_server_hold", "spj_exchange_split",
-    "spj_tuning_set", "spj_tuning_get",
+    "spj_tuning_set", "spj_tuning_get", "spj_exchange_count", "spj_exchange_scatter",
 )
 
 
@@ -147,6 +147,8 @@ def lib():
         L.spj_server_destroy.argtypes = [vp]
         L.spj_server_destroy.restype = None
         L.spj_exchange_split.argtypes = [vp, i64, i32, vp, vp, vp]
+        L.spj_exchange_count.argtypes = [vp, i64, i32, vp, vp]
+        L.spj_exchange_scatter.argtypes = [vp, i64, i32, vp, vp, vp, vp]
         L.spj_tuning_set.argtypes = [ctypes.POINTER(Tuning), i32]
         L.spj_tuning_get.argtypes = [ctypes.POINTER(Tuning), i32]
         _lib = L
@@ -398,6 +400,19 @@ class Server:
             pass
 
 
+def exchange_layout(C, me):
+    """The receive layout of one exchange from the send-count matrix C
+    (C[src][dst]: tuples rank src sends to rank dst): this rank's receive count,
+    where its segment starts in every destination's buffer (the senders with a
+    lower rank come first), and the largest receive count of any rank (the
+    receive buffers' common size)."""
+    world = len(C)
+    recv = sum(int(C[s][me]) for s in range(world))
+    off = [sum(int(C[s][d]) for s in range(me)) for d in range(world)]
+    need = max(sum(int(C[s][d]) for s in range(world)) for d in range(world))
+    return recv, off, need
+
+
 class DistributedJoin:
     """A join of R and S sharded over the ranks of a torch.distributed process
     group, one GPU per rank: the multi-GPU form of the reference's rank-to-rank
@@ -412,15 +427,50 @@ class DistributedJoin:
     device split and the local join; the CPU tests of the exchange protocol pass
     host versions of both and run gloo ranks."""
 
-    def __init__(self, group=None, design=None, split=None, join=None):
+    def __init__(self, group=None, design=None, split=None, join=None, fused=False):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
         self.world = dist.get_world_size(group)
+        self.rank = dist.get_rank(group)
         self.design = design if design is not None else make_design()
         self._split = split if split is not None else self._device_split
         self._join = join if join is not None else self._device_join
+        self.fused = fused
         self._plans = {}
+        self._bufs = {}
+
+    def _fused_exchange(self, T, slot):
+        """The split fused into the send: each tuple is written straight into its
+        destination rank's receive buffer (symmetric memory, peer stores over
+        NVLink) by spj_exchange_scatter, after one all-gather of the size matrix;
+        cross-GPU barriers before (receivers are done with the last exchange) and
+        after (every sender is done)."""
+        import torch
+        import torch.distributed._symmetric_memory as symm
+        stream = torch.cuda.current_stream().cuda_stream
+        world = self.world
+        cnt = torch.empty(world, dtype=torch.int64, device=T.device)
+        check(lib().spj_exchange_count(T.data_ptr(), T.shape[0], world, cnt.data_ptr(), stream))
+        allc = torch.empty(world * world, dtype=torch.int64, device=T.device)
+        self.dist.all_gather_into_tensor(allc, cnt, group=self.group)
+        recv, off, need = exchange_layout(allc.view(world, world).tolist(), self.rank)
+        entry = self._bufs.get(slot)
+        if entry is None or entry[0].shape[0] < need:  # the same decision on every rank: the matrix is global
+            group = self.group if self.group is not None else self.dist.group.WORLD
+            buf = symm.empty((int(need * 1.25) + 1024, 2), dtype=torch.int32, device=T.device)
+            handle = symm.rendezvous(buf, group)
+            ptrs = torch.tensor(list(handle.buffer_ptrs), dtype=torch.int64, device=T.device)
+            entry = (buf, handle, ptrs)
+            self._bufs[slot] = entry
+        buf, handle, ptrs = entry
+        offs = torch.tensor(off, dtype=torch.int64, device=T.device)
+        cursor = torch.empty(world, dtype=torch.int64, device=T.device)
+        handle.barrier(channel=0, timeout_ms=60000)
+        check(lib().spj_exchange_scatter(T.data_ptr(), T.shape[0], world, ptrs.data_ptr(), offs.data_ptr(),
+                                         cursor.data_ptr(), stream))
+        handle.barrier(channel=0, timeout_ms=60000)
+        return buf[:recv]
 
     def _device_split(self, T):
         import torch
@@ -464,12 +514,15 @@ class DistributedJoin:
     def run(self, R, S):
         """R, S: this rank's shards, (n, 2) int32 tensors (key, payload) on this
         rank's device. Returns (pairs, n): this rank's part of the join."""
+        if self.fused:
+            return self._join(self._fused_exchange(R, "R"), self._fused_exchange(S, "S"))
         return self._join(self.exchange(R), self.exchange(S))
 
     def close(self):
         for p in self._plans.values():
             p.close()
         self._plans = {}
+        self._bufs = {}
 
 
 # ------------------------------------------------------------- autotuning --

@@ -99,3 +99,21 @@ def test_exchange_then_local_joins_equal_global_join(oracle, world):
     assert all(r[2] for r in res), "a rank received keys of another destination"
     assert sum(r[3] for r in res) == int((R[:, 0] != 0).sum())
     assert sum(r[4] for r in res) == int((S[:, 0] != 0).sum())
+
+
+def test_exchange_layout_tiles_every_receive_buffer():
+    sys.path.insert(0, os.path.join(ROOT, "spid-join_b200"))
+    import spidjoin
+    rng = np.random.default_rng(3)
+    for world in (1, 2, 3, 8):
+        C = rng.integers(0, 1000, (world, world)).tolist()
+        C[0][world - 1] = 0
+        layouts = [spidjoin.exchange_layout(C, r) for r in range(world)]
+        need = max(sum(C[s][d] for s in range(world)) for d in range(world))
+        for d in range(world):
+            segs = sorted((layouts[s][1][d], layouts[s][1][d] + C[s][d]) for s in range(world))
+            pos = 0
+            for a, b in segs:  # senders' segments follow each other without gaps or overlap
+                assert a == pos
+                pos = b
+            assert pos == layouts[d][0] <= need == layouts[0][2]

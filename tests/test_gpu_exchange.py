@@ -60,3 +60,63 @@ def test_distributed_join_one_rank(spj, oracle):
         dj.close()
     finally:
         dist.destroy_process_group()
+
+
+def test_fused_scatter_into_several_receive_buffers(spj, oracle):
+    # four ranks emulated on one GPU: each shard is scattered straight into the
+    # four receive buffers at the offsets of the size matrix, then every
+    # "rank" joins what it received; the union is the global join
+    import torch
+    world = 4
+    n_r, n_s = 1 << 16, 1 << 18
+    R, S, expect = spj.generate_host(n_r, n_s, 1.1, seed=21)
+    shards = {"R": np.array_split(R, world), "S": np.array_split(S, world)}
+    recv = {}
+    for rel in ("R", "S"):
+        dev = [torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).cuda() for x in shards[rel]]
+        C = []
+        for t in dev:
+            c = torch.empty(world, dtype=torch.int64, device="cuda")
+            spj.check(spj.lib().spj_exchange_count(t.data_ptr(), t.shape[0], world, c.data_ptr(), None))
+            C.append(c.tolist())
+        bufs = [torch.empty((spj.exchange_layout(C, d)[2] + 8, 2), dtype=torch.int32, device="cuda")
+                for d in range(world)]
+        ptrs = torch.tensor([b.data_ptr() for b in bufs], dtype=torch.int64, device="cuda")
+        for src, t in enumerate(dev):
+            offs = torch.tensor(spj.exchange_layout(C, src)[1], dtype=torch.int64, device="cuda")
+            cur = torch.empty(world, dtype=torch.int64, device="cuda")
+            spj.check(spj.lib().spj_exchange_scatter(t.data_ptr(), t.shape[0], world, ptrs.data_ptr(),
+                                                     offs.data_ptr(), cur.data_ptr(), None))
+        torch.cuda.synchronize()
+        recv[rel] = [bufs[d][:spj.exchange_layout(C, d)[0]].cpu().numpy().view(np.uint32) for d in range(world)]
+        whole = np.concatenate(shards[rel])
+        dest = _dest(oracle, whole[:, 0], world)
+        for d in range(world):
+            assert np.all(_dest(oracle, recv[rel][d][:, 0], world) == d)
+            assert np.array_equal(oracle.sort_pairs(recv[rel][d]), oracle.sort_pairs(whole[dest == d]))
+    out = np.concatenate([oracle.simple_join(recv["R"][d], recv["S"][d]) for d in range(world)])
+    assert out.shape == (n_s, 2) and oracle.checksum(out) == expect
+
+
+def test_distributed_join_fused_one_rank(spj, oracle):
+    import torch
+    import torch.distributed as dist
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            device_id=torch.device("cuda", 0))
+    try:
+        n_r, n_s = 1 << 18, 1 << 20
+        R, S, expect = spj.generate_host(n_r, n_s, 1.0, seed=19)
+        dj = spj.DistributedJoin(design=spj.make_design(rank_num=1), fused=True)
+        dR = torch.from_numpy(R.view(np.int32)).cuda()
+        dS = torch.from_numpy(S.view(np.int32)).cuda()
+        for _ in range(2):
+            pairs, n = dj.run(dR, dS)
+            torch.cuda.synchronize()
+            got = pairs[:int(n.item())].cpu().numpy().view(np.uint32)
+            assert got.shape == (n_s, 2) and oracle.checksum(got) == expect
+        dj.close()
+    finally:
+        dist.destroy_process_group()
