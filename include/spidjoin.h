@@ -147,6 +147,7 @@ void spj_destroy(spj_handle_t *h);
 
 typedef struct spj_plan spj_plan_t;
 
+/* |R| and |S| below 2^32 - 2^24 - 1 tuples (output positions are 32-bit). */
 int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_plan_t **out);
 
 /* Output capacity (pairs) that `out` must provide for this plan. */

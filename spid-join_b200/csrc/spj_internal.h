@@ -21,6 +21,8 @@ constexpr int kHistThreads = 1024;
 constexpr int kScatterThreads = 512;
 constexpr int kScatterBlocksPerSM = 2;  // resident scatter CTAs per SM (shared memory and registers)
 constexpr int kJoinThreads = 1024;
+// Relation sizes stay below this, so output positions (|S| + output slack) fit 32 bits.
+constexpr long long kMaxTuples = 0xFFFFFFFFll - (1ll << 24);
 constexpr int kOutChunk = 1024;       // output pairs reserved per warp at a time
 constexpr int kMaxHoles = 12288;      // per join: warps of the emitting kernels (one hole each)
 constexpr int kUpSlots = kMaxHoles + 2;  // chunks that the output's tail [N, reserved) can span

@@ -630,7 +630,7 @@ __global__ void k_units(PlanDev P) {
 // The output state of the join a CTA is working on.
 struct OutCtx {
     Tuple *out;
-    unsigned long long cap;
+    uint32_t cap;  // plans keep the output below 2^32 pairs
     JoinCtr *ctr;
     Hole *holes;
     uint32_t chunk;
@@ -639,7 +639,7 @@ struct OutCtx {
 __device__ __forceinline__ OutCtx out_ctx(const JoinDev &J) {
     OutCtx o;
     o.out = J.out;
-    o.cap = J.out_cap;
+    o.cap = (uint32_t)J.out_cap;
     o.ctr = J.ctr;
     o.holes = J.holes;
     o.chunk = J.out_chunk;
@@ -647,7 +647,7 @@ __device__ __forceinline__ OutCtx out_ctx(const JoinDev &J) {
 }
 
 struct WarpOut {
-    unsigned long long cur, end;
+    uint32_t cur, end;  // output positions (below 2^32)
 };
 
 // Warp-aggregated append: one ballot per 32 candidate pairs; a fresh chunk of
@@ -658,14 +658,14 @@ __device__ __forceinline__ void warp_emit(const OutCtx &o, WarpOut &w, bool has,
     if (mask == 0) return;
     const unsigned m = __popc(mask);
     const unsigned rank = __popc(mask & lanemask_lt());
-    unsigned long long pos;
+    uint32_t pos;
     if (w.cur + m <= w.end) {
         pos = w.cur + rank;
         w.cur += m;
     } else {
-        const unsigned avail = (unsigned)(w.end - w.cur);
-        unsigned long long nb = 0;
-        if ((threadIdx.x & 31) == 0) nb = atomicAdd(&o.ctr->out_reserved, (unsigned long long)o.chunk);
+        const uint32_t avail = w.end - w.cur;
+        uint32_t nb = 0;
+        if ((threadIdx.x & 31) == 0) nb = (uint32_t)atomicAdd(&o.ctr->out_reserved, (unsigned long long)o.chunk);
         nb = __shfl_sync(0xffffffffu, nb, 0);
         pos = rank < avail ? w.cur + rank : nb + (rank - avail);
         w.cur = nb + (m - avail);
@@ -690,7 +690,7 @@ __device__ __forceinline__ void warp_close(const OutCtx &o, WarpOut &w) {
             atomicOr(&o.ctr->error, 8u);
         }
     }
-    w.cur = w.end = 0ull;
+    w.cur = w.end = 0u;
 }
 
 // Table slot of a key: Fibonacci (multiplicative) hashing -- the key times
@@ -814,7 +814,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
     __shared__ unsigned s_slot;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
-    WarpOut w{0ull, 0ull};
+    WarpOut w{0u, 0u};
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu;
     Unit un;
@@ -889,7 +889,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
     Tuple *rs = reinterpret_cast<Tuple *>(smem_u64);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
-    WarpOut w{0ull, 0ull};
+    WarpOut w{0u, 0u};
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0, lmask = 0;
     Unit un;
@@ -982,7 +982,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
     __shared__ unsigned s_slot;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
-    WarpOut w{0ull, 0ull};
+    WarpOut w{0u, 0u};
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0;
     Unit un;
@@ -1095,7 +1095,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
     __shared__ unsigned s_slot;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
-    WarpOut w{0ull, 0ull};
+    WarpOut w{0u, 0u};
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu;
     Unit un;

@@ -372,8 +372,8 @@ static int create_plan(int J, const int64_t *n_r, const int64_t *n_s, const spj_
     if (rc) return rc;
     if (J < 1 || J > 65535) return set_error(SPJ_E_ARG, "a batch holds 1 to 65535 joins");
     for (int j = 0; j < J; j++)
-        if (n_r[j] < 0 || n_s[j] < 0 || n_r[j] >= 0xFFFFFFFFll || n_s[j] >= 0xFFFFFFFFll)
-            return set_error(SPJ_E_ARG, "relation sizes must be in [0, 2^32 - 1)");
+        if (n_r[j] < 0 || n_s[j] < 0 || n_r[j] >= kMaxTuples || n_s[j] >= kMaxTuples)
+            return set_error(SPJ_E_ARG, "relation sizes must be in [0, 2^32 - 2^24 - 1)");
     int sms = 0, dev = 0;
     if ((rc = device_sms(&sms, &dev))) return rc;
     spj_plan *pl = new spj_plan();
@@ -447,6 +447,9 @@ int create_plan_stream(int J, const int64_t *n_r, const int64_t *n_s, const spj_
     int rc = validate_design(design);
     if (rc) return rc;
     if (J < 1 || J > 65535) return set_error(SPJ_E_ARG, "a batch holds 1 to 65535 joins");
+    for (int j = 0; j < J; j++)
+        if (n_r[j] < 0 || n_s[j] < 0 || n_r[j] >= kMaxTuples || n_s[j] >= kMaxTuples)
+            return set_error(SPJ_E_ARG, "relation sizes must be in [0, 2^32 - 2^24 - 1)");
     int sms = 0, dev = 0;
     if ((rc = device_sms(&sms, &dev))) return rc;
     spj_plan *pl = new spj_plan();

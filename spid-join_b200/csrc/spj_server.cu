@@ -264,7 +264,7 @@ int64_t spj_server_output_capacity(spj_server_t *sv, int64_t n_r, int64_t n_s) {
 int spj_server_submit(spj_server_t *sv, const spj_kv_pair_t *r, int64_t n_r, const spj_kv_pair_t *s, int64_t n_s,
                       spj_kv_pair_t *out, int64_t out_capacity, int64_t *n_out, int64_t *id) {
     if (!sv || !out || !n_out || !id) return set_error(SPJ_E_ARG, "NULL argument");
-    if (n_r < 0 || n_s < 0 || n_r >= 0xFFFFFFFFll || n_s >= 0xFFFFFFFFll || (n_r && !r) || (n_s && !s))
+    if (n_r < 0 || n_s < 0 || n_r >= kMaxTuples || n_s >= kMaxTuples || (n_r && !r) || (n_s && !s))
         return set_error(SPJ_E_ARG, "bad columns");
     if (((uintptr_t)r & 15) || ((uintptr_t)s & 15) || ((uintptr_t)out & 15) || ((uintptr_t)n_out & 7))
         return set_error(SPJ_E_ARG, "columns and output must be 16-byte aligned, the count 8-byte aligned");
