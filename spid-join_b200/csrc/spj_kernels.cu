@@ -632,7 +632,6 @@ struct OutCtx {
     Tuple *out;
     uint32_t cap;  // plans keep the output below 2^32 pairs
     JoinCtr *ctr;
-    Hole *holes;
     uint32_t chunk;
 };
 
@@ -641,7 +640,6 @@ __device__ __forceinline__ OutCtx out_ctx(const JoinDev &J) {
     o.out = J.out;
     o.cap = (uint32_t)J.out_cap;
     o.ctr = J.ctr;
-    o.holes = J.holes;
     o.chunk = J.out_chunk;
     return o;
 }
@@ -679,15 +677,15 @@ __device__ __forceinline__ void warp_emit(const OutCtx &o, WarpOut &w, bool has,
     }
 }
 
-// Records the unused tail of the warp's chunk as the warp's hole in this join.
-__device__ __forceinline__ void warp_close(const OutCtx &o, WarpOut &w) {
+// Records the unused tail of the warp's chunk as the warp's hole in join J.
+__device__ __forceinline__ void warp_close(const JoinDev &J, WarpOut &w) {
     if ((threadIdx.x & 31) == 0 && w.end > w.cur) {
-        const unsigned h = atomicAdd(&o.ctr->hole_count, 1u);
+        const unsigned h = atomicAdd(&J.ctr->hole_count, 1u);
         if (h < kMaxHoles) {
-            o.holes[h].begin = w.cur;
-            o.holes[h].end = w.end;
+            J.holes[h].begin = w.cur;
+            J.holes[h].end = w.end;
         } else {
-            atomicOr(&o.ctr->error, 8u);
+            atomicOr(&J.ctr->error, 8u);
         }
     }
     w.cur = w.end = 0u;
@@ -803,7 +801,7 @@ __device__ __forceinline__ bool next_unit(const PlanDev &P, unsigned n_units, un
 // previous join, which leaves that join at most one hole per warp).
 __device__ __forceinline__ void switch_join(const PlanDev &P, uint32_t j, uint32_t &cur_j, OutCtx &o, WarpOut &w) {
     if (j == cur_j) return;
-    if (cur_j != 0xffffffffu) warp_close(o, w);
+    if (cur_j != 0xffffffffu) warp_close(P.join[cur_j], w);
     cur_j = j;
     o = out_ctx(P.join[j]);
 }
@@ -844,7 +842,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
         }
         __syncthreads();
     }
-    if (cur_j != 0xffffffffu) warp_close(o, w);
+    if (cur_j != 0xffffffffu) warp_close(P.join[cur_j], w);
 }
 
 // Block-wide exclusive scan of n <= 256 counters by warp 0 (8 per lane); writes
@@ -953,7 +951,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
         }
         __syncthreads();
     }
-    if (cur_j != 0xffffffffu) warp_close(o, w);
+    if (cur_j != 0xffffffffu) warp_close(P.join[cur_j], w);
 }
 
 // ----------------------------------------------------------- sort-merge join --
@@ -1051,7 +1049,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
         }
         __syncthreads();
     }
-    if (cur_j != 0xffffffffu) warp_close(o, w);
+    if (cur_j != 0xffffffffu) warp_close(P.join[cur_j], w);
 }
 
 // ------------------------------------------- non-partitioned hash join (NPHJ) --
@@ -1143,7 +1141,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
         }
         __syncthreads();
     }
-    if (cur_j != 0xffffffffu) warp_close(o, w);
+    if (cur_j != 0xffffffffu) warp_close(P.join[cur_j], w);
 }
 
 // ------------------------------------------------------------------ fix-up --
@@ -1409,7 +1407,7 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
     mark(5);
     k_fixup_prep<<<J, 1024, (size_t)kUpSlots * 2 * 8, st>>>(P);
     // gaps are spread over all warps of a join's blocks; a batch gives each join fewer blocks
-    k_fixup_copy<<<dim3(std::max<uint32_t>(16, (kMaxHoles + 7) / 8 / J), J), 256, 0, st>>>(P);
+    k_fixup_copy<<<dim3(std::max<uint32_t>(64, (kMaxHoles + 7) / 8 / J), J), 256, 0, st>>>(P);
     mark(6);
     if (ev) {
         pl->ring_next = (pl->ring_next + 1) % spj_plan::kRing;
