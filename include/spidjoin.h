@@ -285,31 +285,41 @@ int spj_join_noalloc(const spj_kv_pair_t *r, int64_t n_r, const spj_kv_pair_t *s
                      int64_t out_capacity, int64_t *n_out, void *stream);
 
 /* The split before the rank-to-rank exchange of a join sharded over `world`
- * GPUs: the B200 form of the reference's global partition scatter into
- * per-rank packets ahead of its rotate-and-stream shuffle
+ * GPUs (this rank is `me`): the B200 form of the reference's global partition
+ * scatter into per-rank packets ahead of its rotate-and-stream shuffle
  * (src/dpu/src/join/glb_partition_packet.c:420-464, src/queryHostFunc.cc:481-777).
- * The destination of a tuple is (glb_partition_hash(key) * world) >> 32. out
- * (device, n pairs) receives the non-padding tuples grouped by destination:
- * destination d's are out[off_d, off_d + counts[d]) with off the exclusive
- * prefix of counts (the order inside a group is unspecified). counts: device
- * int64[2 * world]; the first `world` entries receive the group sizes, the rest
- * is workspace. Allocates nothing, does not synchronise. */
-int spj_exchange_split(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv_pair_t *out, int64_t *counts,
-                       void *stream);
-
-/* The same exchange with the split fused into the send: spj_exchange_count gives
- * the per-destination sizes (counts: device int64[world]); once every rank knows
- * the size matrix, spj_exchange_scatter writes each non-padding tuple straight
- * into its destination's receive buffer. dest_bufs: device array of `world`
- * pointers to the ranks' receive buffers (peer memory mapped into this process,
- * e.g. symmetric memory, written over NVLink); dest_offsets: device
- * int64[world], where this rank's segment starts in each destination buffer;
- * cursor: device int64[world] workspace. Allocates nothing, does not
- * synchronise; the caller orders the receivers' reads after every sender's
- * kernel (a cross-GPU barrier). */
-int spj_exchange_count(const spj_kv_pair_t *tuples, int64_t n, int world, int64_t *counts, void *stream);
-int spj_exchange_scatter(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv_pair_t *const *dest_bufs,
-                         const int64_t *dest_offsets, int64_t *cursor, void *stream);
+ * The destination of a tuple is (glb_partition_hash(key) * world) >> 32, except
+ * for heavy keys (heavy_keys: device uint32[n_heavy], sorted, n_heavy <= 256),
+ * SPID-Join's skew handling across ranks: with heavy_mode 1 (for S) a heavy
+ * key's tuples stay on `me`; with heavy_mode 2 (for R, whose heavy tuples the
+ * caller replicates to every rank) they leave the exchange; heavy_mode 0
+ * ignores the list. Padding (key 0) is dropped.
+ *
+ * spj_exchange_split: out (device, n pairs) receives the routed tuples grouped
+ * by destination: destination d's are out[off_d, off_d + counts[d]) with off the
+ * exclusive prefix of counts (the order inside a group is unspecified);
+ * counts: device int64[2 * world], the first `world` entries receive the group
+ * sizes, the rest is workspace. Then an all-to-all moves the groups.
+ *
+ * spj_exchange_count + spj_exchange_scatter: the split fused into the send.
+ * spj_exchange_count gives the per-destination sizes (counts: device
+ * int64[world]); once every rank knows the size matrix, spj_exchange_scatter
+ * writes each routed tuple straight into its destination's receive buffer.
+ * dest_bufs: device array of `world` pointers to the ranks' receive buffers
+ * (peer memory mapped into this process, e.g. symmetric memory, written over
+ * NVLink); dest_offsets: device int64[world], where this rank's segment starts
+ * in each destination buffer; cursor: device int64[world] workspace. The caller
+ * orders the receivers' reads after every sender's kernel (a cross-GPU
+ * barrier).
+ *
+ * All three allocate nothing and do not synchronise. */
+int spj_exchange_split(const spj_kv_pair_t *tuples, int64_t n, int world, int me, const uint32_t *heavy_keys,
+                       int n_heavy, int heavy_mode, spj_kv_pair_t *out, int64_t *counts, void *stream);
+int spj_exchange_count(const spj_kv_pair_t *tuples, int64_t n, int world, int me, const uint32_t *heavy_keys,
+                       int n_heavy, int heavy_mode, int64_t *counts, void *stream);
+int spj_exchange_scatter(const spj_kv_pair_t *tuples, int64_t n, int world, int me, const uint32_t *heavy_keys,
+                         int n_heavy, int heavy_mode, spj_kv_pair_t *const *dest_bufs, const int64_t *dest_offsets,
+                         int64_t *cursor, void *stream);
 
 /* Histogram of glb_partition_hash(key) & (2^bits - 1) over a device column (key-0
  * tuples skipped): the B200 form of the global partition count kernel

@@ -24,23 +24,62 @@ constexpr int kSplitThreads = 512;
 constexpr int kSplitTile = 4096;  // tuples per block step
 constexpr int kMaxWorld = 1024;
 
+constexpr int kMaxHeavy = 256;
+constexpr uint32_t kDrop = 0xffffffffu;
+
+// Where a tuple goes. Heavy keys (SPID-Join's skew handling across ranks): the
+// S tuples of a heavy key stay on their rank (keep_local) and the R tuples of a
+// heavy key are replicated to every rank by the caller, so they leave this
+// exchange (drop); other keys go to (glb_partition_hash(key) * world) >> 32.
+struct Route {
+    uint32_t world, me;
+    int heavy_mode;  // 0: no heavy keys, 1: heavy stays on `me`, 2: heavy is dropped
+    uint32_t nheavy;
+    const uint32_t *heavy;  // sorted
+};
+
 __device__ __forceinline__ uint32_t dest_of(uint32_t key, uint32_t world) {
     return (uint32_t)(((unsigned long long)glb_partition_hash(key) * world) >> 32);
 }
 
-// counts[d] += tuples of destination d (key-0 padding is dropped).
-__global__ void __launch_bounds__(kSplitThreads) k_split_count(const Tuple *in, unsigned long long n, uint32_t world,
+__device__ __forceinline__ uint32_t route_of(uint32_t key, const Route &rt, const uint32_t *heavy_sm) {
+    if (rt.nheavy) {
+        uint32_t lo = 0, hi = rt.nheavy;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (heavy_sm[mid] < key)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        if (lo < rt.nheavy && heavy_sm[lo] == key) return rt.heavy_mode == 1 ? rt.me : kDrop;
+    }
+    return dest_of(key, rt.world);
+}
+
+__device__ __forceinline__ void load_heavy(const Route &rt, uint32_t *heavy_sm) {
+    for (uint32_t i = threadIdx.x; i < rt.nheavy; i += blockDim.x) heavy_sm[i] = rt.heavy[i];
+}
+
+// counts[d] += tuples of destination d (key-0 padding and dropped heavy keys
+// are not counted).
+__global__ void __launch_bounds__(kSplitThreads) k_split_count(const Tuple *in, unsigned long long n, Route rt,
                                                                unsigned long long *counts) {
     __shared__ uint32_t cnt[kMaxWorld];
-    for (uint32_t d = threadIdx.x; d < world; d += blockDim.x) cnt[d] = 0;
+    __shared__ uint32_t heavy_sm[kMaxHeavy];
+    load_heavy(rt, heavy_sm);
+    for (uint32_t d = threadIdx.x; d < rt.world; d += blockDim.x) cnt[d] = 0;
     __syncthreads();
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const Tuple t = in[i];
-        if (t.key) atomicAdd(&cnt[dest_of(t.key, world)], 1u);
+        if (t.key) {
+            const uint32_t d = route_of(t.key, rt, heavy_sm);
+            if (d != kDrop) atomicAdd(&cnt[d], 1u);
+        }
     }
     __syncthreads();
-    for (uint32_t d = threadIdx.x; d < world; d += blockDim.x)
+    for (uint32_t d = threadIdx.x; d < rt.world; d += blockDim.x)
         if (cnt[d]) atomicAdd(&counts[d], (unsigned long long)cnt[d]);
 }
 
@@ -68,12 +107,15 @@ __global__ void k_split_offsets(const unsigned long long *counts, uint32_t world
 // tuples go to dests[d] (another GPU's receive buffer, written over NVLink);
 // otherwise all go to `out`.
 template <bool kPeers>
-__global__ void __launch_bounds__(kSplitThreads) k_split_scatter(const Tuple *in, unsigned long long n, uint32_t world,
+__global__ void __launch_bounds__(kSplitThreads) k_split_scatter(const Tuple *in, unsigned long long n, Route rt,
                                                                  unsigned long long *cursor, Tuple *out,
                                                                  Tuple *const *dests) {
     __shared__ uint32_t cnt[kMaxWorld];
     __shared__ unsigned long long base[kMaxWorld];
+    __shared__ uint32_t heavy_sm[kMaxHeavy];
+    const uint32_t world = rt.world;
     constexpr int PER = kSplitTile / kSplitThreads;
+    load_heavy(rt, heavy_sm);
     for (unsigned long long t0 = (unsigned long long)blockIdx.x * kSplitTile; t0 < n;
          t0 += (unsigned long long)gridDim.x * kSplitTile) {
         for (uint32_t d = threadIdx.x; d < world; d += blockDim.x) cnt[d] = 0;
@@ -86,8 +128,8 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_scatter(const Tuple *in
             v[k] = i < n ? in[i] : Tuple{0u, 0u};
             dr[k] = 0xffffffffu;
             if (v[k].key) {
-                const uint32_t d = dest_of(v[k].key, world);
-                dr[k] = (d << 16) | atomicAdd(&cnt[d], 1u);
+                const uint32_t d = route_of(v[k].key, rt, heavy_sm);
+                if (d != kDrop) dr[k] = (d << 16) | atomicAdd(&cnt[d], 1u);
             }
         }
         __syncthreads();
@@ -107,34 +149,6 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_scatter(const Tuple *in
 
 }  // namespace
 
-extern "C" {
-
-int spj_exchange_split(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv_pair_t *out, int64_t *counts,
-                       void *stream) {
-    if (world < 1 || world > kMaxWorld) return set_error(SPJ_E_ARG, "world must be in [1, 1024]");
-    if (n < 0 || (n > 0 && (!tuples || !out)) || !counts) return set_error(SPJ_E_ARG, "bad split arguments");
-    int dev = 0, sms = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return set_error(SPJ_E_NODEVICE, "no CUDA device available; libspidjoin has no CPU path");
-    }
-    cudaStream_t st = (cudaStream_t)stream;
-    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(counts);
-    unsigned long long *cursor = cnt + world;
-    e = cudaMemsetAsync(cnt, 0, (size_t)world * 8, st);
-    if (e != cudaSuccess) return cuda_error(e, "split counters");
-    const Tuple *in = reinterpret_cast<const Tuple *>(tuples);
-    if (n > 0) k_split_count<<<sms * 4, kSplitThreads, 0, st>>>(in, (unsigned long long)n, world, cnt);
-    k_split_offsets<<<1, 32, 0, st>>>(cnt, world, cursor);
-    if (n > 0)
-        k_split_scatter<false><<<sms * 4, kSplitThreads, 0, st>>>(in, (unsigned long long)n, world, cursor,
-                                                                   reinterpret_cast<Tuple *>(out), nullptr);
-    e = cudaGetLastError();
-    return e ? cuda_error(e, "split kernels") : SPJ_OK;
-}
-
 static int exchange_device(int *sms) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -146,33 +160,73 @@ static int exchange_device(int *sms) {
     return SPJ_OK;
 }
 
-int spj_exchange_count(const spj_kv_pair_t *tuples, int64_t n, int world, int64_t *counts, void *stream) {
+static int make_route(int world, int me, const uint32_t *heavy, int n_heavy, int heavy_mode, Route *rt) {
     if (world < 1 || world > kMaxWorld) return set_error(SPJ_E_ARG, "world must be in [1, 1024]");
-    if (n < 0 || (n > 0 && !tuples) || !counts) return set_error(SPJ_E_ARG, "bad count arguments");
-    int sms = 0, rc = exchange_device(&sms);
+    if (me < 0 || me >= world) return set_error(SPJ_E_ARG, "rank outside the world");
+    if (n_heavy < 0 || n_heavy > kMaxHeavy || (n_heavy > 0 && !heavy) || heavy_mode < 0 || heavy_mode > 2)
+        return set_error(SPJ_E_ARG, "heavy keys: at most 256, sorted, mode 0..2");
+    *rt = Route{(uint32_t)world, (uint32_t)me, heavy_mode, heavy_mode ? (uint32_t)n_heavy : 0u, heavy};
+    return SPJ_OK;
+}
+
+extern "C" {
+
+int spj_exchange_split(const spj_kv_pair_t *tuples, int64_t n, int world, int me, const uint32_t *heavy_keys,
+                       int n_heavy, int heavy_mode, spj_kv_pair_t *out, int64_t *counts, void *stream) {
+    Route rt;
+    int rc = make_route(world, me, heavy_keys, n_heavy, heavy_mode, &rt);
     if (rc) return rc;
+    if (n < 0 || (n > 0 && (!tuples || !out)) || !counts) return set_error(SPJ_E_ARG, "bad split arguments");
+    int sms = 0;
+    if ((rc = exchange_device(&sms))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(counts);
+    unsigned long long *cursor = cnt + world;
+    cudaError_t e = cudaMemsetAsync(cnt, 0, (size_t)world * 8, st);
+    if (e != cudaSuccess) return cuda_error(e, "split counters");
+    const Tuple *in = reinterpret_cast<const Tuple *>(tuples);
+    if (n > 0) k_split_count<<<sms * 4, kSplitThreads, 0, st>>>(in, (unsigned long long)n, rt, cnt);
+    k_split_offsets<<<1, 32, 0, st>>>(cnt, (uint32_t)world, cursor);
+    if (n > 0)
+        k_split_scatter<false><<<sms * 4, kSplitThreads, 0, st>>>(in, (unsigned long long)n, rt, cursor,
+                                                                   reinterpret_cast<Tuple *>(out), nullptr);
+    e = cudaGetLastError();
+    return e ? cuda_error(e, "split kernels") : SPJ_OK;
+}
+
+int spj_exchange_count(const spj_kv_pair_t *tuples, int64_t n, int world, int me, const uint32_t *heavy_keys,
+                       int n_heavy, int heavy_mode, int64_t *counts, void *stream) {
+    Route rt;
+    int rc = make_route(world, me, heavy_keys, n_heavy, heavy_mode, &rt);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && !tuples) || !counts) return set_error(SPJ_E_ARG, "bad count arguments");
+    int sms = 0;
+    if ((rc = exchange_device(&sms))) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(counts, 0, (size_t)world * 8, st);
     if (e == cudaSuccess && n > 0)
         k_split_count<<<sms * 4, kSplitThreads, 0, st>>>(reinterpret_cast<const Tuple *>(tuples),
-                                                         (unsigned long long)n, world,
+                                                         (unsigned long long)n, rt,
                                                          reinterpret_cast<unsigned long long *>(counts));
     if (e == cudaSuccess) e = cudaGetLastError();
     return e ? cuda_error(e, "count kernel") : SPJ_OK;
 }
 
-int spj_exchange_scatter(const spj_kv_pair_t *tuples, int64_t n, int world, spj_kv_pair_t *const *dest_bufs,
-                         const int64_t *dest_offsets, int64_t *cursor, void *stream) {
-    if (world < 1 || world > kMaxWorld) return set_error(SPJ_E_ARG, "world must be in [1, 1024]");
+int spj_exchange_scatter(const spj_kv_pair_t *tuples, int64_t n, int world, int me, const uint32_t *heavy_keys,
+                         int n_heavy, int heavy_mode, spj_kv_pair_t *const *dest_bufs, const int64_t *dest_offsets,
+                         int64_t *cursor, void *stream) {
+    Route rt;
+    int rc = make_route(world, me, heavy_keys, n_heavy, heavy_mode, &rt);
+    if (rc) return rc;
     if (n < 0 || (n > 0 && !tuples) || !dest_bufs || !dest_offsets || !cursor)
         return set_error(SPJ_E_ARG, "bad scatter arguments");
-    int sms = 0, rc = exchange_device(&sms);
-    if (rc) return rc;
+    int sms = 0;
+    if ((rc = exchange_device(&sms))) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = cudaMemcpyAsync(cursor, dest_offsets, (size_t)world * 8, cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess && n > 0)
         k_split_scatter<true><<<sms * 4, kSplitThreads, 0, st>>>(
-            reinterpret_cast<const Tuple *>(tuples), (unsigned long long)n, world,
+            reinterpret_cast<const Tuple *>(tuples), (unsigned long long)n, rt,
             reinterpret_cast<unsigned long long *>(cursor), nullptr, reinterpret_cast<Tuple *const *>(dest_bufs));
     if (e == cudaSuccess) e = cudaGetLastError();
     return e ? cuda_error(e, "exchange scatter kernel") : SPJ_OK;

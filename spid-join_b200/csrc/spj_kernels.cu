@@ -810,7 +810,8 @@ __device__ __forceinline__ void switch_join(const PlanDev &P, uint32_t j, uint32
 __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
     extern __shared__ unsigned long long table[];
     __shared__ unsigned s_slot;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
     WarpOut w{0u, 0u};
     OutCtx o{};
@@ -885,7 +886,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
     __shared__ unsigned s_slot;
     __shared__ uint32_t bcnt[256], boff[257];
     Tuple *rs = reinterpret_cast<Tuple *>(smem_u64);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
     WarpOut w{0u, 0u};
     OutCtx o{};
@@ -978,7 +980,8 @@ __device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v) 
 __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
     extern __shared__ unsigned long long sorted[];
     __shared__ unsigned s_slot;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
     WarpOut w{0u, 0u};
     OutCtx o{};
@@ -1091,7 +1094,8 @@ __global__ void k_nphj_build(PlanDev P) {
 
 __global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
     __shared__ unsigned s_slot;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
     WarpOut w{0u, 0u};
     OutCtx o{};

@@ -146,9 +146,9 @@ def lib():
         L.spj_server_hold.argtypes = [vp, i32]
         L.spj_server_destroy.argtypes = [vp]
         L.spj_server_destroy.restype = None
-        L.spj_exchange_split.argtypes = [vp, i64, i32, vp, vp, vp]
-        L.spj_exchange_count.argtypes = [vp, i64, i32, vp, vp]
-        L.spj_exchange_scatter.argtypes = [vp, i64, i32, vp, vp, vp, vp]
+        L.spj_exchange_split.argtypes = [vp, i64, i32, i32, vp, i32, i32, vp, vp, vp]
+        L.spj_exchange_count.argtypes = [vp, i64, i32, i32, vp, i32, i32, vp, vp]
+        L.spj_exchange_scatter.argtypes = [vp, i64, i32, i32, vp, i32, i32, vp, vp, vp, vp]
         L.spj_tuning_set.argtypes = [ctypes.POINTER(Tuning), i32]
         L.spj_tuning_get.argtypes = [ctypes.POINTER(Tuning), i32]
         _lib = L
@@ -416,18 +416,28 @@ def exchange_layout(C, me):
 class DistributedJoin:
     """A join of R and S sharded over the ranks of a torch.distributed process
     group, one GPU per rank: the multi-GPU form of the reference's rank-to-rank
-    shuffle (src/queryHostFunc.cc:481-777). Every rank splits its shards by
-    destination rank (spj_exchange_split: (glb_partition_hash(key) * world) >> 32),
-    exchanges the per-destination counts and then the tuples of each relation
-    with one all-to-all each (NCCL over NVLink), and joins what it received with
-    its own plan. Rank d's output holds the pairs of the keys whose destination
-    is d; the union over the ranks is the join of the union of the shards.
+    shuffle (src/queryHostFunc.cc:481-777). Every rank routes its shards by
+    destination rank ((glb_partition_hash(key) * world) >> 32), exchanges them,
+    and joins what it received with its own plan; the union over the ranks is
+    the join of the union of the shards.
 
-    `split(T) -> (grouped, counts)` and `join(R, S) -> (pairs, n)` replace the
-    device split and the local join; the CPU tests of the exchange protocol pass
-    host versions of both and run gloo ranks."""
+    Skew across ranks is handled as SPID-Join handles it across DPU rank sets:
+    keys whose estimated share of the global S exceeds heavy_share / world (from
+    an even sample of every rank's S, all-gathered) are heavy; their S tuples
+    stay on the rank that holds them and their R tuples are replicated to every
+    rank, so no rank receives a hot key's whole S.
 
-    def __init__(self, group=None, design=None, split=None, join=None, fused=False):
+    The exchange is either fused (`fused=True`: one kernel routes every tuple
+    straight into its destination's receive buffer in symmetric memory, after an
+    all-gather of the size matrix) or an NCCL all-to-all after a device split.
+    `split(T, heavy, mode) -> (grouped, counts)` and `join(R, S) -> (pairs, n)`
+    replace the device split and the local join; the CPU tests of the exchange
+    protocol pass host versions of both and run gloo ranks."""
+
+    MAX_HEAVY = 256
+
+    def __init__(self, group=None, design=None, split=None, join=None, fused=False, heavy=True,
+                 heavy_share=0.25, sample=1 << 16):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
@@ -437,24 +447,107 @@ class DistributedJoin:
         self._split = split if split is not None else self._device_split
         self._join = join if join is not None else self._device_join
         self.fused = fused
+        self.heavy = heavy
+        self.heavy_share = heavy_share
+        self.sample = sample
+        self.last_heavy = []
         self._plans = {}
         self._bufs = {}
 
-    def _fused_exchange(self, T, slot):
-        """The split fused into the send: each tuple is written straight into its
-        destination rank's receive buffer (symmetric memory, peer stores over
-        NVLink) by spj_exchange_scatter, after one all-gather of the size matrix;
-        cross-GPU barriers before (receivers are done with the last exchange) and
-        after (every sender is done)."""
+    # ---- heavy keys
+    def heavy_keys(self, S):
+        """The sorted heavy keys (python ints), the same list on every rank."""
+        import torch
+        n = int(S.shape[0])
+        k = min(n, self.sample)
+        cand = torch.zeros((64, 2), dtype=torch.int64, device=S.device)
+        if k > 0:
+            idx = torch.linspace(0, n - 1, k, device=S.device).long()
+            keys = S[idx, 0].long() & 0xFFFFFFFF
+            keys = keys[keys != 0]
+            if keys.numel():
+                u, c = torch.unique(keys, return_counts=True)
+                top = torch.topk(c, min(64, c.numel()))
+                cand[:top.values.numel(), 0] = u[top.indices]
+                cand[:top.values.numel(), 1] = (top.values.double() * (n / k)).long()
+        allc = torch.empty((self.world * 64, 2), dtype=torch.int64, device=S.device)
+        self.dist.all_gather_into_tensor(allc, cand, group=self.group)
+        tot = torch.tensor([n], dtype=torch.int64, device=S.device)
+        self.dist.all_reduce(tot, group=self.group)
+        est = {}
+        for key, cnt in allc.tolist():
+            if key:
+                est[key] = est.get(key, 0) + cnt
+        bar = self.heavy_share * int(tot.item()) / self.world
+        hot = sorted((k2 for k2, c in est.items() if c >= bar and c > 0), key=lambda k2: -est[k2])
+        return sorted(hot[:self.MAX_HEAVY])
+
+    def _replicated_rows(self, R, heavy):
+        """Every rank's R tuples of the heavy keys, gathered on every rank."""
+        import torch
+        hk = torch.tensor([h - (1 << 32) if h >= (1 << 31) else h for h in heavy], dtype=torch.int32,
+                          device=R.device)
+        rows = R[torch.isin(R[:, 0], hk)] if R.shape[0] else R[:0]
+        cnt = torch.tensor([rows.shape[0]], dtype=torch.int64, device=R.device)
+        allcnt = torch.empty(self.world, dtype=torch.int64, device=R.device)
+        self.dist.all_gather_into_tensor(allcnt, cnt, group=self.group)
+        m = int(allcnt.max().item())
+        if m == 0:
+            return R[:0]
+        pad = torch.zeros((m, 2), dtype=R.dtype, device=R.device)
+        pad[:rows.shape[0]] = rows
+        allrows = torch.empty((self.world * m, 2), dtype=R.dtype, device=R.device)
+        self.dist.all_gather_into_tensor(allrows.view(-1), pad.view(-1), group=self.group)
+        return allrows[allrows[:, 0] != 0]
+
+    # ---- exchanges
+    def _heavy_dev(self, heavy, device):
+        import torch
+        return torch.tensor([h - (1 << 32) if h >= (1 << 31) else h for h in heavy] or [0], dtype=torch.int32,
+                            device=device)
+
+    def _device_split(self, T, heavy, mode):
+        import torch
+        hd = self._heavy_dev(heavy, T.device)
+        out = torch.empty_like(T)
+        cnt = torch.empty(2 * self.world, dtype=torch.int64, device=T.device)
+        check(lib().spj_exchange_split(T.data_ptr(), T.shape[0], self.world, self.rank, hd.data_ptr(), len(heavy),
+                                       mode, out.data_ptr(), cnt.data_ptr(), torch.cuda.current_stream().cuda_stream))
+        return out, cnt[:self.world]
+
+    def exchange(self, T, heavy=(), mode=0, extra=0):
+        """All-to-all exchange of the (n, 2) int32 tuples T routed by destination
+        rank; returns (buffer, received): the received tuples are buffer[:received],
+        with `extra` spare rows after them."""
+        import torch
+        grouped, cnt = self._split(T, list(heavy), mode)
+        recv_cnt = torch.empty_like(cnt)
+        self.dist.all_to_all_single(recv_cnt, cnt, group=self.group)
+        send, recv = [int(x) for x in cnt.tolist()], [int(x) for x in recv_cnt.tolist()]
+        got = torch.empty((sum(recv) + extra, 2), dtype=T.dtype, device=T.device)
+        src = grouped[:sum(send)].contiguous().view(torch.int64).view(-1)
+        self.dist.all_to_all_single(got[:sum(recv)].view(torch.int64).view(-1), src, output_split_sizes=recv,
+                                    input_split_sizes=send, group=self.group)
+        return got, sum(recv)
+
+    def _fused_exchange(self, T, slot, heavy=(), mode=0, extra=0):
+        """The split fused into the send: each routed tuple is written straight
+        into its destination rank's receive buffer (symmetric memory, peer stores
+        over NVLink) by spj_exchange_scatter, after one all-gather of the size
+        matrix; cross-GPU barriers before (receivers are done with the last
+        exchange) and after (every sender is done)."""
         import torch
         import torch.distributed._symmetric_memory as symm
         stream = torch.cuda.current_stream().cuda_stream
         world = self.world
+        hd = self._heavy_dev(list(heavy), T.device)
         cnt = torch.empty(world, dtype=torch.int64, device=T.device)
-        check(lib().spj_exchange_count(T.data_ptr(), T.shape[0], world, cnt.data_ptr(), stream))
+        check(lib().spj_exchange_count(T.data_ptr(), T.shape[0], world, self.rank, hd.data_ptr(), len(heavy), mode,
+                                       cnt.data_ptr(), stream))
         allc = torch.empty(world * world, dtype=torch.int64, device=T.device)
         self.dist.all_gather_into_tensor(allc, cnt, group=self.group)
         recv, off, need = exchange_layout(allc.view(world, world).tolist(), self.rank)
+        need += extra
         entry = self._bufs.get(slot)
         if entry is None or entry[0].shape[0] < need:  # the same decision on every rank: the matrix is global
             group = self.group if self.group is not None else self.dist.group.WORLD
@@ -467,18 +560,10 @@ class DistributedJoin:
         offs = torch.tensor(off, dtype=torch.int64, device=T.device)
         cursor = torch.empty(world, dtype=torch.int64, device=T.device)
         handle.barrier(channel=0, timeout_ms=60000)
-        check(lib().spj_exchange_scatter(T.data_ptr(), T.shape[0], world, ptrs.data_ptr(), offs.data_ptr(),
-                                         cursor.data_ptr(), stream))
+        check(lib().spj_exchange_scatter(T.data_ptr(), T.shape[0], world, self.rank, hd.data_ptr(), len(heavy), mode,
+                                         ptrs.data_ptr(), offs.data_ptr(), cursor.data_ptr(), stream))
         handle.barrier(channel=0, timeout_ms=60000)
-        return buf[:recv]
-
-    def _device_split(self, T):
-        import torch
-        out = torch.empty_like(T)
-        cnt = torch.empty(2 * self.world, dtype=torch.int64, device=T.device)
-        check(lib().spj_exchange_split(T.data_ptr(), T.shape[0], self.world, out.data_ptr(), cnt.data_ptr(),
-                                       torch.cuda.current_stream().cuda_stream))
-        return out, cnt[:self.world]
+        return buf, recv
 
     def _device_join(self, R, S):
         import torch
@@ -497,26 +582,23 @@ class DistributedJoin:
                      torch.cuda.current_stream().cuda_stream)
         return out, n
 
-    def exchange(self, T):
-        """Splits the (n, 2) int32 tuples T by destination rank and exchanges
-        them; returns the tuples this rank receives."""
-        import torch
-        grouped, cnt = self._split(T)
-        recv_cnt = torch.empty_like(cnt)
-        self.dist.all_to_all_single(recv_cnt, cnt, group=self.group)
-        send, recv = [int(x) for x in cnt.tolist()], [int(x) for x in recv_cnt.tolist()]
-        got = torch.empty((sum(recv), 2), dtype=T.dtype, device=T.device)
-        src = grouped[:sum(send)].contiguous().view(torch.int64).view(-1)
-        self.dist.all_to_all_single(got.view(torch.int64).view(-1), src, output_split_sizes=recv,
-                                    input_split_sizes=send, group=self.group)
-        return got
-
     def run(self, R, S):
         """R, S: this rank's shards, (n, 2) int32 tensors (key, payload) on this
         rank's device. Returns (pairs, n): this rank's part of the join."""
+        # heavy keys matter only across ranks; heavy="always" also routes them on one rank
+        heavy = self.heavy_keys(S) if self.heavy and (self.world > 1 or self.heavy == "always") else []
+        self.last_heavy = heavy
+        rows = self._replicated_rows(R, heavy) if heavy else R[:0]
+        h = int(rows.shape[0])
         if self.fused:
-            return self._join(self._fused_exchange(R, "R"), self._fused_exchange(S, "S"))
-        return self._join(self.exchange(R), self.exchange(S))
+            rb, nr = self._fused_exchange(R, "R", heavy, 2 if heavy else 0, extra=h)
+            sb, ns = self._fused_exchange(S, "S", heavy, 1 if heavy else 0)
+        else:
+            rb, nr = self.exchange(R, heavy, 2 if heavy else 0, extra=h)
+            sb, ns = self.exchange(S, heavy, 1 if heavy else 0)
+        if h:
+            rb[nr:nr + h] = rows
+        return self._join(rb[:nr + h], sb[:ns])
 
     def close(self):
         for p in self._plans.values():

@@ -26,11 +26,15 @@ def _dest(keys, world):
     return ((h * np.uint64(world)) >> np.uint64(32)).astype(np.int64)
 
 
-def _dataset(seed, n_r, n_s, world):
+def _dataset(seed, n_r, n_s, hot=0.0):
     rng = np.random.default_rng(seed)
     keys = rng.permutation(n_r).astype(np.uint32) + 1
+    keys[:3] = [0x80000001, 0xFFFFFF00, 0x7FFFFFFF]  # keys above 2^31 too
     R = np.stack([keys, np.arange(n_r, dtype=np.uint32)], axis=1)
     sk = keys[rng.integers(0, n_r, n_s)]
+    if hot:  # two hot keys carry a share `hot` of S each
+        sk[rng.random(n_s) < hot] = keys[1]
+        sk[rng.random(n_s) < hot] = keys[7]
     sk[rng.random(n_s) < 0.05] = 0                       # padding
     miss = rng.random(n_s) < 0.05
     sk[miss] = (n_r + 1 + rng.integers(0, 1000, int(miss.sum()))).astype(np.uint32)  # no partner
@@ -38,7 +42,7 @@ def _dataset(seed, n_r, n_s, world):
     return R, S
 
 
-def _rank_main(rank, world, port, seed, out_q):
+def _rank_main(rank, world, port, seed, out_q, hot=0.0):
     import torch
     import torch.distributed as dist
     sys.path.insert(0, os.path.join(ROOT, "spid-join_b200"))
@@ -49,16 +53,21 @@ def _rank_main(rank, world, port, seed, out_q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        R, S = _dataset(seed, 5000, 20000, world)
+        R, S = _dataset(seed, 5000, 20000, hot)
         # uneven shards: rank i holds a contiguous slice of each relation
         rb = np.linspace(0, R.shape[0], world + 1).astype(int)
         sb = (np.linspace(0, 1, world + 1) ** 1.5 * S.shape[0]).astype(int)
         myR, myS = R[rb[rank]:rb[rank + 1]], S[sb[rank]:sb[rank + 1]]
 
-        def split(T):
+        def split(T, heavy, mode):
             a = T.numpy().view(np.uint32).reshape(-1, 2)
             a = a[a[:, 0] != 0]
             d = _dest(a[:, 0], world)
+            hv = np.isin(a[:, 0], np.array(heavy, dtype=np.uint32))
+            if mode == 1:
+                d[hv] = rank
+            elif mode == 2:
+                a, d = a[~hv], d[~hv]
             order = np.argsort(d, kind="stable")
             counts = np.bincount(d, minlength=world).astype(np.int64)
             return torch.from_numpy(a[order].view(np.int32).copy()), torch.from_numpy(counts)
@@ -72,32 +81,41 @@ def _rank_main(rank, world, port, seed, out_q):
 
         dj = spidjoin.DistributedJoin(split=split, join=join)
         pairs, n = dj.run(torch.from_numpy(myR.view(np.int32).copy()), torch.from_numpy(myS.view(np.int32).copy()))
-        ok_dest = all(bool(np.all(_dest(received[x][:, 0], world) == rank)) for x in ("R", "S"))
+        heavy = np.array(dj.last_heavy, dtype=np.uint32)
+        hr = np.isin(received["R"][:, 0], heavy)
+        hs = np.isin(received["S"][:, 0], heavy)
+        ok_dest = (bool(np.all(_dest(received["R"][~hr, 0], world) == rank)) and
+                   bool(np.all(_dest(received["S"][~hs, 0], world) == rank)) and
+                   int(hr.sum()) == len(heavy) and  # every rank holds every heavy key's R tuple
+                   np.array_equal(np.sort(received["S"][hs, 1]), np.sort(myS[np.isin(myS[:, 0], heavy), 1])))
         out_q.put((rank, pairs[:int(n[0])].numpy().view(np.uint32).copy(), ok_dest,
-                   received["R"].shape[0], received["S"].shape[0]))
+                   received["R"].shape[0] - int(hr.sum()), received["S"].shape[0], dj.last_heavy))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_exchange_then_local_joins_equal_global_join(oracle, world):
+@pytest.mark.parametrize("world,hot", [(2, 0.0), (3, 0.0), (3, 0.2), (2, 0.3)])
+def test_exchange_then_local_joins_equal_global_join(oracle, world, hot):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, 7, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, 7, q, hot)) for r in range(world)]
     for p in procs:
         p.start()
     res = [q.get(timeout=240) for _ in range(world)]
     for p in procs:
         p.join(60)
         assert p.exitcode == 0
-    R, S = _dataset(7, 5000, 20000, world)
+    R, S = _dataset(7, 5000, 20000, hot)
     want = oracle.sort_pairs(oracle.simple_join(R, S))
     got = oracle.sort_pairs(np.concatenate([r[1] for r in res]))
     assert np.array_equal(got, want)
     assert all(r[2] for r in res), "a rank received keys of another destination"
-    assert sum(r[3] for r in res) == int((R[:, 0] != 0).sum())
+    heavy = res[0][5]
+    assert all(r[5] == heavy for r in res)  # every rank computed the same heavy list
+    assert (len(heavy) >= 2) == (hot > 0)
+    assert sum(r[3] for r in res) == int((R[:, 0] != 0).sum()) - len(heavy)
     assert sum(r[4] for r in res) == int((S[:, 0] != 0).sum())
 
 

@@ -24,7 +24,8 @@ def test_exchange_split_groups_by_destination(spj, oracle, world):
     dS = torch.from_numpy(S.view(np.int32)).cuda()
     out = torch.empty_like(dS)
     cnt = torch.empty(2 * world, dtype=torch.int64, device="cuda")
-    spj.check(spj.lib().spj_exchange_split(dS.data_ptr(), n_s, world, out.data_ptr(), cnt.data_ptr(), None))
+    spj.check(spj.lib().spj_exchange_split(dS.data_ptr(), n_s, world, 0, None, 0, 0, out.data_ptr(), cnt.data_ptr(),
+                                           None))
     torch.cuda.synchronize()
     counts = cnt[:world].cpu().numpy()
     keep = S[S[:, 0] != 0]
@@ -36,6 +37,31 @@ def test_exchange_split_groups_by_destination(spj, oracle, world):
         seg = got[off[r]:off[r + 1]]
         assert np.all(_dest(oracle, seg[:, 0], world) == r)
         assert np.array_equal(oracle.sort_pairs(seg), oracle.sort_pairs(keep[d == r]))
+
+
+@pytest.mark.parametrize("fused", [False, True])
+def test_distributed_join_heavy_keys_one_rank(spj, oracle, fused):
+    # Zipf 1.5: the top key is ~38% of S, so the heavy-key path (S kept, R
+    # replicated through the all-gather) runs even with one rank
+    import torch
+    import torch.distributed as dist
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            device_id=torch.device("cuda", 0))
+    try:
+        n_r, n_s = 1 << 17, 1 << 20
+        R, S, expect = spj.generate_host(n_r, n_s, 1.5, seed=23)
+        dj = spj.DistributedJoin(design=spj.make_design(rank_num=1), fused=fused, heavy="always")
+        pairs, n = dj.run(torch.from_numpy(R.view(np.int32)).cuda(), torch.from_numpy(S.view(np.int32)).cuda())
+        torch.cuda.synchronize()
+        got = pairs[:int(n.item())].cpu().numpy().view(np.uint32)
+        assert len(dj.last_heavy) >= 1
+        assert got.shape == (n_s, 2) and oracle.checksum(got) == expect
+        dj.close()
+    finally:
+        dist.destroy_process_group()
 
 
 def test_distributed_join_one_rank(spj, oracle):
@@ -77,7 +103,7 @@ def test_fused_scatter_into_several_receive_buffers(spj, oracle):
         C = []
         for t in dev:
             c = torch.empty(world, dtype=torch.int64, device="cuda")
-            spj.check(spj.lib().spj_exchange_count(t.data_ptr(), t.shape[0], world, c.data_ptr(), None))
+            spj.check(spj.lib().spj_exchange_count(t.data_ptr(), t.shape[0], world, 0, None, 0, 0, c.data_ptr(), None))
             C.append(c.tolist())
         bufs = [torch.empty((spj.exchange_layout(C, d)[2] + 8, 2), dtype=torch.int32, device="cuda")
                 for d in range(world)]
@@ -85,7 +111,7 @@ def test_fused_scatter_into_several_receive_buffers(spj, oracle):
         for src, t in enumerate(dev):
             offs = torch.tensor(spj.exchange_layout(C, src)[1], dtype=torch.int64, device="cuda")
             cur = torch.empty(world, dtype=torch.int64, device="cuda")
-            spj.check(spj.lib().spj_exchange_scatter(t.data_ptr(), t.shape[0], world, ptrs.data_ptr(),
+            spj.check(spj.lib().spj_exchange_scatter(t.data_ptr(), t.shape[0], world, src, None, 0, 0, ptrs.data_ptr(),
                                                      offs.data_ptr(), cur.data_ptr(), None))
         torch.cuda.synchronize()
         recv[rel] = [bufs[d][:spj.exchange_layout(C, d)[0]].cpu().numpy().view(np.uint32) for d in range(world)]
@@ -120,3 +146,38 @@ def test_distributed_join_fused_one_rank(spj, oracle):
         dj.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_exchange_split_routes_heavy_keys(spj, oracle, mode):
+    # heavy keys (sorted, unsigned): with mode 1 their tuples stay on rank `me`,
+    # with mode 2 they leave the exchange; every other tuple goes by the hash
+    import torch
+    world, me, n = 6, 4, 1 << 18
+    rng = np.random.default_rng(31)
+    keys = rng.integers(1, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    heavy = np.array(sorted({int(keys[5]), int(keys[77]), 0xFFFFFFF0, int(keys[1000])}), dtype=np.uint32)
+    keys[rng.random(n) < 0.3] = keys[5]
+    keys[::50] = 0xFFFFFFF0
+    T = np.stack([keys, np.arange(n, dtype=np.uint32)], axis=1)
+    dT = torch.from_numpy(T.view(np.int32)).cuda()
+    dH = torch.from_numpy(heavy.view(np.int32)).cuda()
+    out = torch.empty_like(dT)
+    cnt = torch.empty(2 * world, dtype=torch.int64, device="cuda")
+    spj.check(spj.lib().spj_exchange_split(dT.data_ptr(), n, world, me, dH.data_ptr(), len(heavy), mode,
+                                           out.data_ptr(), cnt.data_ptr(), None))
+    torch.cuda.synchronize()
+    d = _dest(oracle, T[:, 0], world)
+    hv = np.isin(T[:, 0], heavy)
+    keep = np.ones(n, dtype=bool)
+    if mode == 1:
+        d[hv] = me
+    else:
+        keep = ~hv
+    counts = cnt[:world].cpu().numpy()
+    assert np.array_equal(counts, np.bincount(d[keep], minlength=world))
+    got = out.cpu().numpy().view(np.uint32)[:int(counts.sum())]
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for r in range(world):
+        want = T[keep & (d == r)]
+        assert np.array_equal(oracle.sort_pairs(got[off[r]:off[r + 1]]), oracle.sort_pairs(want))
