@@ -846,45 +846,50 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
     if (cur_j != 0xffffffffu) warp_close(P.join[cur_j], w);
 }
 
-// Block-wide exclusive scan of n <= 256 counters by warp 0 (8 per lane); writes
-// off[0..n) and returns nothing (callers synchronise).
-__device__ __forceinline__ void warp0_scan256(const uint32_t *cnt, uint32_t *off, int n) {
+// Block-wide exclusive scan of n <= 1024 counters by warp 0 (8 per lane per
+// step); writes off[0..n] (off[n] = total); callers synchronise.
+__device__ __forceinline__ void warp0_scan1024(const uint32_t *cnt, uint32_t *off, int n) {
     if (threadIdx.x >= 32) return;
     const int lane = threadIdx.x;
-    uint32_t c[8], sum = 0;
+    uint32_t carry = 0;
+    for (int base = 0; base < n; base += 256) {  // 8 counters per lane per step
+        uint32_t c[8], sum = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        const int j = lane * 8 + i;
-        c[i] = j < n ? cnt[j] : 0;
-        sum += c[i];
-    }
-    uint32_t incl = sum;
+        for (int i = 0; i < 8; i++) {
+            const int j = base + lane * 8 + i;
+            c[i] = j < n ? cnt[j] : 0;
+            sum += c[i];
+        }
+        uint32_t incl = sum;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += x;
-    }
-    uint32_t run = incl - sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += x;
+        }
+        uint32_t run = carry + incl - sum;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        const int j = lane * 8 + i;
-        if (j < n) off[j] = run;
-        run += c[i];
+        for (int i = 0; i < 8; i++) {
+            const int j = base + lane * 8 + i;
+            if (j < n) off[j] = run;
+            run += c[i];
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
     }
-    if (lane == 31) off[n] = incl;
+    if (lane == 0) off[n] = carry;
 }
 
 // ---------------------------------------------------------- nested-loop join --
 // nested_loop_join.c:184-231 on B200. The R partition is counting-sorted in
-// shared memory into L sub-partitions (hash bits above the partition bits) of
-// about 64 tuples on average (well under the 256 of the sweep's definition);
+// shared memory into L <= 1024 sub-partitions (hash bits above the partition
+// bits) of about 16 tuples on average (well under the 256 of the sweep's
+// definition);
 // each S tuple compares its key with every R tuple of its sub-partition and takes
 // the first equal one. S is rewritten in place: unmatched S tuples are emitted
 // unchanged.
 __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
     extern __shared__ unsigned long long smem_u64[];
     __shared__ unsigned s_slot;
-    __shared__ uint32_t bcnt[256], boff[257];
+    __shared__ uint32_t bcnt[1024], boff[1025];
     Tuple *rs = reinterpret_cast<Tuple *>(smem_u64);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
@@ -904,15 +909,15 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
             nr = min(Rr.total[un.p], cap);
             if (threadIdx.x == 0 && Rr.total[un.p] > cap) atomicOr(&J.ctr->error, 1u);
             uint32_t L = 1;
-            while (L < 256 && L * 64 < nr) L <<= 1;
+            while (L < 1024 && L * 16 < nr) L <<= 1;
             lmask = L - 1;
-            for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) bcnt[i] = 0;
+            for (uint32_t i = threadIdx.x; i < 1024; i += blockDim.x) bcnt[i] = 0;
             __syncthreads();
             const Tuple *pr = Rr.out + Rr.base[un.p];
             for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x)
                 atomicAdd(&bcnt[(glb_partition_hash(pr[i].key) >> bits) & lmask], 1u);
             __syncthreads();
-            warp0_scan256(bcnt, boff, (int)L);
+            warp0_scan1024(bcnt, boff, (int)L);
             __syncthreads();
             for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) bcnt[i] = boff[i];
             __syncthreads();
@@ -958,25 +963,12 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
 
 // ----------------------------------------------------------- sort-merge join --
 // mpsm_join_sort_probe.c:152-236 on B200. The R partition is bitonic-sorted by
-// key in shared memory; S is taken in runs of 32 tuples that each warp sorts with
-// a shuffle network, and every sorted S key is merged into R by a lower-bound
-// search (merge path). A matched S tuple becomes (R.payload, S.payload), an
-// unmatched one stays as it is (S is rewritten in place).
-__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, j);
-            const bool up = (lane & k) == 0;
-            const bool low = (lane & j) == 0;
-            v = (low == up) ? (v < o ? v : o) : (v < o ? o : v);
-        }
-    }
-    return v;
-}
-
+// key in shared memory, and every S tuple finds its key in the sorted run by a
+// lower-bound search (the merge step of the reference, done per tuple: the
+// output is a multiset, so S need not be sorted first -- sorting each warp's 32
+// S tuples with a shuffle network cost 30% of the join). A matched S tuple
+// becomes (R.payload, S.payload), an unmatched one stays as it is (S is
+// rewritten in place).
 __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
     extern __shared__ unsigned long long sorted[];
     __shared__ unsigned s_slot;
@@ -1025,12 +1017,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
             const bool in = idx < un.s_end;
             Tuple t = in ? ps[idx] : Tuple{0u, 0u};
             const bool valid = in && t.key != 0;
-            const unsigned nvalid = __popc(__ballot_sync(0xffffffffu, valid));
-            unsigned long long v = valid ? ((unsigned long long)t.key << 32) | t.pay : ~0ull;
-            v = warp_sort32(v);
-            const bool mine = (unsigned)lane < nvalid;
-            t.key = (uint32_t)(v >> 32);
-            t.pay = (uint32_t)v;
+            const bool mine = valid;
             bool hit = false;
             uint32_t rp = 0;
             if (mine && nr) {
@@ -1428,9 +1415,13 @@ cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm)
     e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (1 << kMaxRadixBits) * 4);
     if (e) return e;
     // the largest table any plan may use, so plans of different sizes coexist
-    for (const void *k : {(const void *)k_join_phj, (const void *)k_join_smj, (const void *)k_join_nl})
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem - 1024 - 2048)))
+    for (const void *k : {(const void *)k_join_phj, (const void *)k_join_smj, (const void *)k_join_nl}) {
+        cudaFuncAttributes fa;
+        if ((e = cudaFuncGetAttributes(&fa, k))) return e;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      max_smem - (int)fa.sharedSizeBytes - 1024)))
             return e;
+    }
     e = cudaFuncSetAttribute(k_scatter1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));
     if (e) return e;
     e = cudaFuncSetAttribute(k_scatter2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));

@@ -78,7 +78,7 @@ static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 static int max_table_slots(int dev) {
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    return ((max_smem - 4096) / 8) & ~1;
+    return ((max_smem - 12288) / 8) & ~1;  // room for the join kernels' static shared memory
 }
 
 // ------------------------------------------------------------------ tuning --
@@ -132,7 +132,9 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
             // least 64 partitions per rank, and -- for a join that runs alone --
             // at least 8 partitions per SM so that a small join still fills the GPU
             // (in a batch the other joins do).
-            const uint64_t target = std::max<uint64_t>(1, (uint64_t)ts / 3);
+            // (the sort-merge join sorts each R partition in shared memory: half
+            // as large partitions keep its sort in a power of two below the table)
+            const uint64_t target = std::max<uint64_t>(1, (uint64_t)ts / (d.join_alg == SPJ_ALG_SMJ ? 6 : 3));
             const int need = ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + target - 1) / target));
             const int par = alone ? ceil_log2((uint64_t)8 * sms) : 0;
             const int minb = ceil_log2((uint64_t)64 * d.rank_num);
@@ -165,9 +167,12 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
         sh.chunk[r] = (uint32_t)c;
     }
     sh.item_target = (uint32_t)std::max<int64_t>(16384, (n_r + n_s) / (64 * sms));
-    // small joins reserve small output chunks, so a batch's output slack stays small
+    // small joins reserve small output chunks, so a batch's output slack stays
+    // small; in a batch every warp leaves a hole in each join it touched, so
+    // chunks stop at 256 pairs there (a quarter of the fix-up's data to move)
+    const uint32_t oc_max = batch_tuples > 0 ? 256u : (uint32_t)kOutChunk;
     uint32_t oc = 32;
-    while (oc < (uint32_t)kOutChunk && (int64_t)oc * 8192 < n_s) oc <<= 1;
+    while (oc < oc_max && (int64_t)oc * 8192 < n_s) oc <<= 1;
     sh.out_chunk = oc;
     sh.unit_tuples = d.unit_tuples > 0                ? (uint32_t)d.unit_tuples
                      : (tune && tune->unit_tuples > 0) ? (uint32_t)tune->unit_tuples
