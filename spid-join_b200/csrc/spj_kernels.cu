@@ -209,11 +209,13 @@ __global__ void __launch_bounds__(1024) k_basescan(PlanDev P) {
 // is the scatter itself.
 struct __align__(128) TileSmem {
     Tuple inbuf[2][kTile];     // bulk-copy double buffer of input tiles
-    Tuple stage[kTile];        // tile sorted by bucket
-    uint8_t bkt[kTile];
+    Tuple stage[kTile + 256];  // tile sorted by bucket (+1 spare slot per bucket with bulk stores)
+    uint8_t bkt[kTile];        // bucket of each stage slot (element stores)
     uint32_t cnt[256];
-    uint32_t off[256];
-    uint32_t wpos[256];        // cursor - off: global position of stage slot j is wpos[b] + j
+    uint32_t off[256];         // stage slot of the bucket's first tuple in this tile
+    uint32_t wpos[256];        // element stores: global position of stage slot j is wpos[b] + j
+    uint32_t len[256];         // bulk stores: the bucket's tuples in this tile
+    uint32_t gpos[256];        // bulk stores: global position of the bucket's first tuple
     uint32_t cursor[256];
     uint64_t bar[2];
     uint32_t valid;
@@ -225,13 +227,26 @@ struct __align__(128) TileSmem {
 // tiles arrive by bulk copy (TMA) into a double buffer, so the next tile is in
 // flight while this one is sorted and written. A tuple at an odd boundary index
 // is moved with an ordinary load (bulk copies need 16-byte alignment).
+// Each tile is counting-sorted by bucket in shared memory, then written out in
+// one of two ways (kBulk):
+//  * element stores: one stage slot per thread, consecutive threads write a
+//    bucket's run with coalesced stores;
+//  * bulk stores: each bucket's run starts at a stage slot of the same 16-byte
+//    parity as its global address (the spare slot per bucket absorbs the shift)
+//    and leaves as one bulk store (TMA) of its aligned body, plus at most one
+//    ordinary store at each end, issued by the bucket's thread. The writer
+//    threads' proxy fence is the price; long runs (hot buckets) repay it.
 // Returns false (the same value in every thread) when a bulk copy timed out.
-template <bool kHot, typename BucketFn>
+template <bool kHot, bool kBulk, typename BucketFn>
 __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint32_t b, uint32_t e,
                                               Tuple *__restrict__ out, TileSmem &S, int nb, BucketFn bucket_of,
                                               uint32_t (&uses)[2], unsigned int *err) {
     constexpr int PER = kTile / kScatterThreads;
+    constexpr uint32_t kBulkMin = 8;  // bulk-store bodies shorter than this go by ordinary stores
     uint2 *o2 = reinterpret_cast<uint2 *>(out);
+    const uint2 *st2 = reinterpret_cast<const uint2 *>(S.stage);
+    const uint32_t par0 = (uint32_t)(reinterpret_cast<uintptr_t>(out) >> 3) & 1u;  // address parity of out[0]
+    const bool writer = kBulk && (int)threadIdx.x < nb;
     if (b >= e) return true;
     if (threadIdx.x < 2) {  // boundary tuples at odd indices
         const bool head = threadIdx.x == 0;
@@ -270,6 +285,7 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
         if (__syncthreads_or(!ok)) {  // a copy timed out (error bit set): all threads stop alike
             // copies already issued may still land: give them a bounded wait before leaving
             if (threadIdx.x == 0 && t + 1 < ntiles) mbar_wait(&S.bar[buf ^ 1], uses[buf ^ 1] & 1u, err);
+            if (writer) bulk_wait_all();
             return false;
         }
         Tuple v[PER];
@@ -294,15 +310,16 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
             }
             br[k] = bk != 0xffffu ? (bk << 16) | atomicAdd(&S.cnt[bk], 1u) : 0xffff0000u;
         }
+        if (writer) bulk_wait_read();  // the previous tile's bulk stores have read the stage
         __syncthreads();
-        if (threadIdx.x < 32) {  // exclusive scan of the <= 256 bucket counts
+        if (threadIdx.x < 32) {  // exclusive scan of the <= 256 bucket counts (+1 each with bulk stores)
             const int lane = threadIdx.x;
             uint32_t c[8], sum = 0;
 #pragma unroll
             for (int i = 0; i < 8; i++) {
                 const int j = lane * 8 + i;
                 c[i] = j < nb ? S.cnt[j] : 0;
-                sum += c[i];
+                sum += j < nb ? c[i] + (kBulk ? 1u : 0u) : 0u;
             }
             uint32_t incl = sum;
 #pragma unroll
@@ -315,14 +332,22 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
             for (int i = 0; i < 8; i++) {
                 const int j = lane * 8 + i;
                 if (j < nb) {
-                    S.off[j] = run;
-                    S.wpos[j] = S.cursor[j] - run;
-                    S.cursor[j] += c[i];
+                    const uint32_t g = S.cursor[j];
+                    if (kBulk) {
+                        S.off[j] = run + ((run ^ (g + par0)) & 1u);
+                        S.len[j] = c[i];
+                        S.gpos[j] = g;
+                        run += c[i] + 1;
+                    } else {
+                        S.off[j] = run;
+                        S.wpos[j] = g - run;
+                        run += c[i];
+                    }
+                    S.cursor[j] = g + c[i];
                     S.cnt[j] = 0;
                 }
-                run += c[i];
             }
-            if (lane == 31) S.valid = incl;
+            if (!kBulk && lane == 31) S.valid = incl;
         }
         __syncthreads();
 #pragma unroll
@@ -331,35 +356,65 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
             if (bk != 0xffffu) {
                 const uint32_t slot = S.off[bk] + (br[k] & 0xffffu);
                 S.stage[slot] = v[k];
-                S.bkt[slot] = (uint8_t)bk;
+                if (!kBulk) S.bkt[slot] = (uint8_t)bk;
             }
         }
-        __syncthreads();
-        // write phase, unrolled so all shared loads are in flight before the stores
-        const uint32_t valid = S.valid;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const uint32_t j = threadIdx.x + k * kScatterThreads;
-            if (j < valid) {
-                v[k] = S.stage[j];
-                br[k] = S.bkt[j];
+        if (kBulk) {
+            fence_proxy_async_smem();  // the stage writes before the bulk stores that read them
+            __syncthreads();
+            if (writer) {  // bucket threadIdx.x's run of this tile
+                uint32_t c = S.len[threadIdx.x];
+                if (c) {
+                    uint32_t g = S.gpos[threadIdx.x], sl = S.off[threadIdx.x];
+                    if ((g + par0) & 1u) {  // head tuple up to the 16-byte boundary
+                        o2[g++] = st2[sl++];
+                        c--;
+                    }
+                    const uint32_t body = c & ~1u;
+                    if (body >= kBulkMin) {
+                        bulk_store(o2 + g, st2 + sl, body * 8);
+                        bulk_commit();
+                    } else {
+                        for (uint32_t i = 0; i < body; i++) o2[g + i] = st2[sl + i];
+                    }
+                    if (c & 1u) o2[g + body] = st2[sl + body];
+                }
             }
-        }
+            // the next tile's rank phase may start: counts are zero, and the stage
+            // is rewritten only after its writers' bulk stores have read it
+        } else {
+            __syncthreads();
+            // write phase, unrolled so all shared loads are in flight before the stores
+            const uint32_t valid = S.valid;
 #pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const uint32_t j = threadIdx.x + k * kScatterThreads;
-            if (j < valid) br[k] = S.wpos[br[k]] + j;
-        }
+            for (int k = 0; k < PER; k++) {
+                const uint32_t j = threadIdx.x + k * kScatterThreads;
+                if (j < valid) {
+                    v[k] = S.stage[j];
+                    br[k] = S.bkt[j];
+                }
+            }
 #pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const uint32_t j = threadIdx.x + k * kScatterThreads;
-            if (j < valid) o2[br[k]] = make_uint2(v[k].key, v[k].pay);
+            for (int k = 0; k < PER; k++) {
+                const uint32_t j = threadIdx.x + k * kScatterThreads;
+                if (j < valid) br[k] = S.wpos[br[k]] + j;
+            }
+#pragma unroll
+            for (int k = 0; k < PER; k++) {
+                const uint32_t j = threadIdx.x + k * kScatterThreads;
+                if (j < valid) o2[br[k]] = make_uint2(v[k].key, v[k].pay);
+            }
+            // the next tile's rank phase may start: counts are zero, and its first
+            // barrier orders these reads of stage/wpos before they are rewritten
         }
-        // the next tile's rank phase may start: counts are zero, and its first
-        // barrier orders these reads of stage/wpos before they are rewritten
     }
+    if (writer) bulk_wait_read();
     return true;
 }
+
+// Bulk stores pay for their proxy fence once runs average 32 tuples or more:
+// passes of at most 128 buckets, and pass-2 segments of one heavy chunk.
+constexpr int kBulkMaxBuckets = 128;
 
 __device__ __forceinline__ void tile_init(TileSmem &S) {
     for (int i = threadIdx.x; i < 256; i += blockDim.x) S.cnt[i] = 0;
@@ -398,9 +453,12 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
     const uint32_t e0 = min(R.n, b0 + R.chunk);
     Tuple *dst = b2 ? R.tmp : R.out;
     uint32_t uses[2] = {0, 0};
-    scatter_range<false>(R.in, b0, e0, dst, S, nb,
-                  [=](uint32_t key) { return (int)((glb_partition_hash(key) & mask) >> b2); }, uses,
-                  &J.ctr->error);
+    auto coarse = [=](uint32_t key) { return (int)((glb_partition_hash(key) & mask) >> b2); };
+    if (nb <= kBulkMaxBuckets)
+        scatter_range<false, true>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error);
+    else
+        scatter_range<false, false>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error);
+    bulk_wait_all();  // this thread's bulk stores are performed before the CTA retires
 }
 
 // Work list of pass 2: for every (relation, coarse bucket), runs of consecutive
@@ -501,11 +559,15 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
         __syncthreads();
         const uint32_t beg = R.base[cb << b2] + S.seg_begin;
         auto fine = [=](uint32_t key) { return (int)(glb_partition_hash(key) & qmask); };
-        const bool ok = hot ? scatter_range<true>(R.tmp, beg, beg + S.seg_len, R.out, S, nb, fine, uses, &J.ctr->error)
-                            : scatter_range<false>(R.tmp, beg, beg + S.seg_len, R.out, S, nb, fine, uses, &J.ctr->error);
+        const uint32_t e2 = beg + S.seg_len;
+        const bool ok = hot ? scatter_range<true, true>(R.tmp, beg, e2, R.out, S, nb, fine, uses, &J.ctr->error)
+                        : nb <= kBulkMaxBuckets
+                            ? scatter_range<false, true>(R.tmp, beg, e2, R.out, S, nb, fine, uses, &J.ctr->error)
+                            : scatter_range<false, false>(R.tmp, beg, e2, R.out, S, nb, fine, uses, &J.ctr->error);
         __syncthreads();
         if (!ok) break;
     }
+    bulk_wait_all();  // this thread's bulk stores are performed before the CTA retires
 }
 
 // ----------------------------------------------------------------- units --
@@ -828,6 +890,9 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
         const Tuple *ps = P.rel[2 * un.join + 1].out;
         constexpr int U = 4;
         for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
+            // the warp's next 128 S tuples (8 lines) start towards L2 while these are probed
+            const uint32_t nxt = base + nwarps * 32 * U + lane * 16;
+            if (lane < 8 && nxt < un.s_end) prefetch_l2(ps + nxt);
             Tuple t[U];
 #pragma unroll
             for (int k = 0; k < U; k++) {
