@@ -158,15 +158,32 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, uuid=None):
+    def __init__(self, uuid=None, period_ms=20):
+        """Starts nvidia-smi sampling every `period_ms` and waits (at most 5 s)
+        for its first sample, so that sampling is running before the timed
+        region begins."""
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        cmd = ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "100"]
+        cmd = ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", str(period_ms)]
         if uuid:
             cmd.append("--id=" + uuid)
+        self.mark_rows = 0
         try:
             self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < 5.0 and not self._rows():
+            time.sleep(0.02)
+
+    def _rows(self):
+        self.f.flush()
+        with open(self.f.name) as g:
+            return [ln.strip().split(", ") for ln in g if ln.strip()]
+
+    def mark(self):
+        """The timed region starts now: only later samples are reported."""
+        if self.p is not None:
+            self.mark_rows = len(self._rows())
 
     def stop(self):
         if self.p is None:
@@ -176,10 +193,11 @@ class ClockSampler:
             self.p.wait(5)
         except Exception:
             self.p.kill()
-        self.f.flush()
-        self.f.seek(0)
-        rows = [ln.strip().split(", ") for ln in self.f if ln.strip()]
+        rows = self._rows()
         os.unlink(self.f.name)
+        timed = rows[self.mark_rows:]
+        # a timed region shorter than the sampling period: the last sample before its end
+        rows, window = (timed, "timed region") if timed else (rows[-1:], "last sample before the timed region ended")
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
@@ -194,7 +212,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window": window}
 
 
 # ---------------------------------------------------------------- our arm --
@@ -264,6 +282,8 @@ def run_ours(args):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    if sampler:
+        sampler.mark()
     ev0.record(stream)
     for _ in range(args.steps):
         step()
@@ -441,6 +461,8 @@ def run_distributed(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dist.barrier()
     torch.cuda.synchronize()
+    if sampler:
+        sampler.mark()
     ev0.record(stream)
     for _ in range(args.steps):
         pairs, n = dj.run(dR, dS)
@@ -579,6 +601,7 @@ def run_batched(args):
     sampler = ClockSampler()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    sampler.mark()
     ev0.record()
     for _ in range(args.steps):
         graph.replay()
@@ -781,6 +804,7 @@ def run_served(args):
 
     serve_stream(spj, server, pool, R, S, outs, n_out, 0, 1.0, 64, SEED)  # warm-up burst
     sampler = ClockSampler()
+    sampler.mark()
     served = leg(server, args.c5_rate, args.c5_seconds, 1 << 20, SEED + 1)
     clocks = sampler.stop()
     sat = leg(server, 0, args.c5_sat_seconds, 256, SEED + 2)
