@@ -106,7 +106,9 @@ int spj_load_column(spj_handle_t *h, const void *tuples, int64_t num_tuples, int
 int spj_prepare(spj_handle_t *h, const spj_design_t *design);
 
 /* void StartJoin(join_design_t), include/join_internals.hpp:321: enqueues the
- * column copies and the join on the instance's stream and returns. */
+ * column copies and the join on the instance's stream and returns. Columns
+ * loaded since the last spj_prepare are prepared for first (with the current
+ * design). */
 int spj_start(spj_handle_t *h, const spj_design_t *design);
 
 typedef struct {

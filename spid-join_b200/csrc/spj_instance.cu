@@ -13,8 +13,12 @@
 // slices so that the three streams of an instance overlap: slice i+1 is copied
 // to the device while slice i is joined and slice i-1's pairs are copied back
 // (the host link carries both directions at once). Every slice joins all of R,
-// so the union of the slices' outputs is the join's output. Instances are
-// independent.
+// so the union of the slices' outputs is the join's output. R is partitioned
+// once per join: the slices after the first reuse its partitions and count and
+// scatter only their own S, so slices can be small and the tail after the last
+// input copy (the last slice's join and result copy) short. All slices have
+// one length and one plan: the device copy of S is padded to whole slices with
+// key-0 tuples, the empty key, which no pass keeps. Instances are independent.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -28,9 +32,12 @@
 using namespace spj;
 
 namespace {
-constexpr int kMaxSlices = 16;
-constexpr int64_t kSliceMin = 1ll << 24;     // host S below this is joined in one piece
-constexpr int64_t kSliceTuples = 1ll << 25;  // target S tuples per slice
+constexpr int kMaxSlices = 32;
+constexpr int64_t kSliceMin = 1ll << 24;  // host S below this is joined in one piece
+// Target S tuples per slice. Every slice's join still builds the tables of all
+// of R's partitions (~1.4 ms for 2^27 R tuples), so a slice must carry enough S
+// for its upload to cover that: 2^24 tuples (128 MiB, ~2.6 ms of upload).
+constexpr int64_t kSliceTuples = 1ll << 24;
 }  // namespace
 
 struct spj_handle {
@@ -40,12 +47,12 @@ struct spj_handle {
     bool col_set[2] = {false, false};
     bool on_device[2] = {false, false};
     spj_design_t design{};
-    spj_plan_t *plan = nullptr;       // joins R with a full slice
-    spj_plan_t *plan_last = nullptr;  // joins R with a shorter last slice (or null)
+    spj_plan_t *plan = nullptr;  // joins R with one slice
     int nslices = 1;
-    int64_t slice = 0;      // S tuples per slice (multiple of 256; the last may be shorter)
+    int64_t slice = 0;      // S tuples per slice (multiple of 256 when sliced)
     int64_t slice_cap = 0;  // output pairs reserved per slice on the device
     bool started = false;
+    bool loaded = false;  // a column was loaded after the last prepare
     cudaStream_t stream = nullptr, s_in = nullptr, s_out = nullptr;  // joins, host->device, device->host
     spj_kv_pair_t *d_col[2] = {nullptr, nullptr};  // device copies of host columns
     spj_kv_pair_t *d_out = nullptr;                // nslices x slice_cap pairs
@@ -70,17 +77,13 @@ static void free_buffers(spj_handle_t *h) {
     cudaFree(h->d_out);
     h->d_out = nullptr;
     if (h->plan) spj_plan_destroy(h->plan);
-    if (h->plan_last) spj_plan_destroy(h->plan_last);
-    h->plan = h->plan_last = nullptr;
+    h->plan = nullptr;
     h->nslices = 1;
 }
 
-static spj_plan_t *slice_plan(spj_handle_t *h, int i) {
-    return (i == h->nslices - 1 && h->plan_last) ? h->plan_last : h->plan;
-}
-
+// Host S tuples of slice i (the device copy of a sliced S is padded to whole slices).
 static int64_t slice_len(const spj_handle_t *h, int i) {
-    return std::min(h->slice, h->n[1] - (int64_t)i * h->slice);
+    return std::max<int64_t>(0, std::min(h->slice, h->n[1] - (int64_t)i * h->slice));
 }
 
 extern "C" {
@@ -137,6 +140,7 @@ int spj_load_column(spj_handle_t *h, const void *tuples, int64_t num_tuples, int
     h->n[side] = num_tuples;
     h->on_device[side] = dev;
     h->col_set[side] = true;
+    h->loaded = true;
     return SPJ_OK;
 }
 
@@ -144,6 +148,7 @@ int spj_prepare(spj_handle_t *h, const spj_design_t *design) {
     if (!h) return set_error(SPJ_E_ARG, "handle is NULL");
     if (h->started) return set_error(SPJ_E_STATE, "join in flight; call spj_finish first");
     if (!h->col_set[0] || !h->col_set[1]) return set_error(SPJ_E_STATE, "load both columns before prepare");
+    h->loaded = false;
     spj_design_t d = design ? *design : h->design;
     // the instance's rank layout is authoritative (JoinInstance(r, R, r/R))
     d.rank_num = h->ranks;
@@ -160,8 +165,7 @@ int spj_prepare(spj_handle_t *h, const spj_design_t *design) {
     bool same_copies = true;  // device copies exist exactly for the host columns
     for (int i = 0; i < 2; i++) same_copies &= (h->d_col[i] != nullptr) == (!h->on_device[i] && h->n[i] > 0);
     if (h->plan && same_copies && h->plan->n_r == h->n[0] && h->nslices == ns && h->slice == slice &&
-        h->n[1] == (int64_t)(ns - 1) * slice + (h->plan_last ? h->plan_last->n_s : slice) &&
-        memcmp(&h->plan->design, &d, sizeof(d)) == 0) {
+        h->plan->n_s == slice && memcmp(&h->plan->design, &d, sizeof(d)) == 0) {
         h->design = d;
         return SPJ_OK;  // reuse the plans and their buffers
     }
@@ -169,16 +173,15 @@ int spj_prepare(spj_handle_t *h, const spj_design_t *design) {
     h->nslices = ns;
     h->slice = slice;
     int rc = spj_plan_create(h->n[0], slice, &d, &h->plan);
-    const int64_t last = h->n[1] - (int64_t)(ns - 1) * slice;
-    if (rc == SPJ_OK && last != slice) rc = spj_plan_create(h->n[0], last, &d, &h->plan_last);
     if (rc) {
         free_buffers(h);
         return rc;
     }
     h->design = d;
     cudaError_t e = cudaSuccess;
+    const int64_t s_dev = ns > 1 ? (int64_t)ns * slice : h->n[1];  // device S tuples, padding included
     for (int i = 0; i < 2 && e == cudaSuccess; i++)
-        if (!h->on_device[i] && h->n[i] > 0) e = cudaMalloc(&h->d_col[i], (size_t)h->n[i] * 8);
+        if (!h->on_device[i] && h->n[i] > 0) e = cudaMalloc(&h->d_col[i], (size_t)(i ? s_dev : h->n[0]) * 8);
     h->slice_cap = spj_plan_output_capacity(h->plan);
     if (e == cudaSuccess) e = cudaMalloc(&h->d_out, (size_t)h->slice_cap * ns * 8);
     if (e == cudaSuccess && h->h_out_cap < h->n[1]) {
@@ -199,6 +202,10 @@ int spj_start(spj_handle_t *h, const spj_design_t *design) {
     if (!h) return set_error(SPJ_E_ARG, "handle is NULL");
     if (!h->plan) return set_error(SPJ_E_STATE, "spj_prepare must precede spj_start");
     if (h->started) return set_error(SPJ_E_STATE, "join already started");
+    if (h->loaded) {  // columns changed since the last prepare: size the plans for them
+        int rc = spj_prepare(h, &h->design);
+        if (rc) return rc;
+    }
     if (design) {
         spj_design_t d = *design;
         d.rank_num = h->ranks;
@@ -214,7 +221,10 @@ int spj_start(spj_handle_t *h, const spj_design_t *design) {
         col[i] = h->n[i] == 0 ? h->d_out  // never read; any aligned device pointer
                               : h->on_device[i] ? (const spj_kv_pair_t *)h->col[i] : h->d_col[i];
     cudaError_t e = cudaSuccess;
-    if (!h->on_device[0] && h->n[0] > 0)
+    const int64_t s_dev = h->nslices > 1 ? (int64_t)h->nslices * h->slice : h->n[1];
+    if (s_dev > h->n[1])  // key-0 padding of the last slice, before its copy on the same stream
+        e = cudaMemsetAsync(h->d_col[1] + h->n[1], 0, (size_t)(s_dev - h->n[1]) * 8, h->s_in);
+    if (e == cudaSuccess && !h->on_device[0] && h->n[0] > 0)
         e = cudaMemcpyAsync(h->d_col[0], h->col[0], (size_t)h->n[0] * 8, cudaMemcpyHostToDevice, h->s_in);
     for (int i = 0; i < h->nslices && e == cudaSuccess; i++) {
         const int64_t off = (int64_t)i * h->slice, len = slice_len(h, i);
@@ -226,12 +236,13 @@ int spj_start(spj_handle_t *h, const spj_design_t *design) {
     if (e == cudaSuccess && h->events) e = cudaEventRecord(h->ev[1], h->s_in);
     if (e != cudaSuccess) return cuda_error(e, "column copy");
     for (int i = 0; i < h->nslices; i++) {
-        spj_plan_t *pl = slice_plan(h, i);
+        spj_plan_t *pl = h->plan;
         const int64_t off = (int64_t)i * h->slice;
         e = cudaStreamWaitEvent(h->stream, h->ev_in[i], 0);
         if (e != cudaSuccess) return cuda_error(e, "slice dependency");
-        int rc = spj_plan_execute(pl, col[0], h->n[1] ? col[1] + off : col[1], h->d_out + (size_t)i * h->slice_cap,
-                                  h->d_n + i, h->stream);
+        // slice 0 partitions R; the later slices reuse its partitions
+        int rc = plan_execute(pl, col[0], h->n[1] ? col[1] + off : col[1], h->d_out + (size_t)i * h->slice_cap,
+                              h->d_n + i, h->stream, i > 0);
         if (rc) return rc;
         e = cudaMemcpyAsync(h->h_n + i, h->d_n + i, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess)
@@ -292,7 +303,7 @@ int spj_record_logs(spj_handle_t *h, spj_stats_t *out, int print) {
     if (!h) return set_error(SPJ_E_ARG, "handle is NULL");
     if (!h->plan) return set_error(SPJ_E_STATE, "no join has run");
     spj_stats_t st;
-    int rc = spj_plan_stats(slice_plan(h, h->nslices - 1), &st);  // the last slice's join
+    int rc = spj_plan_stats(h->plan, &st);  // the last slice's join
     st.n_pairs = h->n_pairs;
     st.h2d_ms = h->h2d_ms;
     st.d2h_ms = h->d2h_ms;

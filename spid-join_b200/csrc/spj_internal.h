@@ -180,8 +180,13 @@ const spj_tuning_t *find_tuning(int64_t n_r, int64_t n_s, spj_tuning_t *out);
 // and fills pl->dev, the per-join descriptors and the host image of the
 // descriptor arrays.
 size_t layout_plan(spj_plan *pl, char *arena, bool image);
-cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st);
-cudaError_t init_single(spj_plan *pl, cudaStream_t st);
+// keep_r (one-join plans): R's partitions from the plan's previous execution on
+// the same stream are reused; only S is counted and scattered.
+cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r = false);
+cudaError_t init_single(spj_plan *pl, cudaStream_t st, bool keep_r = false);
+// spj_plan_execute with keep_r (see launch_pipeline).
+int plan_execute(spj_plan *pl, const spj_kv_pair_t *r, const spj_kv_pair_t *s, spj_kv_pair_t *out, int64_t *n_out,
+                 cudaStream_t st, bool keep_r);
 cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm);
 int create_plan_stream(int J, const int64_t *n_r, const int64_t *n_s, const spj_design_t *design,
                        const spj_kv_pair_t *const *r, const spj_kv_pair_t *const *s, spj_kv_pair_t *const *out,

@@ -50,21 +50,24 @@ __device__ __forceinline__ uint32_t find_slot(const uint32_t *prefix, uint32_t n
 }
 
 // Writes the descriptors of a one-join plan from kernel parameters (no host copy).
+// With keep_r, R owns no chunk, partition or coarse bucket of the count and
+// scatter grids (its partitions are reused), and every CTA of them maps to S.
 __global__ void k_init_single(PlanDev P, RelDev r0, RelDev r1, JoinDev j0, uint32_t nch0, uint32_t nch1, uint32_t f,
-                              uint32_t f1) {
+                              uint32_t f1, bool keep_r) {
     if (threadIdx.x != 0) return;
     P.rel[0] = r0;
     P.rel[1] = r1;
     P.join[0] = j0;
+    const uint32_t rch = keep_r ? 0u : nch0, rf = keep_r ? 0u : f, rf1 = keep_r ? 0u : f1;
     P.chunk_prefix[0] = 0;
-    P.chunk_prefix[1] = nch0;
-    P.chunk_prefix[2] = nch0 + nch1;
+    P.chunk_prefix[1] = rch;
+    P.chunk_prefix[2] = rch + nch1;
     P.part_prefix[0] = 0;
-    P.part_prefix[1] = f;
-    P.part_prefix[2] = 2 * f;
+    P.part_prefix[1] = rf;
+    P.part_prefix[2] = rf + f;
     P.coarse_prefix[0] = 0;
-    P.coarse_prefix[1] = f1;
-    P.coarse_prefix[2] = 2 * f1;
+    P.coarse_prefix[1] = rf1;
+    P.coarse_prefix[2] = rf1 + f1;
     P.jpart_prefix[0] = 0;
     P.jpart_prefix[1] = f;
 }
@@ -1406,16 +1409,27 @@ __global__ void k_hist_single(const Tuple *t, uint64_t n, int bits, uint32_t *hi
 // Entry points used by spj_plan.cu and spj_noalloc.cu (C++ linkage, internal).
 namespace spj {
 
-cudaError_t init_single(spj_plan *pl, cudaStream_t st) {
+cudaError_t init_single(spj_plan *pl, cudaStream_t st, bool keep_r) {
     const JoinHost &h = pl->joins[0];
     const uint32_t f = 1u << h.dev.bits;
     const uint32_t f1 = h.dev.fine_bits ? 1u << (h.dev.bits - h.dev.fine_bits) : 0u;
-    k_init_single<<<1, 32, 0, st>>>(pl->dev, h.rel[0], h.rel[1], h.dev, h.rel[0].nchunks, h.rel[1].nchunks, f, f1);
+    k_init_single<<<1, 32, 0, st>>>(pl->dev, h.rel[0], h.rel[1], h.dev, h.rel[0].nchunks, h.rel[1].nchunks, f, f1,
+                                    keep_r && pl->dev.alg != SPJ_ALG_NPHJ);
     return cudaGetLastError();
 }
 
-cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st) {
-    PlanDev &P = pl->dev;
+cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
+    PlanDev P = pl->dev;
+    if (keep_r && P.alg != SPJ_ALG_NPHJ) {
+        // one-join plan whose R partitions (out, hist offsets, totals) are still in
+        // its buffers from its previous execution: count and scatter S only. The
+        // base scan still runs over both relations (it rederives R's bases and
+        // largest partition from the kept totals).
+        const JoinHost &h = pl->joins[0];
+        P.total_chunks = h.rel[1].nchunks;
+        P.total_parts = 1u << h.dev.bits;
+        P.total_coarse = h.dev.fine_bits ? 1u << (h.dev.bits - h.dev.fine_bits) : 0u;
+    }
     // timing events are recorded on eager launches only (not while a graph is captured)
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st, &cap);

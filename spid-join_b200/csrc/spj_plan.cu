@@ -16,7 +16,6 @@
 
 namespace spj {
 
-cudaError_t init_single(spj_plan *pl, cudaStream_t st);
 cudaError_t launch_checksum(const spj_kv_pair_t *pairs, const int64_t *n_dev, uint64_t *sum_dev, int sms,
                             cudaStream_t st);
 cudaError_t launch_generate(uint64_t seed, int64_t n_r, int64_t n_s, double zipf_s, spj_kv_pair_t *r,
@@ -531,6 +530,29 @@ int64_t join_output_capacity(int64_t n_r, int64_t n_s, const spj_design_t &d, bo
     return n_s + (int64_t)blocks * (kJoinThreads / 32) * sh.out_chunk;
 }
 
+// Executes a one-join plan; with keep_r, R's partitions from the plan's previous
+// execution on the same stream are reused (only S is counted and scattered).
+int plan_execute(spj_plan *pl, const spj_kv_pair_t *r, const spj_kv_pair_t *s, spj_kv_pair_t *out, int64_t *n_out,
+                 cudaStream_t st, bool keep_r) {
+    if (!pl) return set_error(SPJ_E_ARG, "plan is NULL");
+    if (pl->joins.size() != 1) return set_error(SPJ_E_ARG, "a batch plan runs with spj_batch_execute");
+    if ((pl->n_r && !r) || (pl->n_s && !s) || !out) return set_error(SPJ_E_ARG, "NULL column or output");
+    if (((uintptr_t)r & 15) || ((uintptr_t)s & 15) || ((uintptr_t)out & 7))
+        return set_error(SPJ_E_ARG, "columns must be 16-byte aligned and the output 8-byte aligned");
+    JoinHost &h = pl->joins[0];
+    // an empty relation still needs a readable, aligned column pointer
+    h.rel[0].in = r ? reinterpret_cast<const Tuple *>(r) : reinterpret_cast<const Tuple *>(out);
+    h.rel[1].in = s ? reinterpret_cast<const Tuple *>(s) : reinterpret_cast<const Tuple *>(out);
+    h.dev.out = reinterpret_cast<Tuple *>(out);
+    h.dev.n_out_user = reinterpret_cast<unsigned long long *>(n_out);
+    cudaError_t e = init_single(pl, st, keep_r);
+    if (e != cudaSuccess) return cuda_error(e, "descriptor kernel");
+    SPJ_CUDA(cudaMemsetAsync(pl->dev.bctr, 0, sizeof(BatchCtr) + sizeof(JoinCtr), st));
+    e = launch_pipeline(pl, st, keep_r);
+    if (e != cudaSuccess) return cuda_error(e, "join kernels");
+    return SPJ_OK;
+}
+
 }  // namespace spj
 
 extern "C" {
@@ -545,25 +567,9 @@ int64_t spj_plan_output_capacity(const spj_plan_t *plan) {
 
 int spj_plan_execute(spj_plan_t *pl, const spj_kv_pair_t *r, const spj_kv_pair_t *s, spj_kv_pair_t *out,
                      int64_t *n_out, void *stream) {
-    if (!pl) return set_error(SPJ_E_ARG, "plan is NULL");
-    if (pl->joins.size() != 1) return set_error(SPJ_E_ARG, "a batch plan runs with spj_batch_execute");
-    if ((pl->n_r && !r) || (pl->n_s && !s) || !out) return set_error(SPJ_E_ARG, "NULL column or output");
-    if (((uintptr_t)r & 15) || ((uintptr_t)s & 15) || ((uintptr_t)out & 7))
-        return set_error(SPJ_E_ARG, "columns must be 16-byte aligned and the output 8-byte aligned");
-    cudaStream_t st = (cudaStream_t)stream;
-    JoinHost &h = pl->joins[0];
-    // an empty relation still needs a readable, aligned column pointer
-    h.rel[0].in = r ? reinterpret_cast<const Tuple *>(r) : reinterpret_cast<const Tuple *>(out);
-    h.rel[1].in = s ? reinterpret_cast<const Tuple *>(s) : reinterpret_cast<const Tuple *>(out);
-    h.dev.out = reinterpret_cast<Tuple *>(out);
-    h.dev.n_out_user = reinterpret_cast<unsigned long long *>(n_out);
-    cudaError_t e = init_single(pl, st);
-    if (e != cudaSuccess) return cuda_error(e, "descriptor kernel");
-    SPJ_CUDA(cudaMemsetAsync(pl->dev.bctr, 0, sizeof(BatchCtr) + sizeof(JoinCtr), st));
-    e = launch_pipeline(pl, st);
-    if (e != cudaSuccess) return cuda_error(e, "join kernels");
-    return SPJ_OK;
+    return plan_execute(pl, r, s, out, n_out, (cudaStream_t)stream, false);
 }
+
 
 static void fill_stats(const spj_plan *pl, const JoinCtr &c, spj_stats_t *out) {
     out->n_pairs = (int64_t)c.n_out;

@@ -221,11 +221,14 @@ def test_algorithms_edge_sizes(spj, oracle, alg, nr, ns):
     assert same_multiset(oracle, out, oracle.simple_join(R, S, keep_unmatched=alg in ("smj", "nl")))
 
 
-@pytest.mark.parametrize("alg", [0, 2])
+@pytest.mark.parametrize("alg", [0, 1, 2, 3])
 def test_host_columns_joined_in_overlapped_slices(spj, oracle, alg):
     # |S| above 2^26 host tuples: the instance joins S in slices (copy-in,
-    # join and copy-out of different slices overlap); the last slice is
-    # shorter. The union of the slices must be the whole join, twice in a row.
+    # join and copy-out of different slices overlap); the first slice is
+    # shorter and has a plan of its own, and every slice after the first of
+    # its plan reuses R's partitions. The union of the slices must be the whole
+    # join, twice in a row, and again after both columns are replaced by new
+    # ones of the same sizes (the plans are reused; R is partitioned anew).
     n_r, n_s = 1 << 22, (1 << 26) + (1 << 20) + 7
     R, S, expect = spj.generate_host(n_r, n_s, 1.0, seed=77)
     inst = spj.JoinInstance(4, 4, 1)
@@ -239,5 +242,12 @@ def test_host_columns_joined_in_overlapped_slices(spj, oracle, alg):
         assert out.shape == (n_s, 2)
         assert oracle.checksum(out) == expect
     logs = inst.RecordLogs()
-    inst.close()
     assert logs["n_pairs"] == n_s
+    R2, S2, expect2 = spj.generate_host(n_r, n_s, 0.5, seed=78)
+    inst.LoadColumn(R2, n_r, "left")
+    inst.LoadColumn(S2, n_s, "right")
+    inst.PrepareJoin(d)
+    inst.StartJoin(d)
+    out = inst.FinishJoin().pairs()
+    inst.close()
+    assert out.shape == (n_s, 2) and oracle.checksum(out) == expect2
