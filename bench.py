@@ -72,13 +72,16 @@ def emit(obj):
 
 
 # ------------------------------------------------------------ CPU baseline --
-def cpu_reference_run(wl, steps, warmup):
+def cpu_reference_run(wl, steps, warmup, layout=None):
     """The reference's pipeline restated in C on all host cores, on a sample of
-    the workload: returns (tuples/s per step list, description, cores)."""
+    the workload (with rank layout `layout`, default the workload's): returns
+    (tuples/s per step list, description, cores)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     import spidjoin
     n_r, n_s, zipf, (ranks, rsets, bset), _ = WORKLOADS[wl]
+    if layout:
+        ranks, rsets, bset = layout
     sr, ss = max(n_r // CPU_SAMPLE_DIV, 1), max(n_s // CPU_SAMPLE_DIV, 1)
     R, S, expect = spidjoin.generate_host(sr, ss, zipf, seed=SEED)
     cores = os.cpu_count() or 1
@@ -139,9 +142,9 @@ def run_reference(args):
                 if args.workload == "c4" else
                 "served join stream, |R| log-uniform [2^10, 2^22], R:S in {1,2,4,8}, Zipf s ~ U[0, 1.5]")
     else:
-        rates, sample, cores = cpu_reference_run(args.workload, args.steps, args.warmup)
-        n_r, n_s = WORKLOADS[args.workload][:2]
-        tot, desc = n_r + n_s, WORKLOADS[args.workload][4]
+        n_r, n_s, _, layout, desc = workload_spec(args)
+        rates, sample, cores = cpu_reference_run(args.workload, args.steps, args.warmup, layout)
+        tot = n_r + n_s
     v = statistics.median(rates)
     emit({"impl": "reference", "metric": METRIC, "value": v, "unit": "tuples/s", "n_gpus": args.gpus,
           "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / v * 1e3,
@@ -150,6 +153,18 @@ def run_reference(args):
           "cpu_baseline": {"value": v, "unit": "tuples/s", "cores": cores, "kind": "port", "sample": sample},
           "e2e": {"value": v, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     return 0
+
+
+def workload_spec(args):
+    """The workload's sizes, skew, rank layout (-r, -R, -B) and description;
+    --groups G replaces the layout by G rank sets of one rank each (-r G -R G -B 1)."""
+    n_r, n_s, zipf, layout, desc = WORKLOADS[args.workload]
+    if args.groups > 0:
+        g = args.groups
+        layout = (g, g, 1)
+        desc = (desc.split(", groups of")[0].split(", replication groups of")[0] +
+                f", replication groups of {g} (-r {g} -R {g} -B 1)")
+    return n_r, n_s, zipf, layout, desc
 
 
 # ------------------------------------------------------------------ clocks --
@@ -240,7 +255,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    n_r, n_s, zipf, (ranks, rsets, bset), desc = WORKLOADS[args.workload]
+    n_r, n_s, zipf, (ranks, rsets, bset), desc = workload_spec(args)
     design = spj.make_design(rank_num=ranks, rank_set=rsets, bank_set=bset, join_alg=args.alg,
                              skew_mode=args.skew, input_size=n_r, rs_ratio=max(n_s // n_r, 1),
                              zipf_factor=int(round(zipf * 100)), radix_bits=args.bits,
@@ -357,7 +372,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        rates, sample, cores = cpu_reference_run(args.workload, 1, 0)
+        rates, sample, cores = cpu_reference_run(args.workload, 1, 0, workload_spec(args)[3])
         cpu = {"value": rates[0], "unit": "tuples/s", "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
@@ -410,7 +425,7 @@ def run_distributed(args):
                               WORLD_SIZE="1")
     dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                             device_id=torch.device("cuda", local))
-    n_r, n_s, zipf, (ranks, rsets, bset), desc = WORKLOADS[args.workload]
+    n_r, n_s, zipf, (ranks, rsets, bset), desc = workload_spec(args)
     design = spj.make_design(rank_num=ranks, rank_set=rsets, bank_set=bset, join_alg=args.alg,
                              skew_mode=args.skew, input_size=n_r, rs_ratio=max(n_s // n_r, 1),
                              zipf_factor=int(round(zipf * 100)), radix_bits=args.bits,
@@ -846,7 +861,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--alg", type=int, default=0)
-    ap.add_argument("--skew", type=int, default=0)
+    ap.add_argument("--skew", type=int, default=0, help="0 = adaptive replication, 1 = every partition")
+    ap.add_argument("--groups", type=int, default=0, help="replication groups G: -r G -R G -B 1 (0 = the workload's)")
     ap.add_argument("--bits", type=int, default=0, help="radix bits (0 = planner)")
     ap.add_argument("--slots", type=int, default=0, help="table slots per CTA (0 = planner)")
     ap.add_argument("--unit", type=int, default=0, help="max S tuples per work unit (0 = planner)")
