@@ -7,9 +7,14 @@ fraction of the HBM roofline, on the seeded synthetic relations.
 One step = one plain join (partition, build, probe, compaction) of the workload
 with R and S resident in HBM. Rank 0 prints one JSON line. Under torchrun with
 N > 1 the step is one join sharded over the N GPUs (each rank holds the
-workload's |R| and |S|: weak scaling): split by destination rank, NCCL
-all-to-all of R and S, local join; the time is the max over ranks
-(`--replicas`: N independent joins instead).
+workload's |R| and |S|: weak scaling): split by destination rank, exchange of R
+and S (`--exchange fused`, the default: a scatter straight into the peers'
+receive buffers; `nccl`: NCCL all-to-all), local join; the time is the max over
+ranks (`--replicas`: N independent joins instead).
+Workloads: c1, c2 (default), c3, their uniform/skewed twins, c4 (batched), c5
+(served stream); `--alg` picks the local join (0 hash, 1 non-partitioned hash,
+2 sort-merge, 3 nested loop), `--groups G` the replication groups (-r G -R G
+-B 1), `--skew 1` fixed instead of adaptive replication.
 `--impl reference` times the reference's algorithm restated on the host cores
 (the oracle's pipeline restatement; the UPMEM original cannot run here).
 """
