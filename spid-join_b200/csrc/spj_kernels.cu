@@ -862,6 +862,38 @@ __device__ __forceinline__ bool next_unit(const PlanDev &P, unsigned n_units, un
     return true;
 }
 
+// Units claimed one ahead (the join kernels that build per partition): while
+// a unit is probed, the CTA's last warp starts the next unit's R partition
+// towards L2, so that unit's build finds its tuples there. unit_claim_first
+// once, then unit_claim_next per unit; unit_prefetch_next_r after a barrier
+// that follows unit_claim_next (the next index is written by thread 0).
+__device__ __forceinline__ void unit_claim_first(const PlanDev &P, unsigned *s_next) {
+    if (threadIdx.x == 0) *s_next = atomicAdd(&P.bctr->unit_next, 1u);
+}
+
+__device__ __forceinline__ bool unit_claim_next(const PlanDev &P, unsigned n_units, unsigned *s_next, Unit &un) {
+    __syncthreads();
+    const unsigned u = *s_next;
+    __syncthreads();
+    if (u >= n_units) return false;
+    un = P.units[u];
+    if (threadIdx.x == 0) *s_next = atomicAdd(&P.bctr->unit_next, 1u);
+    return true;
+}
+
+__device__ __forceinline__ void unit_prefetch_next_r(const PlanDev &P, unsigned n_units, const unsigned *s_next,
+                                                     const Unit &un) {
+    if ((threadIdx.x >> 5) != (blockDim.x >> 5) - 1) return;
+    const unsigned nu = *s_next;
+    if (nu >= n_units) return;
+    const Unit un2 = P.units[nu];
+    if (un2.join == un.join && un2.p == un.p) return;  // the same table: nothing to fetch
+    const RelDev &R2 = P.rel[2 * un2.join];
+    const uint32_t nr2 = R2.total[un2.p];
+    const Tuple *pr2 = R2.out + R2.base[un2.p];
+    for (uint32_t i = (threadIdx.x & 31) * 16; i < nr2; i += 32 * 16) prefetch_l2(pr2 + i);
+}
+
 // Switches the CTA's output state to join j (closing the warp's chunk of the
 // previous join, which leaves that join at most one hole per warp).
 __device__ __forceinline__ void switch_join(const PlanDev &P, uint32_t j, uint32_t &cur_j, OutCtx &o, WarpOut &w) {
@@ -874,7 +906,7 @@ __device__ __forceinline__ void switch_join(const PlanDev &P, uint32_t j, uint32
 // ----------------------------------------------------- partitioned hash join --
 __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
     extern __shared__ unsigned long long table[];
-    __shared__ unsigned s_slot;
+    __shared__ unsigned s_next;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
@@ -882,13 +914,17 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu;
     Unit un;
-    while (next_unit(P, n_units, &s_slot, un)) {
+    unit_claim_first(P, &s_next);
+    while (unit_claim_next(P, n_units, &s_next, un)) {
         const JoinDev &J = P.join[un.join];
         if (un.join != cur_j || un.p != cur_p) {
             switch_join(P, un.join, cur_j, o, w);
             build_table(P, J, un.join, un.p, table);
             cur_p = un.p;
         }
+        else
+            __syncthreads();  // the next unit's index is written
+        unit_prefetch_next_r(P, n_units, &s_next, un);
         const uint32_t ts = J.table_slots;
         const Tuple *ps = P.rel[2 * un.join + 1].out;
         constexpr int U = 4;
@@ -956,7 +992,7 @@ __device__ __forceinline__ void warp0_scan1024(const uint32_t *cnt, uint32_t *of
 // unchanged.
 __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
     extern __shared__ unsigned long long smem_u64[];
-    __shared__ unsigned s_slot;
+    __shared__ unsigned s_next;
     __shared__ uint32_t bcnt[1024], boff[1025];
     Tuple *rs = reinterpret_cast<Tuple *>(smem_u64);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -966,7 +1002,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0, lmask = 0;
     Unit un;
-    while (next_unit(P, n_units, &s_slot, un)) {
+    unit_claim_first(P, &s_next);
+    while (unit_claim_next(P, n_units, &s_next, un)) {
         const JoinDev &J = P.join[un.join];
         const uint32_t bits = J.bits;
         if (un.join != cur_j || un.p != cur_p) {
@@ -995,7 +1032,10 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
                 rs[atomicAdd(&bcnt[b], 1u)] = t;
             }
             __syncthreads();
+        } else {
+            __syncthreads();  // the next unit's index is written
         }
+        unit_prefetch_next_r(P, n_units, &s_next, un);
         const Tuple *ps = P.rel[2 * un.join + 1].out;
         constexpr int U = 4;
         for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
@@ -1047,6 +1087,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0;
     Unit un;
+    // (no one-ahead claim: the sort, not the load, bounds this build)
     while (next_unit(P, n_units, &s_slot, un)) {
         const JoinDev &J = P.join[un.join];
         if (un.join != cur_j || un.p != cur_p) {
