@@ -12,7 +12,7 @@
 //   k_units      work units: (join, partition, S range); heavy partitions split
 //   k_join_*     persistent CTAs over the unit queue: build the R partition's
 //                shared-memory structure, probe the unit's S range, emit pairs with
-//                warp-aggregated reservations of 1024-pair output chunks
+//                warp-aggregated reservations of output chunks (32-1024 pairs)
 //   k_fixup_*    per join: move the pairs of partly used last chunks into the
 //                holes those chunks left, so the output is dense
 //

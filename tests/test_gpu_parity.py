@@ -251,3 +251,24 @@ def test_host_columns_joined_in_overlapped_slices(spj, oracle, alg):
     out = inst.FinishJoin().pairs()
     inst.close()
     assert out.shape == (n_s, 2) and oracle.checksum(out) == expect2
+
+
+def test_start_after_loading_columns_of_other_sizes(spj, oracle):
+    # StartJoin after LoadColumn without PrepareJoin: the instance prepares for
+    # the new sizes itself. A sliced S whose size is not a multiple of the slice
+    # (key-0 padding in the last slice), then an unsliced one, then the first
+    # sizes again: every join exact.
+    inst = spj.JoinInstance(1, 1, 1)
+    d = spj.make_design(rank_num=1)
+    for i, (n_r, n_s, z) in enumerate([(1 << 16, (1 << 24) + 5, 1.0), (1 << 15, 3 << 20, 0.0),
+                                       (1 << 16, (1 << 24) + 5, 1.2)]):
+        R, S, expect = spj.generate_host(n_r, n_s, z, seed=90 + i)
+        inst.LoadColumn(R, n_r, "left")
+        inst.LoadColumn(S, n_s, "right")
+        if i == 0:
+            inst.PrepareJoin(d)
+        inst.StartJoin(d)
+        out = inst.FinishJoin().pairs()
+        assert out.shape == (n_s, 2) and oracle.checksum(out) == expect
+    inst.close()
+
