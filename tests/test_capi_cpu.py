@@ -52,6 +52,17 @@ def test_bad_arguments(spj):
         spj.JoinInstance(4, 3, 1)  # ranks must equal groups x per group
 
 
+def test_relation_sizes_beyond_32_bit_positions_are_rejected(spj):
+    # output and partition positions are 32-bit: a relation may hold at most
+    # 2^32 - 2^24 - 2 tuples; larger ones are refused before any device work
+    too_big = (1 << 32) - (1 << 24) - 1
+    for n_r, n_s in [(1, too_big), (too_big, 1), (1, 1 << 33)]:
+        with pytest.raises(spj.SpjError, match="ARG.*2\\^32"):
+            spj.Plan(n_r, n_s)
+    with pytest.raises(spj.SpjError, match="ARG.*2\\^32"):
+        spj.Batch([1, too_big], [1, 1])
+
+
 def test_generator_relations(spj, oracle):
     R, S, expect = spj.generate_host(10000, 40000, 0.0, seed=123)
     assert sorted(R[:, 0].tolist()) == list(range(1, 10001))     # permutation of 1..n
