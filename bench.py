@@ -45,7 +45,6 @@ WORKLOADS = {
 }
 SEED = 0x5EED5EED
 METRIC = "join tuples/s (|R|+|S|)"
-CPU_SAMPLE_DIV = 32   # the CPU legs run |R|/32, |S|/32 of the same workload
 
 
 def launches_per_join(alg, radix_bits, single=True):
@@ -77,31 +76,40 @@ def emit(obj):
 
 
 # ------------------------------------------------------------ CPU baseline --
-def cpu_reference_run(wl, steps, warmup, layout=None):
-    """The reference's pipeline restated in C on all host cores, on a sample of
-    the workload (with rank layout `layout`, default the workload's): returns
-    (tuples/s per step list, description, cores)."""
+def _oracle():
+    """The oracle (test infrastructure): the CPU arms' only library. They load
+    no product library, so nothing of this repository's GPU path runs there."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    import spidjoin
-    n_r, n_s, zipf, (ranks, rsets, bset), _ = WORKLOADS[wl]
-    if layout:
-        ranks, rsets, bset = layout
-    sr, ss = max(n_r // CPU_SAMPLE_DIV, 1), max(n_s // CPU_SAMPLE_DIV, 1)
-    R, S, expect = spidjoin.generate_host(sr, ss, zipf, seed=SEED)
+    return oracle
+
+
+def cpu_reference_run(n_r, n_s, zipf, layout, steps, warmup, data=None):
+    """The reference's pipeline restated in C (the oracle's port of its global
+    partition, rank-set / bank-set replication and local hash join) on all host
+    cores, over the whole workload: `warmup` untimed and `steps` timed joins.
+    `data` = (R, S, expected checksum) as host arrays, else the oracle's own copy
+    of the seeded generator makes them. Returns (seconds per timed step, sample
+    description, threads)."""
+    oracle = _oracle()
+    ranks, rsets, bset = layout
+    if data is None:
+        data = oracle.generate(n_r, n_s, zipf, seed=SEED)
+    R, S, expect = data
     cores = os.cpu_count() or 1
-    rates = []
+    secs = []
     for i in range(warmup + steps):
         t0 = time.perf_counter()
         out = oracle.refpipe_join(R, S, ranks=ranks, rank_sets=rsets, bank_set=bset, alg=0, nthreads=cores)
         dt = time.perf_counter() - t0
-        if i == 0:
-            assert out.shape[0] == ss and oracle.checksum(out) == expect, "CPU restatement disagrees"
+        if i == 0 and (out.shape[0] != n_s or oracle.checksum(out) != expect & (2**64 - 1)):
+            raise SystemExit("CPU restatement disagrees with the generator's expected join")
+        del out
         if i >= warmup:
-            rates.append((sr + ss) / dt)
-    sample = (f"|R|=2^{sr.bit_length() - 1} |S|=2^{ss.bit_length() - 1} (1/{CPU_SAMPLE_DIV} of the workload, "
-              f"same Zipf and layout), reference pipeline restated in C, {cores} threads")
-    return rates, sample, cores
+            secs.append(dt)
+    sample = (f"the whole workload (|R|={n_r}, |S|={n_s}, Zipf {zipf:g}, -r {ranks} -R {rsets} -B {bset}), "
+              f"reference pipeline restated in C (oracle), {cores} threads, {steps} timed joins")
+    return secs, sample, cores
 
 
 def cpu_reference_specs(specs, steps, warmup, budget_tuples=24 << 20):
@@ -109,16 +117,14 @@ def cpu_reference_specs(specs, steps, warmup, budget_tuples=24 << 20):
     joins: each step joins the first joins of `specs` whose sizes add up to
     about `budget_tuples` (every join in full), and the rate is their tuples
     over the summed time."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    import spidjoin
+    oracle = _oracle()
     take, tot = [], 0
     for n_r, n_s, z in specs:
         if tot + n_r + n_s > budget_tuples and take:
             continue
         take.append((n_r, n_s, z))
         tot += n_r + n_s
-    data = [spidjoin.generate_host(n_r, n_s, z, seed=SEED + 77 + i) for i, (n_r, n_s, z) in enumerate(take)]
+    data = [oracle.generate(n_r, n_s, z, seed=SEED + 77 + i) for i, (n_r, n_s, z) in enumerate(take)]
     cores = os.cpu_count() or 1
     rates = []
     for it in range(warmup + steps):
@@ -137,6 +143,8 @@ def cpu_reference_specs(specs, steps, warmup, budget_tuples=24 << 20):
 
 
 def run_reference(args):
+    """The reference arm: the reference's join algorithm restated in C, on the
+    host cores, on the same workload; rank 0 alone under torchrun."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
@@ -146,13 +154,15 @@ def run_reference(args):
         desc = ("batched joins, |R| log-uniform [2^12, 2^24], R:S in {1,2,4,8}, Zipf s ~ U[0, 1.5]"
                 if args.workload == "c4" else
                 "served join stream, |R| log-uniform [2^10, 2^22], R:S in {1,2,4,8}, Zipf s ~ U[0, 1.5]")
+        v = statistics.median(rates)
+        ms_step = tot / v * 1e3
     else:
-        n_r, n_s, _, layout, desc = workload_spec(args)
-        rates, sample, cores = cpu_reference_run(args.workload, args.steps, args.warmup, layout)
-        tot = n_r + n_s
-    v = statistics.median(rates)
+        n_r, n_s, zipf, layout, desc = workload_spec(args)
+        secs, sample, cores = cpu_reference_run(n_r, n_s, zipf, layout, args.steps, args.warmup)
+        ms_step = statistics.mean(secs) * 1e3
+        v = (n_r + n_s) / (ms_step / 1e3)
     emit({"impl": "reference", "metric": METRIC, "value": v, "unit": "tuples/s", "n_gpus": args.gpus,
-          "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / v * 1e3,
+          "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
           "config": {"workload": desc, "sample": sample},
           "cpu_baseline": {"value": v, "unit": "tuples/s", "cores": cores, "kind": "port", "sample": sample},
@@ -248,6 +258,74 @@ def traffic_from_profiles(kernel, units):
         return None
 
 
+def device_join_leg(spj, n_r, n_s, zipf, layout, args, steps, warmup, seed, sample_clocks, keep_inputs=False):
+    """One plain join of the given shape with R and S resident in HBM (seeded,
+    generated on the device): `warmup` untimed steps and a result check (count
+    and checksum against the generator's exact answer), then `steps` steps
+    bracketed by CUDA events on the launching stream, with the SM clocks sampled
+    inside the timed region. Returns a dict; with keep_inputs it holds the
+    device columns for the end-to-end leg."""
+    import torch
+    ranks, rsets, bset = layout
+    design = spj.make_design(rank_num=ranks, rank_set=rsets, bank_set=bset, join_alg=args.alg,
+                             skew_mode=args.skew, input_size=n_r, rs_ratio=max(n_s // n_r, 1),
+                             zipf_factor=int(round(zipf * 100)), radix_bits=args.bits,
+                             table_slots=args.slots, unit_tuples=args.unit)
+    ws, rank, local = dist_env()
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    lib = spj.lib()
+    dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
+    dS = torch.empty((n_s, 2), dtype=torch.int32, device="cuda")
+    expect = torch.zeros(1, dtype=torch.int64, device="cuda")
+    spj.check(lib.spj_generate_device(seed, n_r, n_s, zipf, dR.data_ptr(), dS.data_ptr(), expect.data_ptr(), sp))
+    plan = spj.Plan(n_r, n_s, design)
+    out = torch.empty((plan.output_capacity, 2), dtype=torch.int32, device="cuda")
+    n_out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    csum = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    def step():
+        plan.execute(dR.data_ptr(), dS.data_ptr(), out.data_ptr(), n_out.data_ptr(), sp)
+
+    for _ in range(warmup):
+        step()
+    spj.check(lib.spj_checksum_device(out.data_ptr(), n_out.data_ptr(), csum.data_ptr(), sp))
+    torch.cuda.synchronize()
+    st = plan.stats()
+    ok = int(n_out.item()) == n_s and int(csum.item()) == int(expect.item())
+    if not ok:
+        raise SystemExit(f"join result check failed: {int(n_out.item())} pairs, checksum mismatch")
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid) if sample_clocks else None
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.mark()
+    ev0.record(stream)
+    for _ in range(steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    ms = ev0.elapsed_time(ev1)
+    kts = [plan.kernel_times(b) for b in range(min(steps, 128))]
+    kmean = {k: statistics.mean(x[k] for x in kts) for k in kts[0]}
+    res = {"ms": ms, "ms_step": ms / steps, "kmean": kmean, "stats": st, "n_pairs": int(n_out.item()),
+           "ok": ok, "clocks": clocks, "design": design, "expect": int(expect.item())}
+    del out
+    plan.close()
+    if keep_inputs:
+        res["dR"], res["dS"] = dR, dS
+    else:
+        del dR, dS
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_ours(args):
     import torch
     import spidjoin as spj
@@ -261,69 +339,19 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     n_r, n_s, zipf, (ranks, rsets, bset), desc = workload_spec(args)
-    design = spj.make_design(rank_num=ranks, rank_set=rsets, bank_set=bset, join_alg=args.alg,
-                             skew_mode=args.skew, input_size=n_r, rs_ratio=max(n_s // n_r, 1),
-                             zipf_factor=int(round(zipf * 100)), radix_bits=args.bits,
-                             table_slots=args.slots, unit_tuples=args.unit)
-    stream = torch.cuda.current_stream()
-    sp = stream.cuda_stream
-    lib = spj.lib()
-
-    # inputs resident in HBM (seeded, generated on the device)
-    dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
-    dS = torch.empty((n_s, 2), dtype=torch.int32, device="cuda")
-    expect = torch.zeros(1, dtype=torch.int64, device="cuda")
-    spj.check(lib.spj_generate_device(SEED + rank, n_r, n_s, zipf, dR.data_ptr(), dS.data_ptr(),
-                                      expect.data_ptr(), sp))
-    plan = spj.Plan(n_r, n_s, design)
-    out = torch.empty((plan.output_capacity, 2), dtype=torch.int32, device="cuda")
-    n_out = torch.zeros(1, dtype=torch.int64, device="cuda")
-    csum = torch.zeros(1, dtype=torch.int64, device="cuda")
-
-    def step():
-        plan.execute(dR.data_ptr(), dS.data_ptr(), out.data_ptr(), n_out.data_ptr(), sp)
-
-    for _ in range(args.warmup):
-        step()
-    spj.check(lib.spj_checksum_device(out.data_ptr(), n_out.data_ptr(), csum.data_ptr(), sp))
-    torch.cuda.synchronize()
-    st = plan.stats()
-    ok = int(n_out.item()) == n_s and int(csum.item()) == int(expect.item())
-    if not ok:
-        raise SystemExit(f"join result check failed: {int(n_out.item())} pairs, checksum mismatch")
-
-    uuid = None
-    try:
-        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
-    except Exception:
-        pass
-    sampler = ClockSampler(uuid) if rank == 0 else None
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
+    if dist:  # every rank warmed up and checked before the common timed region
         dist.barrier()
-    torch.cuda.synchronize()
-    if sampler:
-        sampler.mark()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    clocks = sampler.stop() if sampler else None
-    ms = ev0.elapsed_time(ev1)
+    leg = device_join_leg(spj, n_r, n_s, zipf, (ranks, rsets, bset), args, args.steps, args.warmup, SEED + rank,
+                          rank == 0, keep_inputs=True)
+    ms = leg["ms"]
     if dist:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     ms_step = ms / args.steps
     value = ws * (n_r + n_s) / (ms_step / 1e3)
-
-    # per-kernel device times over the timed steps (CUDA events between launches)
-    kts = [plan.kernel_times(b) for b in range(min(args.steps, 128))]
-    kmean = {k: statistics.mean(x[k] for x in kts) for k in kts[0]}
-    n_pairs = int(n_out.item())
+    kmean, st, n_pairs, design = leg["kmean"], leg["stats"], leg["n_pairs"], leg["design"]
+    dR, dS = leg.pop("dR"), leg.pop("dS")
     alg_bytes = {  # algorithmic bytes per launch
         "k_hist": 8 * (n_r + n_s),
         "k_scatter": 16 * (n_r + n_s),
@@ -336,19 +364,18 @@ def run_ours(args):
     traffic = traffic_from_profiles(dom, n_r + n_s)
     pipe_bytes = 24 * (n_r + n_s) + 8 * n_pairs
     pipe_gbs = pipe_bytes / (ms_step / 1e3) / 1e9
-    del out
-    plan.close()
-    torch.cuda.empty_cache()
 
     # end to end through the JoinInstance API with pinned host columns
     e2e = None
-    if not args.no_e2e:
+    hR = hS = None
+    if not args.no_e2e or (rank == 0 and ws == 1 and not args.no_cpu):
         hR = torch.empty((n_r, 2), dtype=torch.int32, pin_memory=True)
         hS = torch.empty((n_s, 2), dtype=torch.int32, pin_memory=True)
         hR.copy_(dR)
         hS.copy_(dS)
-        del dR, dS
-        torch.cuda.empty_cache()
+    del dR, dS
+    torch.cuda.empty_cache()
+    if not args.no_e2e:
         inst = spj.JoinInstance(ranks, rsets, ranks // rsets)
         inst.LoadColumn((hR.data_ptr(), n_r), n_r, "left")
         inst.LoadColumn((hS.data_ptr(), n_s), n_s, "right")
@@ -375,13 +402,37 @@ def run_ours(args):
                "h2d_bytes_per_step": 8 * (n_r + n_s), "d2h_bytes_per_step": 8 * got + 8,
                "ms_per_step": el / ke * 1e3}
 
+    # the CPU baseline: the reference pipeline restated in C on the same bytes
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        rates, sample, cores = cpu_reference_run(args.workload, 1, 0, workload_spec(args)[3])
-        cpu = {"value": rates[0], "unit": "tuples/s", "cores": cores, "kind": "port", "sample": sample}
+        import numpy as np
+        R = hR.numpy().view(np.uint32)
+        S = hS.numpy().view(np.uint32)
+        secs, sample, cores = cpu_reference_run(n_r, n_s, zipf, (ranks, rsets, bset), 1, 1,
+                                                data=(R, S, leg["expect"]))
+        cpu = {"value": (n_r + n_s) / statistics.mean(secs), "unit": "tuples/s", "cores": cores, "kind": "port",
+               "sample": sample, "ms_per_step": statistics.mean(secs) * 1e3}
+        del R, S
+    del hR, hS
+
+    # the north-star comparisons on the same GPU: the C2 shape at Zipf 1.5
+    # against uniform, and the batched form of config 4 against one plain join
+    # per join (every join checked)
+    extra = {}
+    if rank == 0 and ws == 1 and args.workload == "c2" and not args.no_extra:
+        k = max(3, min(args.steps, 10))
+        uni = device_join_leg(spj, n_r, n_s, 0.0, (ranks, rsets, bset), args, k, 3, SEED + 11, True)
+        z15 = device_join_leg(spj, n_r, n_s, 1.5, (ranks, rsets, bset), args, k, 3, SEED + 12, True)
+        extra["skew"] = {
+            "workload": f"|R|=2^27 |S|=2^29, -r {ranks} -R {rsets} -B {bset}: uniform vs Zipf 1.5",
+            "uniform_ms": uni["ms_step"], "zipf_1_5_ms": z15["ms_step"], "zipf_1_0_ms": ms_step,
+            "zipf_1_5_vs_uniform": z15["ms_step"] / uni["ms_step"], "target": "<= 1.5",
+            "steps": k, "checked": uni["ok"] and z15["ok"],
+            "clocks": {"uniform": uni["clocks"], "zipf_1_5": z15["clocks"]}}
+        extra["batched"] = batched_compare(spj, args, steps=max(3, min(args.steps, 5)), warmup=3)
 
     if rank == 0:
-        emit({
+        line = {
             "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
@@ -399,10 +450,12 @@ def run_ours(args):
             "kernels_ms": kmean,
             "e2e": e2e, "cpu_baseline": cpu,
             "gpu_launches": launches_per_join(args.alg, st["radix_bits"]) * args.steps,
-            "clocks": clocks,
-            "check": {"n_pairs": n_pairs, "checksum_ok": ok, "max_s_partition": st["max_s_partition"],
+            "clocks": leg["clocks"],
+            "check": {"n_pairs": n_pairs, "checksum_ok": leg["ok"], "max_s_partition": st["max_s_partition"],
                       "units": st["units"]},
-        })
+        }
+        line.update(extra)
+        emit(line)
     if dist:
         dist.destroy_process_group()
     return 0
@@ -565,12 +618,12 @@ def c4_specs(n_joins=256, seed=SEED + 4, scale=1.0):
     return specs
 
 
-def run_batched(args):
+def batched_compare(spj, args, steps, warmup):
+    """Config 4: the 256 joins as one batch plan replayed from a CUDA graph,
+    against one pre-created plain plan per join (the device times of its
+    executions summed); every join of both forms checked against the
+    generator's exact count and checksum. Returns a dict."""
     import torch
-    import spidjoin as spj
-
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
     specs = c4_specs(scale=args.c4_scale)
     J = len(specs)
     tot = sum(a + b for a, b, _ in specs)
@@ -591,7 +644,17 @@ def run_batched(args):
         S.append(dS)
         exp.append(e)
     torch.cuda.synchronize()
-    exp = [int(e.item()) for e in exp]
+    exp_t = torch.cat(exp)
+    n_s_t = torch.tensor([b for _, b, _ in specs], dtype=torch.int64, device="cuda")
+
+    def wrong(outs, n_out):
+        """Joins whose count or checksum differs from the generator's answer."""
+        cs = torch.zeros(J, dtype=torch.int64, device="cuda")
+        for j in range(J):
+            spj.check(lib.spj_checksum_device(outs[j].data_ptr(), n_out[j:j + 1].data_ptr(), cs[j:j + 1].data_ptr(),
+                                              None))
+        torch.cuda.synchronize()
+        return int(((cs != exp_t) | (n_out != n_s_t)).sum().item())
 
     batch = spj.Batch([a for a, _, _ in specs], [b for _, b, _ in specs], design)
     outs = [torch.empty((batch.output_capacity(j), 2), dtype=torch.int32, device="cuda") for j in range(J)]
@@ -606,16 +669,10 @@ def run_batched(args):
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph):
         batch.execute(torch.cuda.current_stream().cuda_stream)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         graph.replay()
-    # every join checked against the generator's exact checksum
-    cs = torch.zeros(1, dtype=torch.int64, device="cuda")
-    bad = 0
-    for j in range(J):
-        spj.check(lib.spj_checksum_device(outs[j].data_ptr(), n_out[j:j + 1].data_ptr(), cs.data_ptr(), None))
-        torch.cuda.synchronize()
-        if int(n_out[j].item()) != specs[j][1] or int(cs.item()) != exp[j]:
-            bad += 1
+    torch.cuda.synchronize()
+    bad = wrong(outs, n_out)
     if bad:
         raise SystemExit(f"batched join check failed for {bad} joins")
     sampler = ClockSampler()
@@ -623,12 +680,12 @@ def run_batched(args):
     torch.cuda.synchronize()
     sampler.mark()
     ev0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         graph.replay()
     ev1.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    ms_batched = ev0.elapsed_time(ev1) / args.steps
+    ms_batched = ev0.elapsed_time(ev1) / steps
     del graph
     batch.execute(0)  # one eager run for the per-kernel split
     kmean = batch.kernel_times(0)
@@ -636,11 +693,14 @@ def run_batched(args):
 
     # plain: one plan per join, its device time per execution, summed over joins
     plain_ms = 0.0
+    n_out.zero_()
+    plain_outs = []
     for j, (n_r, n_s, z) in enumerate(specs):
         plan = spj.Plan(n_r, n_s, design)
         o = outs[j] if outs[j].shape[0] >= plan.output_capacity else \
             torch.empty((plan.output_capacity, 2), dtype=torch.int32, device="cuda")
-        n1 = torch.zeros(1, dtype=torch.int64, device="cuda")
+        plain_outs.append(o)
+        n1 = n_out[j:j + 1]
         plan.execute(R[j].data_ptr(), S[j].data_ptr(), o.data_ptr(), n1.data_ptr(), 0)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         reps = 3
@@ -649,29 +709,46 @@ def run_batched(args):
             plan.execute(R[j].data_ptr(), S[j].data_ptr(), o.data_ptr(), n1.data_ptr(), 0)
         b.record()
         torch.cuda.synchronize()
-        if int(n1.item()) != n_s:
-            raise SystemExit(f"plain join {j} returned {int(n1.item())} pairs")
         plain_ms += a.elapsed_time(b) / reps
         plan.close()
+    bad = wrong(plain_outs, n_out)
+    if bad:
+        raise SystemExit(f"plain join check failed for {bad} joins")
     pipe_bytes = sum(24 * (a + b) + 8 * b for a, b, _ in specs)
     peak, peak_kind = peaks()
-    value = tot / (ms_batched / 1e3)
+    del outs, plain_outs, R, S
+    torch.cuda.empty_cache()
+    return {"workload": f"batched: {J} joins, |R| log-uniform [2^12, 2^24], R:S in {{1,2,4,8}}, "
+                        f"Zipf s ~ U[0, 1.5], one seed; one CUDA graph per step",
+            "joins": J, "tuples": tot, "scale": args.c4_scale, "tuning": tuning,
+            "value": tot / (ms_batched / 1e3), "ms_per_step": ms_batched, "steps": steps,
+            "plain": {"value": tot / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                      "how": "one pre-created plan per join, CUDA-event device time per execution, summed"},
+            "batched_vs_plain": plain_ms / ms_batched, "target": ">= 3",
+            "pipeline_roofline": {"achieved": pipe_bytes / (ms_batched / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                  "frac": pipe_bytes / (ms_batched / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
+            "clocks": clocks, "kernels_ms_eager": kmean,
+            "check": {"joins_checked": 2 * J, "all_exact": True,
+                      "how": "count and 64-bit checksum of every join, batched and plain"}}
+
+
+def run_batched(args):
+    import torch
+    import spidjoin as spj
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    r = batched_compare(spj, args, args.steps, args.warmup)
     emit({
-        "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": r["value"], "unit": "tuples/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"batched: {J} joins, |R| log-uniform [2^12, 2^24], R:S in {{1,2,4,8}}, "
-                               f"Zipf s ~ U[0, 1.5], one seed; one CUDA graph per step",
-                   "joins": J, "tuples": tot, "join_alg": args.alg, "scale": args.c4_scale, "tuning": tuning,
-                   "l2": "inputs larger than L2; no flush"},
-        "plain": {"value": tot / (plain_ms / 1e3), "ms_per_step": plain_ms,
-                  "how": "one pre-created plan per join, CUDA-event device time per execution, summed"},
-        "batched_vs_plain": plain_ms / ms_batched,
-        "pipeline_roofline": {"achieved": pipe_bytes / (ms_batched / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                              "frac": pipe_bytes / (ms_batched / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
-        "gpu_launches": launches_per_join(args.alg, 15, single=False) * args.steps, "clocks": clocks,
-        "kernels_ms_eager": kmean,
-        "check": {"joins_checked": J, "all_exact": True},
+        "config": {"workload": r["workload"], "joins": r["joins"], "tuples": r["tuples"], "join_alg": args.alg,
+                   "scale": args.c4_scale, "tuning": r["tuning"], "l2": "inputs larger than L2; no flush"},
+        "plain": r["plain"], "batched_vs_plain": r["batched_vs_plain"],
+        "pipeline_roofline": r["pipeline_roofline"],
+        "gpu_launches": launches_per_join(args.alg, 15, single=False) * args.steps, "clocks": r["clocks"],
+        "kernels_ms_eager": r["kernels_ms_eager"], "check": r["check"],
     })
     return 0
 
@@ -886,6 +963,7 @@ def main():
     ap.add_argument("--exchange", default="fused", choices=["fused", "nccl"], help="sharded join's exchange")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="c2: skip the skew and batched comparisons")
     ap.add_argument("--nr", type=int, default=0, help="custom workload: |R| (with --ns, --zipf)")
     ap.add_argument("--ns", type=int, default=0)
     ap.add_argument("--zipf", type=float, default=0.0)

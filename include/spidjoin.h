@@ -267,10 +267,11 @@ int spj_server_reset_stats(spj_server_t *server);
 void spj_server_destroy(spj_server_t *server);
 
 /* The join for callers that cannot allocate device memory while they run it: a
- * runtime whose memory pool owns the whole GPU, code running under CUDA stream
- * capture (where cudaMalloc is not allowed), or a latency-bound loop that must
- * not wait on the allocator. No counterpart in the reference, whose host buffers
- * are allocated per join. It computes what spj_plan_execute computes (the
+ * database engine or other host runtime whose own pool allocator owns the whole
+ * GPU (a cudaMalloc from inside a query would fail or take memory from that
+ * pool), or a latency-bound loop that must not stall on the allocator
+ * (cudaMalloc and cudaFree can synchronise the device). No counterpart in the
+ * reference, whose host buffers are allocated per join. It computes what spj_plan_execute computes (the
  * partitioned hash join, SPJ_ALG_PHJ) but takes all scratch memory from one
  * fixed 32 MiB region inside the library, allocated once when the library loads
  * on a GPU and held until the process exits; the call allocates nothing.

@@ -26,9 +26,7 @@ _lib = None
 
 def build():
     """Compile liboracle.so (and the reference hash library when the reference tree exists)."""
-    subprocess.check_call(["make", "-s", "-C", HERE, "all"])
-    if os.path.isdir("/root/reference/src/dpu/src"):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+    subprocess.check_call(["make", "-s", "-C", HERE, "all", "ref-if-present"])
 
 
 def lib():
@@ -53,6 +51,13 @@ def lib():
         L.orc_simple_join.argtypes = [vp, i64, vp, i64, i32, vp]
         L.orc_refpipe_join.restype = i64
         L.orc_refpipe_join.argtypes = [vp, i64, vp, i64, i32, i32, i32, i32, i32, vp]
+        L.orc_simple_join_mt.restype = i64
+        L.orc_simple_join_mt.argtypes = [vp, i64, vp, i64, i32, i32, vp]
+        L.orc_sort_pairs_mt.restype = i32
+        L.orc_sort_pairs_mt.argtypes = [vp, i64, i32]
+        L.orc_generate.restype = i32
+        L.orc_generate.argtypes = [ctypes.c_uint64, i64, i64, ctypes.c_double, vp, vp,
+                                   ctypes.POINTER(ctypes.c_uint64), i32]
         L.orc_refpipe_dpu_sizes.restype = i32
         L.orc_refpipe_dpu_sizes.argtypes = [vp, i64, vp, i64, i32, i32, i32, i32, vp, vp]
         _lib = L
@@ -111,6 +116,29 @@ def sort_pairs(pairs):
     return p
 
 
+def sort_pairs_mt(pairs, nthreads=None, inplace=False):
+    """sort_pairs with threads (the same canonical order); in place when asked."""
+    p = _tuples(pairs) if inplace else _tuples(pairs).copy()
+    rc = lib().orc_sort_pairs_mt(_ptr(p), p.shape[0], nthreads or os.cpu_count() or 1)
+    if rc:
+        raise RuntimeError(ERRORS.get(rc, rc))
+    return p
+
+
+def generate(n_r, n_s, zipf=0.0, seed=1, nthreads=None):
+    """The benchmark relations (R, S) and the checksum of their join, restated
+    here so that checkers and CPU arms need no product library. Same values as
+    the product's generator."""
+    R = np.empty((n_r, 2), dtype=np.uint32)
+    S = np.empty((n_s, 2), dtype=np.uint32)
+    exp = ctypes.c_uint64(0)
+    rc = lib().orc_generate(seed & (2**64 - 1), n_r, n_s, float(zipf), _ptr(R), _ptr(S), ctypes.byref(exp),
+                            nthreads or os.cpu_count() or 1)
+    if rc:
+        raise RuntimeError(ERRORS.get(rc, rc))
+    return R, S, int(exp.value)
+
+
 def partition_count(tuples, P, type_=0, rank_sets=1, ranks_per_set=1):
     t = _tuples(tuples)
     hist = np.zeros(P, dtype=np.uint32)
@@ -127,11 +155,22 @@ def simple_join(R, S, keep_unmatched=False):
     return out[:m]
 
 
+def simple_join_mt(R, S, keep_unmatched=False, nthreads=None):
+    """simple_join with threads: byte-identical output (same pairs, same order)."""
+    R, S = _tuples(R), _tuples(S)
+    out = np.empty((max(S.shape[0], 1), 2), dtype=np.uint32)
+    m = lib().orc_simple_join_mt(_ptr(R), R.shape[0], _ptr(S), S.shape[0], int(keep_unmatched),
+                                 nthreads or os.cpu_count() or 1, _ptr(out))
+    if m < 0:
+        raise RuntimeError(ERRORS.get(m, m))
+    return out[:m]
+
+
 def refpipe_join(R, S, ranks=1, rank_sets=1, bank_set=1, alg=ALG_PHJ, nthreads=None):
     """The reference pipeline restated: split, partition, replicate, local join."""
     R, S = _tuples(R), _tuples(S)
     nthreads = nthreads or os.cpu_count() or 1
-    out = np.zeros((max(S.shape[0], 1), 2), dtype=np.uint32)
+    out = np.empty((max(S.shape[0], 1), 2), dtype=np.uint32)
     m = lib().orc_refpipe_join(_ptr(R), R.shape[0], _ptr(S), S.shape[0], ranks, rank_sets, bank_set, alg,
                                nthreads, _ptr(out))
     if m < 0:

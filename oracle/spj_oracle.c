@@ -38,6 +38,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <pthread.h>
+#include <math.h>
 
 typedef struct { uint32_t key, pay; } orc_tuple;
 
@@ -599,4 +600,331 @@ int64_t orc_refpipe_join(const orc_tuple *R, int64_t nR, const orc_tuple *S, int
     }
     free_refpipe(&rp);
     return m;
+}
+
+/* ------------------------------------------- threaded checker utilities -- */
+
+/* orc_simple_join with threads, for full-size checks (2^27 R x 2^29 S): the
+ * table maps a key to the smallest R index holding it (a CAS keeps the minimum),
+ * which is exactly the single-threaded rule "first R tuple in R order wins";
+ * S is probed in contiguous slices whose outputs are concatenated in S order.
+ * The result is byte-identical to orc_simple_join. */
+typedef struct {
+    const orc_tuple *R, *S;
+    int64_t nR, nS;
+    uint64_t *tab;   /* (key << 32 | R index + 1), 0 = empty */
+    uint64_t mask;
+    int keep;
+    int64_t slices, per;
+    int64_t *cnt;    /* matches per S slice, then the slice's output offset */
+    orc_tuple *out;
+    int pass;        /* 0 build, 1 count, 2 write */
+} sj_mt_t;
+
+static void sj_build_task(void *ctx, int64_t t)
+{
+    sj_mt_t *c = (sj_mt_t *)ctx;
+    int64_t b = c->per * t, e = b + c->per < c->nR ? b + c->per : c->nR;
+    for (int64_t i = b; i < e; i++) {
+        uint32_t k = c->R[i].key;
+        if (k == 0) continue;
+        uint64_t ent = ((uint64_t)k << 32) | (uint64_t)(i + 1);
+        uint64_t s = mix64(k) & c->mask;
+        for (;;) {
+            uint64_t cur = __atomic_load_n(&c->tab[s], __ATOMIC_RELAXED);
+            if (cur == 0) {
+                if (__atomic_compare_exchange_n(&c->tab[s], &cur, ent, 0, __ATOMIC_RELAXED, __ATOMIC_RELAXED))
+                    break;
+                continue;  /* cur now holds the winner: look at it again */
+            }
+            if ((uint32_t)(cur >> 32) == k) {
+                if ((uint32_t)cur <= (uint32_t)(i + 1)) break;
+                if (__atomic_compare_exchange_n(&c->tab[s], &cur, ent, 0, __ATOMIC_RELAXED, __ATOMIC_RELAXED))
+                    break;
+                continue;
+            }
+            s = (s + 1) & c->mask;
+        }
+    }
+}
+
+static void sj_probe_task(void *ctx, int64_t t)
+{
+    sj_mt_t *c = (sj_mt_t *)ctx;
+    int64_t b = c->per * t, e = b + c->per < c->nS ? b + c->per : c->nS;
+    int64_t m = c->pass == 2 ? c->cnt[t] : 0;
+    for (int64_t i = b; i < e; i++) {
+        uint32_t k = c->S[i].key;
+        if (k == 0) continue;
+        uint64_t s = mix64(k) & c->mask, ent;
+        while ((ent = c->tab[s]) != 0 && (uint32_t)(ent >> 32) != k) s = (s + 1) & c->mask;
+        if (ent) {
+            if (c->pass == 2) {
+                c->out[m].key = c->R[(uint32_t)ent - 1].pay;
+                c->out[m].pay = c->S[i].pay;
+            }
+            m++;
+        } else if (c->keep) {
+            if (c->pass == 2) c->out[m] = c->S[i];
+            m++;
+        }
+    }
+    if (c->pass == 1) c->cnt[t] = m;
+}
+
+int64_t orc_simple_join_mt(const orc_tuple *R, int64_t nR, const orc_tuple *S, int64_t nS, int keep_unmatched,
+                           int nthreads, orc_tuple *out)
+{
+    if (nR < 0 || nS < 0 || nR >= 0xFFFFFFFFll) return ORC_E_ARG;
+    if (nthreads < 1) nthreads = 1;
+    sj_mt_t c;
+    memset(&c, 0, sizeof(c));
+    c.R = R; c.S = S; c.nR = nR; c.nS = nS; c.keep = keep_unmatched; c.out = out;
+    int64_t cap = 16;
+    while (cap < 2 * nR + 16) cap <<= 1;
+    c.mask = (uint64_t)cap - 1;
+    c.tab = (uint64_t *)calloc((size_t)cap, sizeof(uint64_t));
+    int64_t slices = 4 * (int64_t)nthreads;
+    c.cnt = (int64_t *)calloc((size_t)slices, sizeof(int64_t));
+    if (!c.tab || !c.cnt) { free(c.tab); free(c.cnt); return ORC_E_NOMEM; }
+    c.per = (nR + slices - 1) / slices;
+    if (c.per < 1) c.per = 1;
+    parallel_for(nthreads, slices, sj_build_task, &c);
+    c.per = (nS + slices - 1) / slices;
+    if (c.per < 1) c.per = 1;
+    c.pass = 1;
+    parallel_for(nthreads, slices, sj_probe_task, &c);
+    int64_t run = 0;
+    for (int64_t t = 0; t < slices; t++) { int64_t v = c.cnt[t]; c.cnt[t] = run; run += v; }
+    c.pass = 2;
+    parallel_for(nthreads, slices, sj_probe_task, &c);
+    free(c.tab);
+    free(c.cnt);
+    return run;
+}
+
+/* orc_sort_pairs with threads: LSD radix sort, 4 x 16-bit digits, each pass a
+ * per-slice count, one exclusive scan in (digit, slice) order and a per-slice
+ * scatter, so every pass is stable and the result equals orc_sort_pairs. */
+typedef struct {
+    uint64_t *a, *b;
+    int64_t n, per, slices;
+    int64_t *cnt;  /* [slices][65536] */
+    int sh;
+    int phase;     /* 0 count, 1 scatter */
+} rs_mt_t;
+
+static void rs_task(void *ctx, int64_t t)
+{
+    rs_mt_t *c = (rs_mt_t *)ctx;
+    int64_t b = c->per * t, e = b + c->per < c->n ? b + c->per : c->n;
+    int64_t *h = c->cnt + (size_t)t * 65536;
+    if (c->phase == 0) {
+        memset(h, 0, 65536 * sizeof(int64_t));
+        for (int64_t i = b; i < e; i++) h[(c->a[i] >> c->sh) & 0xffff]++;
+    } else {
+        for (int64_t i = b; i < e; i++) c->b[h[(c->a[i] >> c->sh) & 0xffff]++] = c->a[i];
+    }
+}
+
+typedef struct { orc_tuple *p; uint64_t *a; int64_t n, per; int dir; } pack_t;
+
+static void pack_task(void *ctx, int64_t t)
+{
+    pack_t *c = (pack_t *)ctx;
+    int64_t b = c->per * t, e = b + c->per < c->n ? b + c->per : c->n;
+    if (c->dir == 0)
+        for (int64_t i = b; i < e; i++) c->a[i] = ((uint64_t)c->p[i].key << 32) | c->p[i].pay;
+    else
+        for (int64_t i = b; i < e; i++) { c->p[i].key = (uint32_t)(c->a[i] >> 32); c->p[i].pay = (uint32_t)c->a[i]; }
+}
+
+int orc_sort_pairs_mt(orc_tuple *p, int64_t n, int nthreads)
+{
+    if (n <= 1) return ORC_OK;
+    if (nthreads < 1) nthreads = 1;
+    rs_mt_t c;
+    memset(&c, 0, sizeof(c));
+    c.n = n;
+    c.slices = nthreads;
+    c.per = (n + c.slices - 1) / c.slices;
+    c.a = (uint64_t *)malloc((size_t)n * 8);
+    c.b = (uint64_t *)malloc((size_t)n * 8);
+    c.cnt = (int64_t *)malloc((size_t)c.slices * 65536 * sizeof(int64_t));
+    if (!c.a || !c.b || !c.cnt) { free(c.a); free(c.b); free(c.cnt); return ORC_E_NOMEM; }
+    pack_t pk = {p, c.a, n, c.per, 0};
+    parallel_for(nthreads, c.slices, pack_task, &pk);
+    for (int pass = 0; pass < 4; pass++) {
+        c.sh = 16 * pass;
+        c.phase = 0;
+        parallel_for(nthreads, c.slices, rs_task, &c);
+        int64_t run = 0;
+        for (int d = 0; d < 65536; d++)
+            for (int64_t t = 0; t < c.slices; t++) {
+                int64_t v = c.cnt[(size_t)t * 65536 + d];
+                c.cnt[(size_t)t * 65536 + d] = run;
+                run += v;
+            }
+        c.phase = 1;
+        parallel_for(nthreads, c.slices, rs_task, &c);
+        uint64_t *tmp = c.a; c.a = c.b; c.b = tmp;
+    }
+    pk.a = c.a;
+    pk.dir = 1;
+    parallel_for(nthreads, c.slices, pack_task, &pk);
+    free(c.a); free(c.b); free(c.cnt);
+    return ORC_OK;
+}
+
+/* --------------------------------------------- benchmark-relation generator -- */
+
+/* The seeded relations of the benchmark, restated for the checker and for the
+ * CPU arms of the benchmark so that they need no product library: the same
+ * definitions as the product's generator, value for value (a CPU test compares
+ * the two on the host, a GPU test this one with the device's R and uniform S).
+ *   R[i] = (1 + perm_R(i), i): keys a permutation of 1..nR, payload the row id;
+ *   S[j] = (R[m(j)].key, j), m(j) uniform (zipf 0) or perm_rank(zipf_rank(j) - 1).
+ * Pieces: splitmix64 (Steele, Lea, Flood 2014); a 4-round unbalanced Feistel
+ * network on ceil(log2 n) bits with cycle-walking as the permutation; Zipf ranks
+ * by rejection-inversion (Hoermann and Derflinger, ACM TOMACS 6(3), 1996). */
+typedef struct { uint64_t n, seed; int lo_bits, hi_bits; } g_perm;
+
+static g_perm g_make_perm(uint64_t n, uint64_t seed)
+{
+    g_perm p;
+    p.n = n;
+    p.seed = seed;
+    int b = 2;
+    while ((1ull << b) < n) b++;
+    p.lo_bits = b / 2;
+    p.hi_bits = b - p.lo_bits;
+    return p;
+}
+
+static uint64_t g_feistel(const g_perm *p, uint64_t x)
+{
+    const uint64_t lo_mask = (1ull << p->lo_bits) - 1, hi_mask = (1ull << p->hi_bits) - 1;
+    uint64_t lo = x & lo_mask, hi = x >> p->lo_bits;
+    for (int r = 0; r < 4; r += 2) {
+        hi ^= mix64(p->seed + 0x9e3779b97f4a7c15ull * (uint64_t)(r + 1) + lo) & hi_mask;
+        lo ^= mix64(p->seed + 0x9e3779b97f4a7c15ull * (uint64_t)(r + 2) + hi) & lo_mask;
+    }
+    return (hi << p->lo_bits) | lo;
+}
+
+static uint64_t g_perm_apply(const g_perm *p, uint64_t x)
+{
+    uint64_t y = g_feistel(p, x);
+    while (y >= p->n) y = g_feistel(p, y);
+    return y;
+}
+
+static double g_unit(uint64_t seed, uint64_t idx, uint32_t attempt)
+{
+    uint64_t z = mix64(seed ^ mix64(idx * 0x9e3779b97f4a7c15ull + attempt));
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+typedef struct { double s, h_lo, h_hi, squeeze; uint64_t n; } g_zipf;
+
+static double g_rlog1p(double x) { return fabs(x) > 1e-8 ? log1p(x) / x : 1.0 - x * (0.5 - x * (1.0 / 3.0 - 0.25 * x)); }
+static double g_rexpm1(double x) { return fabs(x) > 1e-8 ? expm1(x) / x : 1.0 + 0.5 * x * (1.0 + (x / 3.0) * (1.0 + 0.25 * x)); }
+static double g_H(const g_zipf *z, double x) { double lx = log(x); return g_rexpm1((1.0 - z->s) * lx) * lx; }
+static double g_Hinv(const g_zipf *z, double y)
+{
+    double t = y * (1.0 - z->s);
+    if (t < -1.0) t = -1.0;
+    return exp(g_rlog1p(t) * y);
+}
+static double g_h(const g_zipf *z, double x) { return exp(-z->s * log(x)); }
+
+static g_zipf g_make_zipf(uint64_t n, double s)
+{
+    g_zipf z;
+    z.s = s;
+    z.n = n;
+    z.h_lo = g_H(&z, 1.5) - 1.0;
+    z.h_hi = g_H(&z, (double)n + 0.5);
+    z.squeeze = 2.0 - g_Hinv(&z, g_H(&z, 2.5) - g_h(&z, 2.0));
+    return z;
+}
+
+static uint64_t g_zipf_rank(const g_zipf *z, uint64_t seed, uint64_t idx)
+{
+    for (uint32_t a = 0;; a++) {
+        double y = z->h_hi + g_unit(seed, idx, a) * (z->h_lo - z->h_hi);
+        double x = g_Hinv(z, y);
+        double kd = x + 0.5;
+        uint64_t k = kd < 1.0 ? 1 : (uint64_t)kd;
+        if (k > z->n) k = z->n;
+        if ((double)k - x <= z->squeeze || y >= g_H(z, (double)k + 0.5) - g_h(z, (double)k)) return k;
+        if (a > 1000) return k;
+    }
+}
+
+static uint64_t g_seed_R(uint64_t s) { return mix64(s ^ 0x52454c4154494f4eull); }
+static uint64_t g_seed_rank(uint64_t s) { return mix64(s ^ 0x52414e4b4f524452ull); }
+static uint64_t g_seed_S(uint64_t s) { return mix64(s ^ 0x535354524541414dull); }
+
+typedef struct {
+    uint64_t seed, nR, nS;
+    double zipf;
+    g_perm pr, prank;
+    g_zipf z;
+    orc_tuple *R, *S;
+    int64_t slices;
+    uint64_t *part;  /* per-slice checksum of the expected pairs */
+} gen_t;
+
+static void gen_task(void *ctx, int64_t t)
+{
+    gen_t *g = (gen_t *)ctx;
+    if (g->R) {
+        uint64_t b = g->nR * (uint64_t)t / (uint64_t)g->slices, e = g->nR * (uint64_t)(t + 1) / (uint64_t)g->slices;
+        for (uint64_t i = b; i < e; i++) {
+            g->R[i].key = (uint32_t)(1 + g_perm_apply(&g->pr, i));
+            g->R[i].pay = (uint32_t)i;
+        }
+    }
+    uint64_t b = g->nS * (uint64_t)t / (uint64_t)g->slices, e = g->nS * (uint64_t)(t + 1) / (uint64_t)g->slices;
+    uint64_t acc = 0;
+    const uint64_t ss = g_seed_S(g->seed);
+    for (uint64_t j = b; j < e; j++) {
+        uint64_t row;
+        if (g->zipf <= 0.0)
+            row = (uint64_t)(((unsigned __int128)mix64(ss ^ (j * 0x9e3779b97f4a7c15ull)) * g->nR) >> 64);
+        else
+            row = g_perm_apply(&g->prank, g_zipf_rank(&g->z, ss, j) - 1);
+        if (g->S) {
+            g->S[j].key = (uint32_t)(1 + g_perm_apply(&g->pr, row));
+            g->S[j].pay = (uint32_t)j;
+        }
+        acc += mix64(((uint64_t)(uint32_t)row << 32) | (uint32_t)j);
+    }
+    g->part[t] = acc;
+}
+
+/* Fills R (nR tuples) and S (nS tuples; either may be NULL) and returns in
+ * *expect the checksum of the join's expected output {(m(j), j)}. */
+int orc_generate(uint64_t seed, int64_t nR, int64_t nS, double zipf_s, orc_tuple *R, orc_tuple *S,
+                 uint64_t *expect, int nthreads)
+{
+    if (nR <= 0 || nS < 0 || nR >= 0xFFFFFFFFll || zipf_s < 0) return ORC_E_ARG;
+    if (nthreads < 1) nthreads = 1;
+    gen_t g;
+    memset(&g, 0, sizeof(g));
+    g.seed = seed; g.nR = (uint64_t)nR; g.nS = (uint64_t)nS; g.zipf = zipf_s;
+    g.pr = g_make_perm(g.nR, g_seed_R(seed));
+    g.prank = g_make_perm(g.nR, g_seed_rank(seed));
+    g.z = g_make_zipf(g.nR, zipf_s > 0 ? zipf_s : 1.0);
+    g.R = R; g.S = S;
+    g.slices = 8 * (int64_t)nthreads;
+    g.part = (uint64_t *)calloc((size_t)g.slices, sizeof(uint64_t));
+    if (!g.part) return ORC_E_NOMEM;
+    parallel_for(nthreads, g.slices, gen_task, &g);
+    uint64_t s = 0;
+    for (int64_t t = 0; t < g.slices; t++) s += g.part[t];
+    free(g.part);
+    if (expect) *expect = s;
+    return ORC_OK;
 }

@@ -31,6 +31,10 @@ constexpr int kMaxPassBits = 8;       // buckets per scatter pass <= 256
 constexpr int kTile = 4096;           // tuples sorted per tile in shared memory
 constexpr int kDefaultTableSlots = 12288;  // 96 KB of shared memory
 constexpr int kDefaultUnitTuples = 65536;
+// Shared-memory hash-table slots (8 bytes each) a join CTA can hold on a device
+// with `max_smem` bytes of opt-in shared memory per block, leaving room for the
+// join kernels' static shared memory; pairs of slots are probed together.
+inline int max_table_slots_for(int max_smem) { return ((max_smem - 12288) / 8) & ~1; }
 
 // One relation (R or S) of one join.
 struct RelDev {

@@ -1,14 +1,17 @@
 // spj_noalloc.cu -- the join for callers that cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc at join time: a host runtime that has
-// handed all of the GPU's memory to its own pool allocator, code that runs while
-// a CUDA stream is being captured into a graph (allocation is not allowed in
-// capture), or a real-time loop that must not block on the allocator. For them
+// Some callers cannot call cudaMalloc at join time: a database engine or other
+// host runtime that has handed all of the GPU's memory to its own pool
+// allocator (so a cudaMalloc from inside a query would fail or steal from the
+// pool), or a latency-bound loop that must not stall on the allocator
+// (cudaMalloc and cudaFree can synchronise the device). For them
 // spj_join_noalloc runs the same partitioned hash join as spj_plan_execute, with
 // every piece of scratch memory taken from one fixed region compiled into this
 // library (kScratchBytes below), so the call itself allocates nothing. The price
 // is a size limit (|R| <= 2^20, |S| <= 2^21) and one shared region: calls whose
-// executions overlap on the GPU race on it.
+// executions overlap on the GPU race on it. The first call on each device does
+// a one-time set-up (the region's device address, kernel attributes); make that
+// first call before capturing any stream.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
@@ -66,7 +69,7 @@ int setup_device(int dev, DeviceSetup **out) {
         if (e != cudaSuccess) return cuda_error(e, "configure kernels");
         s.scratch = ptr;
         s.sms = prop.multiProcessorCount;
-        s.table_slots_max = (max_smem - 1024) / 8;
+        s.table_slots_max = max_table_slots_for(max_smem);
         s.done = true;
     }
     *out = &s;

@@ -77,7 +77,7 @@ static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 static int max_table_slots(int dev) {
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    return ((max_smem - 12288) / 8) & ~1;  // room for the join kernels' static shared memory
+    return max_table_slots_for(max_smem);
 }
 
 // ------------------------------------------------------------------ tuning --

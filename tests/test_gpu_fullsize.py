@@ -116,3 +116,38 @@ def test_config4_full_scale_batch(spj, free_cache):
         got = cs.cpu().numpy().astype(np.uint64).tolist()
         assert got == [e % (1 << 64) for e in exp]
     b.close()
+
+
+def test_c2_pairs_equal_oracle_byte_for_byte(spj, oracle, free_cache):
+    """Config 2 in full (2^27 R x 2^29 S, Zipf 1.0, -r 4 -R 4 -B 1) through the C
+    ABI: the pairs, copied to the host, equal the oracle's independent join byte
+    for byte after the canonical sort (ascending (R payload, S payload)); count
+    and checksum are checked beside it. The oracle's threaded join and sort give
+    the same bytes as its single-threaded ones (a CPU test pins that)."""
+    import time
+    import torch
+    n_r, n_s = 1 << 27, 1 << 29
+    t0 = time.time()
+    dR, dS, expect = _device_inputs(spj, n_r, n_s, 1.0, SEED)
+    plan = spj.Plan(n_r, n_s, spj.make_design(rank_num=4, rank_set=4, bank_set=1))
+    out = torch.empty((plan.output_capacity, 2), dtype=torch.int32, device="cuda")
+    n_out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    plan.execute(dR.data_ptr(), dS.data_ptr(), out.data_ptr(), n_out.data_ptr(), None)
+    torch.cuda.synchronize()
+    plan.stats()
+    plan.close()
+    k = int(n_out.item())
+    got = out[:k].cpu().numpy().view(np.uint32)
+    R = dR.cpu().numpy().view(np.uint32)
+    S = dS.cpu().numpy().view(np.uint32)
+    del out, dR, dS
+    torch.cuda.empty_cache()
+    t_gpu = time.time() - t0
+    want = oracle.simple_join_mt(R, S)
+    del R, S
+    assert k == want.shape[0] == n_s
+    assert oracle.checksum(got) == oracle.checksum(want) == expect & (2**64 - 1)
+    oracle.sort_pairs_mt(got, inplace=True)
+    oracle.sort_pairs_mt(want, inplace=True)
+    assert np.array_equal(got, want)
+    print(f"c2 byte-for-byte: {k} pairs; device part {t_gpu:.1f} s, oracle and sorts {time.time() - t0 - t_gpu:.1f} s")

@@ -272,3 +272,21 @@ def test_start_after_loading_columns_of_other_sizes(spj, oracle):
         assert out.shape == (n_s, 2) and oracle.checksum(out) == expect
     inst.close()
 
+
+
+@pytest.mark.parametrize("n_r,n_s,seed", [(1 << 20, 1 << 22, 0x5EED5EED), (100003, 777777, 5)])
+def test_oracle_generator_equals_device_generator(spj, oracle, n_r, n_s, seed):
+    """The CPU arms of the benchmark make their inputs with the oracle's copy of
+    the generator: R and uniform S equal the device generator's bytes, and the
+    expected checksums agree (Zipf S is compared with the product's host
+    generator on the CPU: its exp/log are the host's)."""
+    import torch
+    dR = torch.empty((n_r, 2), dtype=torch.int32, device="cuda")
+    dS = torch.empty((n_s, 2), dtype=torch.int32, device="cuda")
+    e = torch.zeros(1, dtype=torch.int64, device="cuda")
+    spj.check(spj.lib().spj_generate_device(seed, n_r, n_s, 0.0, dR.data_ptr(), dS.data_ptr(), e.data_ptr(), None))
+    torch.cuda.synchronize()
+    R, S, expect = oracle.generate(n_r, n_s, 0.0, seed=seed)
+    assert np.array_equal(dR.cpu().numpy().view(np.uint32), R)
+    assert np.array_equal(dS.cpu().numpy().view(np.uint32), S)
+    assert int(e.item()) & (2**64 - 1) == expect

@@ -125,3 +125,28 @@ def test_refpipe_replication_sizes(oracle, spj, layout):
     rs, ss = oracle.refpipe_dpu_sizes(R, S, ranks, rsets, bset)
     assert rs.sum() == 3000 * rsets * bset   # every R tuple on every replica of its partition
     assert ss.sum() == 9000                  # every S tuple on exactly one replica
+
+
+@pytest.mark.parametrize("n_r,n_s,zipf,seed", [(1000, 5000, 0.0, 3), (1 << 16, 1 << 18, 1.0, 2024),
+                                               (12345, 99999, 1.5, 7), (1 << 20, 1 << 21, 0.0, 0x5EED5EED)])
+def test_oracle_generator_equals_product_host_generator(oracle, spj, n_r, n_s, zipf, seed):
+    """The oracle's restated generator (used by the CPU arms of the benchmark,
+    which load no product library) gives the product generator's bytes and
+    expected checksum."""
+    R, S, e = oracle.generate(n_r, n_s, zipf, seed=seed)
+    R2, S2, e2 = spj.generate_host(n_r, n_s, zipf, seed=seed)
+    assert np.array_equal(R, R2) and np.array_equal(S, S2) and e == e2
+    assert oracle.checksum(oracle.simple_join_mt(R, S)) == e
+
+
+def test_threaded_join_and_sort_equal_single_threaded(oracle):
+    rng = np.random.default_rng(11)
+    # repeated R keys (the first in R order wins), key-0 padding, unmatched S keys
+    R = np.stack([rng.integers(0, 3000, 20000), rng.integers(0, 2**32, 20000)], axis=1).astype(np.uint32)
+    S = np.stack([rng.integers(0, 4000, 90000), np.arange(90000)], axis=1).astype(np.uint32)
+    for keep in (False, True):
+        a = oracle.simple_join(R, S, keep_unmatched=keep)
+        for t in (1, 3, 8):
+            assert np.array_equal(a, oracle.simple_join_mt(R, S, keep_unmatched=keep, nthreads=t))
+    for t in (1, 5, 16):
+        assert np.array_equal(oracle.sort_pairs(S), oracle.sort_pairs_mt(S, nthreads=t))

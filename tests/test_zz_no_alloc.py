@@ -1,6 +1,6 @@
 """spj_join_noalloc: the join for callers that cannot allocate device memory
-while they run it (a memory pool that owns the whole GPU, code under CUDA stream
-capture, a loop that must not wait on the allocator). Its output must equal that
+while they run it (a database engine whose pool allocator owns the whole GPU, a
+loop that must not stall on cudaMalloc/cudaFree). Its output must equal that
 of the regular entry point, spj_plan_execute, bit for bit (the pair multiset,
 compared after a canonical sort), on consecutive calls that reuse its fixed
 scratch region. This file is collected last on purpose."""
@@ -64,3 +64,52 @@ def test_noalloc_rejects_sizes_over_its_limit(spj):
     with pytest.raises(spj.SpjError, match="out_capacity"):
         spj.check(spj.lib().spj_join_noalloc(d.data_ptr(), 8, d.data_ptr(), 8, d.data_ptr(), 16,
                                              n.data_ptr(), None))
+
+
+def _keys_in_one_partition(oracle, n, bits=8):
+    """n distinct keys whose partition hash agrees in its low `bits` bits, so
+    they share one partition of the entry point's one-pass plan (at most 2^8
+    partitions)."""
+    cand = np.arange(1, 1 << 24, dtype=np.uint32)
+    keys = cand[(oracle.glb_partition_hash_np(cand) & ((1 << bits) - 1)) == 0]
+    assert keys.size >= n
+    return keys[:n]
+
+
+def test_noalloc_reports_capacity_errors_and_recovers(spj, oracle):
+    """An R whose keys all fall into one partition overflows that partition's
+    shared-memory table: the count comes back negative with the table bit
+    (error bit 1) set. The next call, on the same shared region, is exact again."""
+    import torch
+    keys = _keys_in_one_partition(oracle, 20000)
+    R = np.stack([keys, np.arange(keys.size)], axis=1).astype(np.uint32)
+    dR = _device(R)
+    cap = R.shape[0] + (1 << 21)
+    out = torch.empty((cap, 2), dtype=torch.int32, device="cuda")
+    n = torch.zeros(1, dtype=torch.int64, device="cuda")
+    spj.check(spj.lib().spj_join_noalloc(dR.data_ptr(), R.shape[0], dR.data_ptr(), R.shape[0], out.data_ptr(), cap,
+                                         n.data_ptr(), None))
+    torch.cuda.synchronize()
+    k = int(n.item())
+    assert k < 0 and ((-1 - k) & 1), f"expected the table-full status, got {k}"
+    R2, S2, expect = spj.generate_host(1 << 20, 1 << 21, 1.0, seed=21)
+    got = _noalloc_join(spj, _device(R2), _device(S2), 1 << 20, 1 << 21)
+    assert got.shape[0] == 1 << 21 and oracle.checksum(got) == expect
+
+
+def test_noalloc_call_leaves_free_device_memory_unchanged(spj):
+    import torch
+    R, S, _ = spj.generate_host(1 << 18, 1 << 20, 1.0, seed=31)
+    dR, dS = _device(R), _device(S)
+    cap = S.shape[0] + (1 << 21)
+    out = torch.empty((cap, 2), dtype=torch.int32, device="cuda")
+    n = torch.zeros(1, dtype=torch.int64, device="cuda")
+    args = (dR.data_ptr(), R.shape[0], dS.data_ptr(), S.shape[0], out.data_ptr(), cap, n.data_ptr(), None)
+    spj.check(spj.lib().spj_join_noalloc(*args))  # first call on the device: set-up
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        spj.check(spj.lib().spj_join_noalloc(*args))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert int(n.item()) == S.shape[0]
