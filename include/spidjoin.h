@@ -53,7 +53,8 @@ enum spj_join_alg {
 
 enum spj_skew_mode {
     SPJ_SKEW_ADAPTIVE = 0, /* heavy partitions split so no work unit exceeds unit_tuples S tuples
-                              (at least `group` units each); sampled heavy keys joined on the fly */
+                              (at least `group` units each); heavy keys found in a sample of S are
+                              joined on the fly (see heavy_sample) */
     SPJ_SKEW_FIXED = 1     /* every heavy partition split into exactly `group` units, the
                               reference's fixed rank-set x bank-set replication */
 };
@@ -76,7 +77,10 @@ typedef struct {
     int radix_bits;     /* partition fan-out = 2^radix_bits */
     int skew_mode;      /* enum spj_skew_mode */
     int unit_tuples;    /* max S tuples per work unit in adaptive mode */
-    int heavy_sample;   /* S keys sampled for heavy-key detection (-1 = off) */
+    int heavy_sample;   /* S keys sampled to find heavy keys, which the first scatter pass joins
+                           on the fly (at most 256 per join; their S tuples skip the
+                           partitioning): 0 = 65536 in the adaptive skew mode when |S| >= 2^20,
+                           else off; > 0 = that many (any skew mode); -1 = off */
     int table_slots;    /* shared-memory hash-table slots per CTA */
     int reserved[7];
 } spj_design_t;
@@ -128,8 +132,8 @@ typedef struct {
     double h2d_ms, partition_ms, join_ms, finish_ms, d2h_ms, total_ms;
     int64_t n_pairs;
     int64_t units;           /* work units executed */
-    int64_t heavy_keys;      /* keys joined on the fly */
-    int64_t heavy_tuples;    /* S tuples joined on the fly */
+    int64_t heavy_keys;      /* heavy keys of the join (found in the sample of S) */
+    int64_t heavy_tuples;    /* pairs the first scatter pass emitted for heavy-key S tuples */
     int64_t max_r_partition; /* largest R partition */
     int64_t max_s_partition; /* largest S partition */
     int radix_bits;

@@ -31,6 +31,13 @@ constexpr int kMaxPassBits = 8;       // buckets per scatter pass <= 256
 constexpr int kTile = 4096;           // tuples sorted per tile in shared memory
 constexpr int kDefaultTableSlots = 12288;  // 96 KB of shared memory
 constexpr int kDefaultUnitTuples = 65536;
+// Heavy keys of one join (S keys frequent enough in a sample of S to be joined on
+// the fly during the first scatter pass instead of being partitioned).
+constexpr int kHeavySlots = 512;          // open-addressing slots of the heavy table
+constexpr int kHeavyMax = 256;            // heavy keys per join (load <= 1/2)
+constexpr int kHeavySampleDefault = 65536;
+constexpr int kHeavySampleMax = 1 << 20;
+constexpr int kSampleSlots = 16384;       // shared-memory counting table of the sample
 // Shared-memory hash-table slots (8 bytes each) a join CTA can hold on a device
 // with `max_smem` bytes of opt-in shared memory per block, leaving room for the
 // join kernels' static shared memory; pairs of slots are probed together.
@@ -51,6 +58,17 @@ struct RelDev {
     uint32_t *base;      // [F] partition starts
 };
 
+// The heavy table of one join: written by the sampling kernel (keys), completed
+// by the count pass over R (the payload of one R tuple per heavy key, `found`),
+// read by the first scatter pass over S. Key 0 marks an empty slot.
+struct HeavyTab {
+    uint32_t n;        // heavy keys
+    uint32_t pad[3];
+    uint32_t key[kHeavySlots];
+    uint32_t pay[kHeavySlots];
+    uint32_t found[kHeavySlots];
+};
+
 struct Hole {
     unsigned long long begin, end;
 };
@@ -67,7 +85,8 @@ struct JoinCtr {
     unsigned int units;               // work units of the join
     unsigned int unit_base;           // its first unit in the queue
     unsigned int unit_fill;
-    unsigned int pad[3];
+    unsigned int heavy_keys;          // keys joined on the fly
+    unsigned long long heavy_tuples;  // S tuples joined on the fly (pairs emitted by the scatter)
 };
 
 // Per-join constants and output state.
@@ -90,6 +109,8 @@ struct JoinDev {
     unsigned long long *gap_off, *data_off;
     unsigned long long *gtable;       // non-partitioned hash join: global table
     unsigned long long gtable_slots;
+    HeavyTab *heavy;                  // null: no heavy-key path for this join
+    uint32_t heavy_sample;            // S keys sampled to find heavy keys
 };
 
 // A work unit: join j, partition p, S range [s_begin, s_end) of the partitioned S column.
@@ -122,6 +143,7 @@ struct PlanDev {
     int max_table_slots;      // join-kernel shared memory
     int alg;                  // one local-join algorithm per batch
     int any_two_pass;
+    int any_heavy;            // some join samples heavy keys
     Unit *units;
     uint32_t max_units;
     uint4 *items;             // pass-2 work items: (relation, coarse bucket, first chunk, end chunk)
@@ -145,6 +167,7 @@ struct JoinShape {
     uint32_t out_chunk = kOutChunk;
     uint32_t unit_tuples = kDefaultUnitTuples;
     unsigned long long gtable_slots = 0;
+    uint32_t heavy_sample = 0;  // 0: no heavy-key path
 };
 
 }  // namespace spj

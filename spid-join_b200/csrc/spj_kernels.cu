@@ -72,6 +72,102 @@ __global__ void k_init_single(PlanDev P, RelDev r0, RelDev r1, JoinDev j0, uint3
     P.jpart_prefix[1] = f;
 }
 
+// ------------------------------------------------------------ heavy keys --
+// SPID-Join spreads a skewed S partition over replicated R tables (rank-set and
+// bank-set replication, glb_partition_count.c:317-318,
+// glb_chipwise_partition_count.c:251-255). On the GPU the adaptive work units do
+// that for every heavy partition; on top of it, the keys that a sample of S
+// shows to be frequent are joined on the fly: the count pass over R records one
+// R payload per heavy key, and the first scatter pass over S emits the pairs of
+// heavy-key S tuples straight into the output instead of partitioning them, so
+// those tuples skip the second pass and the join's read.
+
+// Slot of a heavy key in the heavy table, or -1 (the table is read-only here).
+__device__ __forceinline__ int heavy_find(const HeavyTab *hv, uint32_t key) {
+    uint32_t s = (key * 0x9E3779B1u) >> (32 - 9);  // kHeavySlots = 2^9
+    for (int i = 0; i < kHeavySlots; i++) {
+        const uint32_t k = __ldg(&hv->key[s]);
+        if (k == key) return (int)s;
+        if (k == 0) return -1;
+        s = (s + 1) & (kHeavySlots - 1);
+    }
+    return -1;
+}
+
+// One CTA per join: samples heavy_sample S keys (one at a pseudo-random position
+// inside each of heavy_sample equal strides of S), counts them in a shared-memory
+// table and keeps the keys seen at least T times, T = max(4, sample/16384)
+// doubled until at most kHeavyMax keys remain. Which keys are chosen changes only
+// the speed, never the result.
+__global__ void __launch_bounds__(1024) k_heavy_sample(PlanDev P) {
+    extern __shared__ uint32_t smp[];
+    uint32_t *sk = smp, *sc = smp + kSampleSlots;
+    __shared__ unsigned s_cand, s_n;
+    const JoinDev &J = P.join[blockIdx.x];
+    HeavyTab *hv = J.heavy;
+    if (!hv) return;
+    for (int i = threadIdx.x; i < kSampleSlots; i += blockDim.x) sk[i] = sc[i] = 0;
+    for (int i = threadIdx.x; i < kHeavySlots; i += blockDim.x) {
+        hv->key[i] = 0;
+        hv->found[i] = 0;
+    }
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const RelDev &Rs = P.rel[2 * blockIdx.x + 1];
+    const uint64_t n = Rs.n;
+    const uint32_t m = (uint32_t)min((uint64_t)J.heavy_sample, n);
+    constexpr int U = 8;  // loads in flight per thread
+    for (uint32_t i0 = threadIdx.x; i0 < m; i0 += U * blockDim.x) {
+        uint32_t key[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const uint32_t i = i0 + k * blockDim.x;
+            key[k] = 0;
+            if (i < m) {
+                const uint64_t lo = (uint64_t)i * n / m, hi = (uint64_t)(i + 1) * n / m;
+                const uint64_t idx = lo + mix64(i * 0x9e3779b97f4a7c15ull + n) % (hi - lo);
+                key[k] = Rs.in[idx].key;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            if (!key[k]) continue;
+            uint32_t sl = (key[k] * 0x9E3779B1u) >> (32 - 14);  // kSampleSlots = 2^14
+            for (int step = 0; step < 64; step++) {  // a full neighbourhood drops the sample
+                const uint32_t prev = atomicCAS(&sk[sl], 0u, key[k]);
+                if (prev == 0u || prev == key[k]) {
+                    atomicAdd(&sc[sl], 1u);
+                    break;
+                }
+                sl = (sl + 1) & (kSampleSlots - 1);
+            }
+        }
+    }
+    uint32_t T = max(4u, m >> 14);
+    for (int iter = 0; iter < 24; iter++) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_cand = 0;
+        __syncthreads();
+        unsigned c = 0;
+        for (int i = threadIdx.x; i < kSampleSlots; i += blockDim.x) c += sc[i] >= T ? 1u : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if ((threadIdx.x & 31) == 0 && c) atomicAdd(&s_cand, c);
+        __syncthreads();
+        if (s_cand <= (unsigned)kHeavyMax) break;
+        T *= 2;
+    }
+    for (int i = threadIdx.x; i < kSampleSlots; i += blockDim.x) {
+        const uint32_t key = sk[i];
+        if (!key || sc[i] < T || atomicAdd(&s_n, 1u) >= (unsigned)kHeavyMax) continue;
+        uint32_t sl = (key * 0x9E3779B1u) >> (32 - 9);
+        for (int step = 0; step < kHeavySlots && atomicCAS(&hv->key[sl], 0u, key) != 0u; step++)
+            sl = (sl + 1) & (kHeavySlots - 1);  // at most 256 of the 512 slots are taken
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) hv->n = min(s_n, (unsigned)kHeavyMax);
+}
+
 // ------------------------------------------------------------- histogram --
 // glb_partition_count.c:119-236 on B200: each CTA counts one contiguous chunk
 // into a shared-memory histogram; key-0 tuples are skipped (:190-192).
@@ -83,9 +179,24 @@ __global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P) {
     const int bits = P.join[R.join].bits, b2 = P.join[R.join].fine_bits;
     const uint32_t F = 1u << bits, mask = F - 1;
     for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) sh[i] = 0;
+    // heavy keys: R records one payload per heavy key, S leaves them out of its
+    // partitions (the first scatter pass joins them on the fly)
+    HeavyTab *hv = P.join[R.join].heavy;
+    const int hmode = (hv && hv->n) ? ((r & 1u) ? 2 : 1) : 0;  // 1: R, 2: S
     __syncthreads();
     const uint32_t b = c * R.chunk;
     const uint32_t e = min(R.n, b + R.chunk);
+    auto count = [&](uint32_t key, uint32_t pay) {
+        if (!key) return;
+        if (hmode) {
+            const int hs = heavy_find(hv, key);
+            if (hs >= 0) {
+                if (hmode == 2) return;
+                if (atomicCAS(&hv->found[hs], 0u, 1u) == 0u) hv->pay[hs] = pay;
+            }
+        }
+        atomicAdd(&sh[glb_partition_hash(key) & mask], 1u);
+    };
     if (b < e) {
         const uint4 *in2 = reinterpret_cast<const uint4 *>(R.in);
         const uint32_t b2i = b >> 1, e2 = e >> 1;
@@ -99,13 +210,13 @@ __global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P) {
             }
 #pragma unroll
             for (int k = 0; k < U; k++) {
-                if (v[k].x) atomicAdd(&sh[glb_partition_hash(v[k].x) & mask], 1u);
-                if (v[k].z) atomicAdd(&sh[glb_partition_hash(v[k].z) & mask], 1u);
+                count(v[k].x, v[k].y);
+                count(v[k].z, v[k].w);
             }
         }
         if ((e & 1u) && threadIdx.x == 0) {
-            uint32_t key = R.in[e - 1].key;
-            if (key) atomicAdd(&sh[glb_partition_hash(key) & mask], 1u);
+            const Tuple t = R.in[e - 1];
+            count(t.key, t.pay);
         }
     }
     __syncthreads();
@@ -224,7 +335,29 @@ struct __align__(128) TileSmem {
     uint32_t valid;
     uint32_t seg_begin, seg_len;
     uint32_t item;
+    uint32_t hcnt;             // heavy pairs of the tile being ranked
+    uint32_t hoff, hlen, hpos; // the tile's heavy pairs: stage slot, count, output position
 };
+
+// Where heavy-key S tuples go in the first scatter pass over S: their pairs are
+// appended to the join's output (positions reserved per tile with one atomic).
+struct HeavyOut {
+    const HeavyTab *hv;
+    uint2 *out;
+    uint32_t cap;
+    JoinCtr *ctr;
+    int keep_unmatched;  // SMJ/NL keep an unmatched S tuple as it is
+};
+
+// The output value of heavy-key S tuple t (slot hs): its pair, the tuple itself
+// when unmatched and kept, or nothing (false).
+__device__ __forceinline__ bool heavy_value(const HeavyOut &h, int hs, Tuple &t) {
+    if (__ldg(&h.hv->found[hs])) {
+        t.key = __ldg(&h.hv->pay[hs]);
+        return true;
+    }
+    return h.keep_unmatched != 0;
+}
 
 // Scatters in[b, e) to out[cursor[bucket] ...], advancing the cursors. Input
 // tiles arrive by bulk copy (TMA) into a double buffer, so the next tile is in
@@ -240,10 +373,27 @@ struct __align__(128) TileSmem {
 //    ordinary store at each end, issued by the bucket's thread. The writer
 //    threads' proxy fence is the price; long runs (hot buckets) repay it.
 // Returns false (the same value in every thread) when a bulk copy timed out.
-template <bool kHot, bool kBulk, typename BucketFn>
+// With kHeavy (the first pass over S of a join with heavy keys) a tuple whose key
+// is in the heavy table does not go to a bucket: its output value is staged
+// after the buckets' runs and written to the join's output (see HeavyOut).
+// The tile's heavy pairs, staged at [hoff, hoff + hlen), to the join's output at
+// hpos (coalesced stores by all threads; called after the stage barrier).
+__device__ __forceinline__ void write_heavy_run(const TileSmem &S, const HeavyOut &h) {
+    const uint32_t n = S.hlen, off = S.hoff, pos = S.hpos;
+    const uint2 *st2 = reinterpret_cast<const uint2 *>(S.stage);
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+        if (pos + j < h.cap)
+            h.out[pos + j] = st2[off + j];
+        else
+            atomicOr(&h.ctr->error, 2u);
+    }
+}
+
+template <bool kHot, bool kBulk, bool kHeavy = false, typename BucketFn>
 __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint32_t b, uint32_t e,
                                               Tuple *__restrict__ out, TileSmem &S, int nb, BucketFn bucket_of,
-                                              uint32_t (&uses)[2], unsigned int *err) {
+                                              uint32_t (&uses)[2], unsigned int *err,
+                                              const HeavyOut *hvo = nullptr) {
     constexpr int PER = kTile / kScatterThreads;
     constexpr uint32_t kBulkMin = 8;  // bulk-store bodies shorter than this go by ordinary stores
     uint2 *o2 = reinterpret_cast<uint2 *>(out);
@@ -256,8 +406,19 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
         const uint32_t idx = head ? b : e - 1;
         // head: index b when odd; tail: index e-1 when e is odd, unless that is the head
         if ((head && (b & 1u)) || (!head && (e & 1u) && !((b & 1u) && e - 1 == b))) {
-            const Tuple t = in[idx];
-            if (t.key) {
+            Tuple t = in[idx];
+            int hs = -1;
+            if (kHeavy && t.key) hs = heavy_find(hvo->hv, t.key);
+            if (hs >= 0) {
+                if (heavy_value(*hvo, hs, t)) {
+                    const uint32_t pos = (uint32_t)atomicAdd(&hvo->ctr->out_reserved, 1ull);
+                    if (pos < hvo->cap)
+                        hvo->out[pos] = make_uint2(t.key, t.pay);
+                    else
+                        atomicOr(&hvo->ctr->error, 2u);
+                    atomicAdd(&hvo->ctr->heavy_tuples, 1ull);
+                }
+            } else if (t.key) {
                 const uint32_t pos = atomicAdd(&S.cursor[bucket_of(t.key)], 1u);
                 o2[pos] = make_uint2(t.key, t.pay);
             }
@@ -301,6 +462,26 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
         for (int k = 0; k < PER; k++) {
             const uint32_t idx = threadIdx.x + k * kScatterThreads;
             v[k] = idx < nt ? S.inbuf[buf][idx] : Tuple{0u, 0u};
+            if (kHeavy) {  // heavy key: rank among the tile's heavy pairs (one counter add per warp)
+                int hs = v[k].key ? heavy_find(hvo->hv, v[k].key) : -1;
+                const bool isH = hs >= 0;
+                const bool emit = isH && heavy_value(*hvo, hs, v[k]);
+                const unsigned hm = __ballot_sync(0xffffffffu, emit);
+                if (hm) {
+                    const int leader = __ffs(hm) - 1;
+                    uint32_t base = 0;
+                    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&S.hcnt, (uint32_t)__popc(hm));
+                    base = __shfl_sync(0xffffffffu, base, leader);
+                    if (emit) {
+                        br[k] = 0xfffe0000u | (base + __popc(hm & lanemask_lt()));
+                        continue;
+                    }
+                }
+                if (isH) {  // heavy and unmatched, not kept: dropped
+                    br[k] = 0xffff0000u;
+                    continue;
+                }
+            }
             const uint32_t bk = v[k].key ? (uint32_t)bucket_of(v[k].key) : 0xffffu;
             if (kHot) {
                 const uint32_t b0 = __shfl_sync(0xffffffffu, bk, 0);
@@ -351,12 +532,24 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
                 }
             }
             if (!kBulk && lane == 31) S.valid = incl;
+            if (kHeavy && lane == 31) {  // heavy pairs after the buckets' runs
+                const uint32_t h = S.hcnt;
+                S.hoff = incl;
+                S.hlen = h;
+                S.hcnt = 0;
+                if (h) {
+                    S.hpos = (uint32_t)atomicAdd(&hvo->ctr->out_reserved, (unsigned long long)h);
+                    atomicAdd(&hvo->ctr->heavy_tuples, (unsigned long long)h);
+                }
+            }
         }
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < PER; k++) {
             const uint32_t bk = br[k] >> 16;
-            if (bk != 0xffffu) {
+            if (kHeavy && bk == 0xfffeu) {
+                S.stage[S.hoff + (br[k] & 0xffffu)] = v[k];
+            } else if (bk != 0xffffu) {
                 const uint32_t slot = S.off[bk] + (br[k] & 0xffffu);
                 S.stage[slot] = v[k];
                 if (!kBulk) S.bkt[slot] = (uint8_t)bk;
@@ -385,6 +578,7 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
             }
             // the next tile's rank phase may start: counts are zero, and the stage
             // is rewritten only after its writers' bulk stores have read it
+            if (kHeavy) write_heavy_run(S, *hvo);
         } else {
             __syncthreads();
             // write phase, unrolled so all shared loads are in flight before the stores
@@ -407,6 +601,7 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
                 const uint32_t j = threadIdx.x + k * kScatterThreads;
                 if (j < valid) o2[br[k]] = make_uint2(v[k].key, v[k].pay);
             }
+            if (kHeavy) write_heavy_run(S, *hvo);
             // the next tile's rank phase may start: counts are zero, and its first
             // barrier orders these reads of stage/wpos before they are rewritten
         }
@@ -421,6 +616,7 @@ constexpr int kBulkMaxBuckets = 128;
 
 __device__ __forceinline__ void tile_init(TileSmem &S) {
     for (int i = threadIdx.x; i < 256; i += blockDim.x) S.cnt[i] = 0;
+    if (threadIdx.x == 0) S.hcnt = 0;
     if (threadIdx.x == 0) {
         mbar_init(&S.bar[0], 1);
         mbar_init(&S.bar[1], 1);
@@ -457,10 +653,18 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
     Tuple *dst = b2 ? R.tmp : R.out;
     uint32_t uses[2] = {0, 0};
     auto coarse = [=](uint32_t key) { return (int)((glb_partition_hash(key) & mask) >> b2); };
-    if (nb <= kBulkMaxBuckets)
+    const bool heavy = (r & 1u) && J.heavy && J.heavy->n;  // S of a join with heavy keys
+    if (heavy) {
+        const HeavyOut hvo{J.heavy, reinterpret_cast<uint2 *>(J.out), (uint32_t)J.out_cap, J.ctr, J.keep_unmatched};
+        if (nb <= kBulkMaxBuckets)
+            scatter_range<false, true, true>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo);
+        else
+            scatter_range<false, false, true>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo);
+    } else if (nb <= kBulkMaxBuckets) {
         scatter_range<false, true>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error);
-    else
+    } else {
         scatter_range<false, false>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error);
+    }
     bulk_wait_all();  // this thread's bulk stores are performed before the CTA retires
 }
 
@@ -652,9 +856,28 @@ __global__ void __launch_bounds__(1024) k_units_scan(PlanDev P) {
     __syncthreads();
     uint32_t run = warp_sums[warp] + incl - sum;
     for (uint32_t j = beg; j < end; j++) {
-        JoinCtr *c = P.join[j].ctr;
+        const JoinDev &J = P.join[j];
+        JoinCtr *c = J.ctr;
         c->unit_base = run;
         run += c->units;
+        // the pairs of heavy keys, appended by the first scatter pass, end on a
+        // whole output chunk, so every join chunk is aligned; the rest of their
+        // last chunk is a hole for the fix-up
+        if (J.heavy) {
+            c->heavy_keys = J.heavy->n;
+            const unsigned long long H = c->out_reserved, ch = J.out_chunk;
+            const unsigned long long A = (H + ch - 1) / ch * ch;
+            if (A > H) {
+                const unsigned h = atomicAdd(&c->hole_count, 1u);
+                if (h < kMaxHoles) {
+                    J.holes[h].begin = H;
+                    J.holes[h].end = A;
+                } else {
+                    atomicOr(&c->error, 8u);
+                }
+                c->out_reserved = A;
+            }
+        }
     }
 }
 
@@ -1493,6 +1716,9 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
         mark(4);
         k_nphj_probe<<<pl->join_blocks, kJoinThreads, 0, st>>>(P);
     } else {
+        // heavy keys are sampled when R is partitioned; executions that keep R's
+        // partitions keep its heavy table too
+        if (P.any_heavy && !keep_r) k_heavy_sample<<<J, 1024, (size_t)kSampleSlots * 8, st>>>(P);
         k_hist<<<P.total_chunks, kHistThreads, (size_t)4 << P.max_bits, st>>>(P);
         mark(1);
         k_colscan<<<(P.total_parts + 255) / 256, 256, 0, st>>>(P);
@@ -1542,6 +1768,8 @@ cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm)
                                       max_smem - (int)fa.sharedSizeBytes - 1024)))
             return e;
     }
+    e = cudaFuncSetAttribute(k_heavy_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, kSampleSlots * 8);
+    if (e) return e;
     e = cudaFuncSetAttribute(k_scatter1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));
     if (e) return e;
     e = cudaFuncSetAttribute(k_scatter2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));

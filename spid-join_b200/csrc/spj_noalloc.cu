@@ -120,6 +120,7 @@ extern "C" int spj_join_noalloc(const spj_kv_pair_t *r, int64_t n_r, const spj_k
     pl.n_s = n_s;
     spj_design_default(&pl.design);
     pl.design.rank_num = 1;
+    pl.design.heavy_sample = -1;  // no heavy-key table in the fixed region
     pl.device = dev;
     pl.num_sms = ds->sms;
     pl.have_events = false;

@@ -173,6 +173,19 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     uint32_t oc = 32;
     while (oc < oc_max && (int64_t)oc * 8192 < n_s) oc <<= 1;
     sh.out_chunk = oc;
+    // Heavy keys joined on the fly: S keys frequent in a sample of S are joined
+    // during the first scatter pass (their R payloads found by the count pass
+    // over R) and never partitioned. On by default for the adaptive skew mode
+    // when S has at least 2^20 tuples; heavy_sample > 0 sets the sample size
+    // (also in the fixed mode), -1 turns it off.
+    if (d.join_alg != SPJ_ALG_NPHJ && d.heavy_sample >= 0 && n_s > 0) {
+        int64_t hs = 0;
+        if (d.heavy_sample > 0)
+            hs = d.heavy_sample;
+        else if (d.skew_mode == SPJ_SKEW_ADAPTIVE && n_s >= (1 << 20))
+            hs = kHeavySampleDefault;
+        sh.heavy_sample = (uint32_t)std::min<int64_t>(std::min<int64_t>(hs, kHeavySampleMax), n_s);
+    }
     sh.unit_tuples = d.unit_tuples > 0                ? (uint32_t)d.unit_tuples
                      : (tune && tune->unit_tuples > 0) ? (uint32_t)tune->unit_tuples
                                                        : (uint32_t)kDefaultUnitTuples;
@@ -194,7 +207,7 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
     const size_t o_pref = take((3 * (2 * J + 1) + J + 1) * 4);
     uint64_t max_units = 64, max_items = 1;
     uint32_t tot_chunks = 0, tot_parts = 0, tot_coarse = 0, tot_jparts = 0;
-    int max_bits = 0, max_ts = 2, two = 0;
+    int max_bits = 0, max_ts = 2, two = 0, any_heavy = 0;
     const uint32_t warps = (uint32_t)pl->join_blocks * (kJoinThreads / 32);
     std::vector<uint32_t> chunk_pref(2 * J + 1), part_pref(2 * J + 1), coarse_pref(2 * J + 1), jpart_pref(J + 1);
     for (uint32_t j = 0; j < J; j++) {
@@ -219,7 +232,9 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
         jd.unit_tuples = sh.unit_tuples;
         jd.item_target = sh.item_target;
         jd.out_chunk = sh.out_chunk;
-        jd.out_cap = (unsigned long long)h.n_s + (unsigned long long)warps * sh.out_chunk;
+        // one output chunk per join warp, plus one for the pairs of heavy keys
+        // (their region is rounded up to whole chunks before the join)
+        jd.out_cap = (unsigned long long)h.n_s + (unsigned long long)(warps + 1) * sh.out_chunk;
         jd.gtable_slots = nphj ? sh.gtable_slots : 0;
         const int64_t n[2] = {h.n_r, h.n_s};
         for (int r = 0; r < 2; r++) {
@@ -257,6 +272,8 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
         const size_t o_datas = take(kMaxHoles * sizeof(Hole));
         const size_t o_goff = take(kMaxHoles * 8), o_doff = take(kMaxHoles * 8);
         const size_t o_gt = take(nphj ? jd.gtable_slots * 8 : 0);
+        const size_t o_hv = take(sh.heavy_sample ? sizeof(HeavyTab) : 0);
+        jd.heavy_sample = sh.heavy_sample;
         if (a) {
             jd.ctr = (JoinCtr *)(a + o_ctr + sizeof(BatchCtr)) + j;
             jd.holes = (Hole *)(a + o_holes);
@@ -265,7 +282,9 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
             jd.gap_off = (unsigned long long *)(a + o_goff);
             jd.data_off = (unsigned long long *)(a + o_doff);
             jd.gtable = nphj ? (unsigned long long *)(a + o_gt) : nullptr;
+            jd.heavy = sh.heavy_sample ? (HeavyTab *)(a + o_hv) : nullptr;
         }
+        any_heavy |= sh.heavy_sample ? 1 : 0;
         max_units += nphj ? (uint64_t)h.n_s / jd.unit_tuples + 64
                           : F * (uint64_t)std::max(jd.group, 1) + (uint64_t)h.n_s / jd.unit_tuples + F + 64;
         if (f1) max_items += (uint64_t)(sh.nchunks[0] + sh.nchunks[1]) * f1 + 2 * f1;
@@ -297,6 +316,7 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
         P.max_table_slots = max_ts;
         P.alg = d.join_alg;
         P.any_two_pass = two;
+        P.any_heavy = any_heavy;
         P.units = (Unit *)(a + o_units);
         P.max_units = (uint32_t)std::min<uint64_t>(max_units, 0xFFFFFFFFull);
         P.items = (uint4 *)(a + o_items);
@@ -527,7 +547,7 @@ int64_t join_output_capacity(int64_t n_r, int64_t n_s, const spj_design_t &d, bo
                                     alone ? nullptr : find_tuning(n_r, n_s, &tn));
     const int per_sm = 2048 / kJoinThreads;
     const int blocks = std::min(per_sm * sms, kMaxHoles / (kJoinThreads / 32));
-    return n_s + (int64_t)blocks * (kJoinThreads / 32) * sh.out_chunk;
+    return n_s + ((int64_t)blocks * (kJoinThreads / 32) + 1) * sh.out_chunk;
 }
 
 // Executes a one-join plan; with keep_r, R's partitions from the plan's previous
@@ -578,6 +598,8 @@ static void fill_stats(const spj_plan *pl, const JoinCtr &c, spj_stats_t *out) {
     out->max_s_partition = c.max_s_part;
     out->radix_bits = pl->shapes[0].bits;
     out->table_slots = pl->shapes[0].table_slots;
+    out->heavy_keys = c.heavy_keys;
+    out->heavy_tuples = (int64_t)c.heavy_tuples;
 }
 
 static int ctr_error(const spj_plan *pl, unsigned err, unsigned max_r) {
