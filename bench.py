@@ -47,14 +47,23 @@ SEED = 0x5EED5EED
 METRIC = "join tuples/s (|R|+|S|)"
 
 
-def launches_per_join(alg, radix_bits, single=True):
+def launches_per_join(alg, radix_bits, single=True, heavy=False):
     """Kernels of this library one plan execution launches (see launch_pipeline):
     k_init_single for a single-join plan; the non-partitioned join has no
-    partitioning passes; a second scatter pass (and its work list) above 8 radix bits."""
+    partitioning passes; a second scatter pass (and its work list) above 8 radix
+    bits; the heavy-key sample and the heavy first scatter pass when the plan
+    samples heavy keys."""
     n = 1 if single else 0
     if alg == 1:
         return n + 8
-    return n + 10 + (2 if radix_bits > 8 else 0)
+    return n + 10 + (2 if radix_bits > 8 else 0) + (2 if heavy else 0)
+
+
+def samples_heavy(args, n_s):
+    """Whether the plan samples heavy keys for this join (the planner's rule)."""
+    if args.alg == 1 or args.heavy < 0:
+        return False
+    return args.heavy > 0 or (args.skew == 0 and n_s >= (1 << 20))
 
 
 def peaks():
@@ -270,7 +279,7 @@ def device_join_leg(spj, n_r, n_s, zipf, layout, args, steps, warmup, seed, samp
     design = spj.make_design(rank_num=ranks, rank_set=rsets, bank_set=bset, join_alg=args.alg,
                              skew_mode=args.skew, input_size=n_r, rs_ratio=max(n_s // n_r, 1),
                              zipf_factor=int(round(zipf * 100)), radix_bits=args.bits,
-                             table_slots=args.slots, unit_tuples=args.unit)
+                             table_slots=args.slots, unit_tuples=args.unit, heavy_sample=args.heavy)
     ws, rank, local = dist_env()
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
@@ -428,6 +437,8 @@ def run_ours(args):
             "uniform_ms": uni["ms_step"], "zipf_1_5_ms": z15["ms_step"], "zipf_1_0_ms": ms_step,
             "zipf_1_5_vs_uniform": z15["ms_step"] / uni["ms_step"], "target": "<= 1.5",
             "steps": k, "checked": uni["ok"] and z15["ok"],
+            "kernels_ms": {"uniform": uni["kmean"], "zipf_1_5": z15["kmean"]},
+            "heavy_keys": {"uniform": uni["stats"]["heavy_keys"], "zipf_1_5": z15["stats"]["heavy_keys"]},
             "clocks": {"uniform": uni["clocks"], "zipf_1_5": z15["clocks"]}}
         extra["batched"] = batched_compare(spj, args, steps=max(3, min(args.steps, 5)), warmup=3)
 
@@ -449,10 +460,10 @@ def run_ours(args):
                                   "algorithmic_bytes": pipe_bytes, "formula": "24*(|R|+|S|) + 8*|out|"},
             "kernels_ms": kmean,
             "e2e": e2e, "cpu_baseline": cpu,
-            "gpu_launches": launches_per_join(args.alg, st["radix_bits"]) * args.steps,
+            "gpu_launches": launches_per_join(args.alg, st["radix_bits"], heavy=samples_heavy(args, n_s)) * args.steps,
             "clocks": leg["clocks"],
             "check": {"n_pairs": n_pairs, "checksum_ok": leg["ok"], "max_s_partition": st["max_s_partition"],
-                      "units": st["units"]},
+                      "units": st["units"], "heavy_keys": st["heavy_keys"], "heavy_tuples": st["heavy_tuples"]},
         }
         line.update(extra)
         emit(line)
@@ -948,6 +959,8 @@ def main():
     ap.add_argument("--bits", type=int, default=0, help="radix bits (0 = planner)")
     ap.add_argument("--slots", type=int, default=0, help="table slots per CTA (0 = planner)")
     ap.add_argument("--unit", type=int, default=0, help="max S tuples per work unit (0 = planner)")
+    ap.add_argument("--heavy", type=int, default=0,
+                    help="S keys sampled for heavy keys joined on the fly (0 = planner, -1 = off)")
     ap.add_argument("--c4-scale", type=float, default=1.0, help="scale of the config-4 relation sizes")
     ap.add_argument("--tuning", default=os.path.join(ROOT, "spid-join_b200", "tuning_b200.json"),
                     help="batched workload: autotuner table to install ('' = the planner alone)")

@@ -79,8 +79,11 @@ typedef struct {
     int unit_tuples;    /* max S tuples per work unit in adaptive mode */
     int heavy_sample;   /* S keys sampled to find heavy keys, which the first scatter pass joins
                            on the fly (at most 256 per join; their S tuples skip the
-                           partitioning): 0 = 65536 in the adaptive skew mode when |S| >= 2^20,
-                           else off; > 0 = that many (any skew mode); -1 = off */
+                           partitioning): 0 = 16384 in the adaptive skew mode when |S| >= 2^20,
+                           kept only when the heavy keys hold at least 60% of the sample (below
+                           that the per-tuple filter lookups cost more than they save), else
+                           off; > 0 = that many, kept whatever their share (any skew mode);
+                           -1 = off */
     int table_slots;    /* shared-memory hash-table slots per CTA */
     int reserved[7];
 } spj_design_t;

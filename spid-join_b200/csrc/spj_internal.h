@@ -35,9 +35,10 @@ constexpr int kDefaultUnitTuples = 65536;
 // the fly during the first scatter pass instead of being partitioned).
 constexpr int kHeavySlots = 512;          // open-addressing slots of the heavy table
 constexpr int kHeavyMax = 256;            // heavy keys per join (load <= 1/2)
-constexpr int kHeavySampleDefault = 65536;
+constexpr int kHeavySampleDefault = 16384;  // a key of 1/1000 of S is seen ~16 times
 constexpr int kHeavySampleMax = 1 << 20;
 constexpr int kSampleSlots = 16384;       // shared-memory counting table of the sample
+constexpr double kHeavyMinShare = 0.6;    // automatic mode: least sample share of the heavy keys
 // Shared-memory hash-table slots (8 bytes each) a join CTA can hold on a device
 // with `max_smem` bytes of opt-in shared memory per block, leaving room for the
 // join kernels' static shared memory; pairs of slots are probed together.
@@ -111,6 +112,8 @@ struct JoinDev {
     unsigned long long gtable_slots;
     HeavyTab *heavy;                  // null: no heavy-key path for this join
     uint32_t heavy_sample;            // S keys sampled to find heavy keys
+    int heavy_auto;                   // the planner chose the sample: keep heavy keys only when
+                                      // they hold at least kHeavyMinShare of it
 };
 
 // A work unit: join j, partition p, S range [s_begin, s_end) of the partitioned S column.
@@ -168,6 +171,7 @@ struct JoinShape {
     uint32_t unit_tuples = kDefaultUnitTuples;
     unsigned long long gtable_slots = 0;
     uint32_t heavy_sample = 0;  // 0: no heavy-key path
+    int heavy_auto = 0;
 };
 
 }  // namespace spj

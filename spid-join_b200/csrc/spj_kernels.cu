@@ -82,11 +82,43 @@ __global__ void k_init_single(PlanDev P, RelDev r0, RelDev r1, JoinDev j0, uint3
 // heavy-key S tuples straight into the output instead of partitioning them, so
 // those tuples skip the second pass and the join's read.
 
-// Slot of a heavy key in the heavy table, or -1 (the table is read-only here).
-__device__ __forceinline__ int heavy_find(const HeavyTab *hv, uint32_t key) {
-    uint32_t s = (key * 0x9E3779B1u) >> (32 - 9);  // kHeavySlots = 2^9
+// A CTA's copy of the heavy table in shared memory, with a 2^14-bit filter of
+// the keys' Fibonacci hashes, so that most tuples are told apart from the heavy
+// keys by one shared-memory word (a random gather from the global table would
+// cost a wavefront per line and compete with the tile sort for the L1 pipe).
+struct HeavySmem {
+    uint32_t bm[512];        // filter bit (key * 0x9E3779B1) >> 18
+    uint32_t key[kHeavySlots];
+    uint32_t pay[kHeavySlots];
+    uint32_t found[kHeavySlots / 32];
+};
+
+// Loads the heavy table of one join into shared memory (all threads; callers
+// synchronise before use).
+__device__ __forceinline__ void heavy_smem_load(HeavySmem &H, const HeavyTab *hv) {
+    for (int i = threadIdx.x; i < 512; i += blockDim.x) H.bm[i] = 0;
+    for (int i = threadIdx.x; i < kHeavySlots / 32; i += blockDim.x) H.found[i] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < kHeavySlots; i += blockDim.x) {
+        const uint32_t k = hv->key[i];
+        H.key[i] = k;
+        H.pay[i] = hv->pay[i];
+        if (k) {
+            const uint32_t bi = (k * 0x9E3779B1u) >> 18;
+            atomicOr(&H.bm[bi >> 5], 1u << (bi & 31));
+            if (hv->found[i]) atomicOr(&H.found[i >> 5], 1u << (i & 31));
+        }
+    }
+}
+
+// Slot of a heavy key in the shared-memory table, or -1.
+__device__ __forceinline__ int heavy_find(const HeavySmem &H, uint32_t key) {
+    const uint32_t prod = key * 0x9E3779B1u;
+    const uint32_t bi = prod >> 18;
+    if (!((H.bm[bi >> 5] >> (bi & 31)) & 1u)) return -1;
+    uint32_t s = prod >> (32 - 9);  // kHeavySlots = 2^9
     for (int i = 0; i < kHeavySlots; i++) {
-        const uint32_t k = __ldg(&hv->key[s]);
+        const uint32_t k = H.key[s];
         if (k == key) return (int)s;
         if (k == 0) return -1;
         s = (s + 1) & (kHeavySlots - 1);
@@ -131,12 +163,15 @@ __global__ void __launch_bounds__(1024) k_heavy_sample(PlanDev P) {
         }
 #pragma unroll
         for (int k = 0; k < U; k++) {
-            if (!key[k]) continue;
+            // lanes holding the same key add to its counter once (a hot key's
+            // counter would otherwise take thousands of serialised atomics)
+            const unsigned same = __match_any_sync(0xffffffffu, key[k]);
+            if (!key[k] || (threadIdx.x & 31) != (unsigned)(__ffs(same) - 1)) continue;
             uint32_t sl = (key[k] * 0x9E3779B1u) >> (32 - 14);  // kSampleSlots = 2^14
-            for (int step = 0; step < 64; step++) {  // a full neighbourhood drops the sample
+            for (int step = 0; step < 16; step++) {  // a full neighbourhood drops the sample
                 const uint32_t prev = atomicCAS(&sk[sl], 0u, key[k]);
                 if (prev == 0u || prev == key[k]) {
-                    atomicAdd(&sc[sl], 1u);
+                    atomicAdd(&sc[sl], (uint32_t)__popc(same));
                     break;
                 }
                 sl = (sl + 1) & (kSampleSlots - 1);
@@ -157,6 +192,20 @@ __global__ void __launch_bounds__(1024) k_heavy_sample(PlanDev P) {
         if (s_cand <= (unsigned)kHeavyMax) break;
         T *= 2;
     }
+    // automatic mode: the heavy-key path pays only when the heavy keys hold most of
+    // S (every tuple then takes a filter lookup in the count and first scatter
+    // passes); below kHeavyMinShare of the sample it stays off
+    if (threadIdx.x == 0) s_cand = 0;
+    __syncthreads();
+    {
+        unsigned c = 0;
+        for (int i = threadIdx.x; i < kSampleSlots; i += blockDim.x) c += sc[i] >= T ? sc[i] : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if ((threadIdx.x & 31) == 0 && c) atomicAdd(&s_cand, c);
+    }
+    __syncthreads();
+    if (J.heavy_auto && (double)s_cand < kHeavyMinShare * (double)m) T = 0xffffffffu;
     for (int i = threadIdx.x; i < kSampleSlots; i += blockDim.x) {
         const uint32_t key = sk[i];
         if (!key || sc[i] < T || atomicAdd(&s_n, 1u) >= (unsigned)kHeavyMax) continue;
@@ -183,13 +232,15 @@ __global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P) {
     // partitions (the first scatter pass joins them on the fly)
     HeavyTab *hv = P.join[R.join].heavy;
     const int hmode = (hv && hv->n) ? ((r & 1u) ? 2 : 1) : 0;  // 1: R, 2: S
+    HeavySmem &HS = *reinterpret_cast<HeavySmem *>(sh + F);
+    if (hmode) heavy_smem_load(HS, hv);
     __syncthreads();
     const uint32_t b = c * R.chunk;
     const uint32_t e = min(R.n, b + R.chunk);
     auto count = [&](uint32_t key, uint32_t pay) {
         if (!key) return;
         if (hmode) {
-            const int hs = heavy_find(hv, key);
+            const int hs = heavy_find(HS, key);
             if (hs >= 0) {
                 if (hmode == 2) return;
                 if (atomicCAS(&hv->found[hs], 0u, 1u) == 0u) hv->pay[hs] = pay;
@@ -324,12 +375,18 @@ __global__ void __launch_bounds__(1024) k_basescan(PlanDev P) {
 struct __align__(128) TileSmem {
     Tuple inbuf[2][kTile];     // bulk-copy double buffer of input tiles
     Tuple stage[kTile + 256];  // tile sorted by bucket (+1 spare slot per bucket with bulk stores)
-    uint8_t bkt[kTile];        // bucket of each stage slot (element stores)
+    union {                    // one write-out per call, so the two sets share memory
+        struct {
+            uint8_t bkt[kTile];    // element stores: bucket of each stage slot
+            uint32_t wpos[256];    // element stores: global position of stage slot j is wpos[b] + j
+        };
+        struct {
+            uint32_t len[256];     // bulk stores: the bucket's tuples in this tile
+            uint32_t gpos[256];    // bulk stores: global position of the bucket's first tuple
+        };
+    };
     uint32_t cnt[256];
     uint32_t off[256];         // stage slot of the bucket's first tuple in this tile
-    uint32_t wpos[256];        // element stores: global position of stage slot j is wpos[b] + j
-    uint32_t len[256];         // bulk stores: the bucket's tuples in this tile
-    uint32_t gpos[256];        // bulk stores: global position of the bucket's first tuple
     uint32_t cursor[256];
     uint64_t bar[2];
     uint32_t valid;
@@ -339,10 +396,14 @@ struct __align__(128) TileSmem {
     uint32_t hoff, hlen, hpos; // the tile's heavy pairs: stage slot, count, output position
 };
 
+// Two scatter CTAs fit one SM's 228 KiB of shared memory (1 KiB of it reserved
+// per CTA), with the heavy table's copy as well.
+static_assert(2 * (sizeof(TileSmem) + sizeof(HeavySmem) + 1024) <= 228 * 1024, "two scatter CTAs per SM");
+
 // Where heavy-key S tuples go in the first scatter pass over S: their pairs are
 // appended to the join's output (positions reserved per tile with one atomic).
 struct HeavyOut {
-    const HeavyTab *hv;
+    const HeavySmem *hs;
     uint2 *out;
     uint32_t cap;
     JoinCtr *ctr;
@@ -352,8 +413,8 @@ struct HeavyOut {
 // The output value of heavy-key S tuple t (slot hs): its pair, the tuple itself
 // when unmatched and kept, or nothing (false).
 __device__ __forceinline__ bool heavy_value(const HeavyOut &h, int hs, Tuple &t) {
-    if (__ldg(&h.hv->found[hs])) {
-        t.key = __ldg(&h.hv->pay[hs]);
+    if ((h.hs->found[hs >> 5] >> (hs & 31)) & 1u) {
+        t.key = h.hs->pay[hs];
         return true;
     }
     return h.keep_unmatched != 0;
@@ -408,7 +469,7 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
         if ((head && (b & 1u)) || (!head && (e & 1u) && !((b & 1u) && e - 1 == b))) {
             Tuple t = in[idx];
             int hs = -1;
-            if (kHeavy && t.key) hs = heavy_find(hvo->hv, t.key);
+            if (kHeavy && t.key) hs = heavy_find(*hvo->hs, t.key);
             if (hs >= 0) {
                 if (heavy_value(*hvo, hs, t)) {
                     const uint32_t pos = (uint32_t)atomicAdd(&hvo->ctr->out_reserved, 1ull);
@@ -463,7 +524,7 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
             const uint32_t idx = threadIdx.x + k * kScatterThreads;
             v[k] = idx < nt ? S.inbuf[buf][idx] : Tuple{0u, 0u};
             if (kHeavy) {  // heavy key: rank among the tile's heavy pairs (one counter add per warp)
-                int hs = v[k].key ? heavy_find(hvo->hv, v[k].key) : -1;
+                int hs = v[k].key ? heavy_find(*hvo->hs, v[k].key) : -1;
                 const bool isH = hs >= 0;
                 const bool emit = isH && heavy_value(*hvo, hs, v[k]);
                 const unsigned hm = __ballot_sync(0xffffffffu, emit);
@@ -626,6 +687,14 @@ __device__ __forceinline__ void tile_init(TileSmem &S) {
 
 // Pass 1: one CTA per chunk. Coarse bucket P = p >> b2; the write cursor of
 // (chunk c, bucket P) is base[P << b2] + sum_q off[c][(P << b2) + q].
+// Pass 1: one CTA per chunk. Coarse bucket P = p >> b2; the write cursor of
+// (chunk c, bucket P) is base[P << b2] + sum_q off[c][(P << b2) + q].
+// kHeavyJoins = false covers the joins without heavy keys this execution, true
+// (launched only for plans that sample heavy keys) the joins with them, whose S
+// chunks join their heavy-key tuples on the fly; so the kernel of the common
+// case carries none of the heavy-key code, and a join's R and S chunks still
+// run in one launch.
+template <bool kHeavyJoins>
 __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatter1(PlanDev P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
@@ -633,6 +702,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
     const uint32_t c = blockIdx.x - P.chunk_prefix[r];
     const RelDev R = P.rel[r];
     const JoinDev &J = P.join[R.join];
+    if ((J.heavy && J.heavy->n) != kHeavyJoins) return;
     const int bits = J.bits, b2 = J.fine_bits;
     const uint32_t F = 1u << bits, mask = F - 1;
     const int nb = 1 << (bits - b2);
@@ -647,19 +717,21 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
         for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         if (lane == 0) S.cursor[b] = R.base[b << b2] + sum;
     }
+    const bool heavy = kHeavyJoins && (r & 1u);  // the S of a join with heavy keys
+    HeavySmem &HS = *reinterpret_cast<HeavySmem *>(smem_raw + sizeof(TileSmem));
+    if (heavy) heavy_smem_load(HS, J.heavy);
     __syncthreads();
     const uint32_t b0 = c * R.chunk;
     const uint32_t e0 = min(R.n, b0 + R.chunk);
     Tuple *dst = b2 ? R.tmp : R.out;
     uint32_t uses[2] = {0, 0};
     auto coarse = [=](uint32_t key) { return (int)((glb_partition_hash(key) & mask) >> b2); };
-    const bool heavy = (r & 1u) && J.heavy && J.heavy->n;  // S of a join with heavy keys
     if (heavy) {
-        const HeavyOut hvo{J.heavy, reinterpret_cast<uint2 *>(J.out), (uint32_t)J.out_cap, J.ctr, J.keep_unmatched};
+        const HeavyOut hvo{&HS, reinterpret_cast<uint2 *>(J.out), (uint32_t)J.out_cap, J.ctr, J.keep_unmatched};
         if (nb <= kBulkMaxBuckets)
-            scatter_range<false, true, true>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo);
+            scatter_range<false, true, kHeavyJoins>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo);
         else
-            scatter_range<false, false, true>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo);
+            scatter_range<false, false, kHeavyJoins>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo);
     } else if (nb <= kBulkMaxBuckets) {
         scatter_range<false, true>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error);
     } else {
@@ -1719,12 +1791,14 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
         // heavy keys are sampled when R is partitioned; executions that keep R's
         // partitions keep its heavy table too
         if (P.any_heavy && !keep_r) k_heavy_sample<<<J, 1024, (size_t)kSampleSlots * 8, st>>>(P);
-        k_hist<<<P.total_chunks, kHistThreads, (size_t)4 << P.max_bits, st>>>(P);
+        k_hist<<<P.total_chunks, kHistThreads, ((size_t)4 << P.max_bits) + sizeof(HeavySmem), st>>>(P);
         mark(1);
         k_colscan<<<(P.total_parts + 255) / 256, 256, 0, st>>>(P);
         k_basescan<<<P.nrel, 1024, 0, st>>>(P);
         mark(2);
-        k_scatter1<<<P.total_chunks, kScatterThreads, sizeof(TileSmem), st>>>(P);
+        k_scatter1<false><<<P.total_chunks, kScatterThreads, sizeof(TileSmem), st>>>(P);
+        if (P.any_heavy)
+            k_scatter1<true><<<P.total_chunks, kScatterThreads, sizeof(TileSmem) + sizeof(HeavySmem), st>>>(P);
         if (P.any_two_pass) {
             if (P.total_coarse) k_items<<<(P.total_coarse + 7) / 8, 256, 0, st>>>(P);
             k_scatter2<<<pl->num_sms * kScatterBlocksPerSM, kScatterThreads, sizeof(TileSmem), st>>>(P);
@@ -1758,7 +1832,8 @@ cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm)
     int dev = 0, max_smem = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (1 << kMaxRadixBits) * 4);
+    e = cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (1 << kMaxRadixBits) * 4 + (int)sizeof(HeavySmem));
     if (e) return e;
     // the largest table any plan may use, so plans of different sizes coexist
     for (const void *k : {(const void *)k_join_phj, (const void *)k_join_smj, (const void *)k_join_nl}) {
@@ -1770,11 +1845,14 @@ cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm)
     }
     e = cudaFuncSetAttribute(k_heavy_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, kSampleSlots * 8);
     if (e) return e;
-    e = cudaFuncSetAttribute(k_scatter1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));
+    e = cudaFuncSetAttribute(k_scatter1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));
+    if (e) return e;
+    e = cudaFuncSetAttribute(k_scatter1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(TileSmem) + sizeof(HeavySmem)));
     if (e) return e;
     e = cudaFuncSetAttribute(k_scatter2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem));
     if (e) return e;
-    for (const void *k : {(const void *)k_scatter1, (const void *)k_scatter2, (const void *)k_join_phj,
+    for (const void *k : {(const void *)k_scatter1<false>, (const void *)k_scatter1<true>, (const void *)k_scatter2, (const void *)k_join_phj,
                           (const void *)k_join_smj, (const void *)k_join_nl, (const void *)k_nphj_probe,
                           (const void *)k_hist})
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,

@@ -175,15 +175,18 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     sh.out_chunk = oc;
     // Heavy keys joined on the fly: S keys frequent in a sample of S are joined
     // during the first scatter pass (their R payloads found by the count pass
-    // over R) and never partitioned. On by default for the adaptive skew mode
-    // when S has at least 2^20 tuples; heavy_sample > 0 sets the sample size
-    // (also in the fixed mode), -1 turns it off.
+    // over R) and never partitioned. Automatic for the adaptive skew mode when S
+    // has at least 2^20 tuples: kept only when the heavy keys hold most of the
+    // sample; heavy_sample > 0 sets the sample size and keeps whatever heavy
+    // keys it finds (in either skew mode); -1 turns the path off.
     if (d.join_alg != SPJ_ALG_NPHJ && d.heavy_sample >= 0 && n_s > 0) {
         int64_t hs = 0;
-        if (d.heavy_sample > 0)
+        if (d.heavy_sample > 0) {
             hs = d.heavy_sample;
-        else if (d.skew_mode == SPJ_SKEW_ADAPTIVE && n_s >= (1 << 20))
+        } else if (d.skew_mode == SPJ_SKEW_ADAPTIVE && n_s >= (1 << 20)) {
             hs = kHeavySampleDefault;
+            sh.heavy_auto = 1;
+        }
         sh.heavy_sample = (uint32_t)std::min<int64_t>(std::min<int64_t>(hs, kHeavySampleMax), n_s);
     }
     sh.unit_tuples = d.unit_tuples > 0                ? (uint32_t)d.unit_tuples
@@ -274,6 +277,7 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
         const size_t o_gt = take(nphj ? jd.gtable_slots * 8 : 0);
         const size_t o_hv = take(sh.heavy_sample ? sizeof(HeavyTab) : 0);
         jd.heavy_sample = sh.heavy_sample;
+        jd.heavy_auto = sh.heavy_auto;
         if (a) {
             jd.ctr = (JoinCtr *)(a + o_ctr + sizeof(BatchCtr)) + j;
             jd.holes = (Hole *)(a + o_holes);

@@ -1,7 +1,6 @@
 """GPU tests of the multi-GPU join's pieces that one GPU can run: the device
 split by destination rank (spj_exchange_split) against the oracle's hash, and
 DistributedJoin end to end on a one-rank NCCL group."""
-import socket
 
 import numpy as np
 import pytest
@@ -45,10 +44,8 @@ def test_distributed_join_heavy_keys_one_rank(spj, oracle, fused):
     # replicated through the all-gather) runs even with one rank
     import torch
     import torch.distributed as dist
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        port = s.getsockname()[1]
-    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+    # one rank: an in-process store, no TCP rendezvous (a freed port can be taken again)
+    dist.init_process_group("nccl", store=dist.HashStore(), rank=0, world_size=1,
                             device_id=torch.device("cuda", 0))
     try:
         n_r, n_s = 1 << 17, 1 << 20
@@ -67,10 +64,8 @@ def test_distributed_join_heavy_keys_one_rank(spj, oracle, fused):
 def test_distributed_join_one_rank(spj, oracle):
     import torch
     import torch.distributed as dist
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        port = s.getsockname()[1]
-    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    # one rank: an in-process store, no TCP rendezvous (a freed port can be taken again)
+    dist.init_process_group("nccl", store=dist.HashStore(), rank=0, world_size=1)
     try:
         n_r, n_s = 1 << 18, 1 << 20
         R, S, expect = spj.generate_host(n_r, n_s, 1.0, seed=9)
@@ -127,10 +122,8 @@ def test_fused_scatter_into_several_receive_buffers(spj, oracle):
 def test_distributed_join_fused_one_rank(spj, oracle):
     import torch
     import torch.distributed as dist
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        port = s.getsockname()[1]
-    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+    # one rank: an in-process store, no TCP rendezvous (a freed port can be taken again)
+    dist.init_process_group("nccl", store=dist.HashStore(), rank=0, world_size=1,
                             device_id=torch.device("cuda", 0))
     try:
         n_r, n_s = 1 << 18, 1 << 20

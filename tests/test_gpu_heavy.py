@@ -27,7 +27,7 @@ def test_heavy_keys_zipf_1_5_exact_and_counted(spj, oracle, alg):
 
 def test_heavy_path_off_gives_the_same_pairs(spj, oracle):
     R, S, expect = spj.generate_host(1 << 17, 1 << 20, 1.0, seed=78)
-    on, lon = run_instance(spj, R, S)
+    on, lon = run_instance(spj, R, S, heavy_sample=1 << 16)
     off, loff = run_instance(spj, R, S, heavy_sample=-1)
     assert loff["heavy_keys"] == 0 and loff["heavy_tuples"] == 0 and lon["heavy_keys"] > 0
     assert same_multiset(oracle, on.pairs(), off.pairs())
@@ -46,7 +46,7 @@ def test_heavy_keys_without_r_match(spj, oracle, alg):
     keys[u < 0.35] = 7                            # in R
     keys[(u >= 0.35) & (u < 0.6)] = 3 * n_r + 5   # not in R
     S = np.stack([keys, np.arange(n_s)], 1).astype(np.uint32)
-    res, logs = run_instance(spj, R, S, join_alg=alg)
+    res, logs = run_instance(spj, R, S, join_alg=alg, heavy_sample=1 << 16)
     want = oracle.simple_join(R, S, keep_unmatched=alg in (2, 3))
     assert same_multiset(oracle, res.pairs(), want)
     assert logs["heavy_keys"] >= 2
@@ -62,17 +62,30 @@ def test_heavy_key_repeated_in_r(spj, oracle):
     keys = rng.integers(1, n_r + 1, n_s)
     keys[rng.random(n_s) < 0.5] = 11
     S = np.stack([keys, np.arange(n_s)], 1).astype(np.uint32)
-    out = run_instance(spj, R, S)[0].pairs()
+    res, logs = run_instance(spj, R, S, heavy_sample=1 << 16)
+    out = res.pairs()
+    assert logs["heavy_keys"] >= 1
     assert out.shape[0] == n_s
     assert np.array_equal(np.sort(out[:, 1]), np.arange(n_s, dtype=np.uint32))
     assert np.array_equal(R[out[:, 0], 0], S[out[:, 1], 0])
+
+
+def test_automatic_mode_keeps_heavy_keys_only_under_strong_skew(spj):
+    """The planner's sample keeps its heavy keys only when they hold most of S:
+    on for Zipf 1.5, off for Zipf 1.0 (where a filter lookup per tuple would
+    cost more than the partitioning it saves) and for uniform keys."""
+    for zipf, on in ((1.5, True), (1.0, False), (0.0, False)):
+        R, S, expect = spj.generate_host(1 << 20, 1 << 22, zipf, seed=80)
+        res, logs = run_instance(spj, R, S)
+        assert (logs["heavy_keys"] > 0) == on, zipf
 
 
 def test_heavy_keys_in_a_batch(spj, oracle):
     import torch
     specs = [(1 << 16, 1 << 20, 1.5), (1 << 12, 1 << 20, 1.2), (1 << 18, 1 << 18, 1.0), (5000, 1 << 21, 0.0)]
     data = [spj.generate_host(a, b, z, seed=90 + i) for i, (a, b, z) in enumerate(specs)]
-    batch = spj.Batch([a for a, _, _ in specs], [b for _, b, _ in specs], spj.make_design(rank_num=1))
+    batch = spj.Batch([a for a, _, _ in specs], [b for _, b, _ in specs],
+                      spj.make_design(rank_num=1, heavy_sample=1 << 16))
     dR = [torch.from_numpy(R.view(np.int32)).cuda() for R, _, _ in data]
     dS = [torch.from_numpy(S.view(np.int32)).cuda() for _, S, _ in data]
     outs = [torch.empty((batch.output_capacity(j), 2), dtype=torch.int32, device="cuda") for j in range(len(specs))]
