@@ -63,7 +63,7 @@ def samples_heavy(args, n_s):
     """Whether the plan samples heavy keys for this join (the planner's rule)."""
     if args.alg == 1 or args.heavy < 0:
         return False
-    return args.heavy > 0 or (args.skew == 0 and n_s >= (1 << 20))
+    return args.heavy > 0 or (args.skew == 0 and n_s >= (1 << 24))
 
 
 def peaks():

@@ -79,7 +79,8 @@ typedef struct {
     int unit_tuples;    /* max S tuples per work unit in adaptive mode */
     int heavy_sample;   /* S keys sampled to find heavy keys, which the first scatter pass joins
                            on the fly (at most 256 per join; their S tuples skip the
-                           partitioning): 0 = 16384 in the adaptive skew mode when |S| >= 2^20,
+                           partitioning): 0 = 16384 in the adaptive skew mode when |S| >= 2^24
+                           (2^20 for a join in a batch),
                            kept only when the heavy keys hold at least 60% of the sample (below
                            that the per-tuple filter lookups cost more than they save), else
                            off; > 0 = that many, kept whatever their share (any skew mode);

@@ -1277,6 +1277,172 @@ __device__ __forceinline__ void warp0_scan1024(const uint32_t *cnt, uint32_t *of
     if (lane == 0) off[n] = carry;
 }
 
+// ------------------------------------------------------------ sorted runs --
+// The sort-merge join sorts every R partition once, before any work unit runs
+// (mpsm_join_sort_probe.c:152-236 sorts each DPU's buckets once too), instead of
+// once per unit: a hot partition split into hundreds of units was sorted
+// hundreds of times. A partition of one unit is still sorted by that unit (a
+// separate pass would only add a store and a load of its tuples). Runs of at
+// most `cap` tuples (the largest power of two of the CTA's shared-memory budget)
+// are sorted in place by (key, payload); a partition that fits is one run and is
+// searched in shared memory, a larger one (many repeats of a key) is searched
+// run by run in global memory. The nested-loop join, which sub-partitions its R
+// partition in shared memory, takes the same run search for the partitions that
+// do not fit.
+__device__ __forceinline__ uint32_t run_cap(const JoinDev &J) {
+    uint32_t cap = 1;
+    while (cap * 2 <= (uint32_t)J.table_slots) cap <<= 1;
+    return cap;
+}
+
+__device__ __forceinline__ unsigned long long pack_kp(const Tuple t) {
+    return ((unsigned long long)t.key << 32) | t.pay;
+}
+
+// Bitonic sort of sorted[0, npad) (npad a power of two) by the whole CTA.
+__device__ __forceinline__ void bitonic_sort_smem(unsigned long long *sorted, uint32_t npad) {
+    for (uint32_t k = 2; k <= npad; k <<= 1) {
+        for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+            for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x) {
+                const uint32_t ixj = i ^ jj;
+                if (ixj > i) {
+                    const unsigned long long a = sorted[i], b = sorted[ixj];
+                    if ((a > b) == ((i & k) == 0)) {
+                        sorted[i] = b;
+                        sorted[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Whether k_sort_runs sorts R partition p of join j: a sort-merge partition
+// with more than one work unit or beyond the shared-memory budget, a nested-loop
+// partition beyond its budget.
+__device__ __forceinline__ bool presorted(const PlanDev &P, uint32_t j, uint32_t p) {
+    const JoinDev &J = P.join[j];
+    const uint32_t nr = P.rel[2 * j].total[p];
+    if (J.alg == SPJ_ALG_NL) return nr > (uint32_t)J.table_slots;
+    if (J.alg != SPJ_ALG_SMJ) return false;
+    if (nr > run_cap(J)) return true;
+    uint32_t ns = 0, s0 = 0;
+    return unit_count_of(P, j, p, ns, s0) > 1;
+}
+
+// Merge sort of a[0, npad) by the whole CTA with b[0, npad) as the second
+// buffer (npad a power of two >= 8): runs of four sorted in registers, then
+// log2(npad / 4) rounds in which every thread writes four outputs of a pair of
+// runs, starting where the merge path (Odeh, Green, Mwassi, Shmueli, Birk,
+// "Merge Path - Parallel Merging Made Simple", IPDPSW 2012) crosses its
+// diagonal. Ten barriers for 4096 keys instead of the bitonic network's 78.
+// Returns the buffer that holds the result.
+__device__ __forceinline__ unsigned long long *merge_sort_smem(unsigned long long *a, unsigned long long *b,
+                                                              uint32_t npad) {
+    constexpr uint32_t E = 4;
+    for (uint32_t g = threadIdx.x; g * E < npad; g += blockDim.x) {
+        unsigned long long v0 = a[g * E], v1 = a[g * E + 1], v2 = a[g * E + 2], v3 = a[g * E + 3], t;
+#define SPJ_CX(x, y) \
+    if (x > y) {     \
+        t = x;       \
+        x = y;       \
+        y = t;       \
+    }
+        SPJ_CX(v0, v1) SPJ_CX(v2, v3) SPJ_CX(v0, v2) SPJ_CX(v1, v3) SPJ_CX(v1, v2)
+#undef SPJ_CX
+        a[g * E] = v0;
+        a[g * E + 1] = v1;
+        a[g * E + 2] = v2;
+        a[g * E + 3] = v3;
+    }
+    __syncthreads();
+    unsigned long long *src = a, *dst = b;
+    for (uint32_t L = E; L < npad; L <<= 1) {
+        for (uint32_t k0 = threadIdx.x * E; k0 < npad; k0 += blockDim.x * E) {
+            const uint32_t base = k0 & ~(2 * L - 1), d = k0 - base;
+            const unsigned long long *A = src + base, *B = A + L;
+            uint32_t lo = d > L ? d - L : 0, hi = min(d, L);
+            while (lo < hi) {  // first i with A[i] > B[d - 1 - i]: ties take A first
+                const uint32_t mid = (lo + hi) >> 1;
+                if (A[mid] <= B[d - 1 - mid])
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            uint32_t i = lo, j = d - lo;
+#pragma unroll
+            for (uint32_t e = 0; e < E; e++) {
+                const bool takeA = j >= L || (i < L && A[i] <= B[j]);
+                dst[k0 + e] = takeA ? A[i++] : B[j++];
+            }
+        }
+        __syncthreads();
+        unsigned long long *t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+// Sorts buf[0, npad) (npad a power of two) by the whole CTA, using up to
+// `room` entries of shared memory from buf; returns where the result is.
+__device__ __forceinline__ unsigned long long *sort_smem(unsigned long long *buf, uint32_t npad, uint32_t room) {
+    if (npad >= 8 && 2 * npad <= room) return merge_sort_smem(buf, buf + npad, npad);
+    bitonic_sort_smem(buf, npad);
+    return buf;
+}
+
+// One CTA per flat partition: the partitions `presorted` names, sorted in runs
+// of run_cap tuples.
+__global__ void __launch_bounds__(kJoinThreads, 2) k_sort_runs(PlanDev P) {
+    extern __shared__ unsigned long long sorted[];
+    const uint32_t t = blockIdx.x;
+    const uint32_t j = find_slot(P.jpart_prefix, P.njoin, t);
+    const uint32_t p = t - P.jpart_prefix[j];
+    const JoinDev &J = P.join[j];
+    const RelDev &Rr = P.rel[2 * j];
+    const uint32_t nr = Rr.total[p];
+    if (nr == 0 || P.rel[2 * j + 1].total[p] == 0 || !presorted(P, j, p)) return;  // nothing to sort
+    const uint32_t cap = run_cap(J);
+    Tuple *pr = Rr.out + Rr.base[p];
+    for (uint32_t r0 = 0; r0 < nr; r0 += cap) {
+        const uint32_t len = min(cap, nr - r0);
+        uint32_t npad = 1;
+        while (npad < len) npad <<= 1;
+        for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x) sorted[i] = i < len ? pack_kp(pr[r0 + i]) : ~0ull;
+        __syncthreads();
+        const unsigned long long *res = sort_smem(sorted, npad, (uint32_t)J.table_slots);
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+            const unsigned long long v = res[i];
+            pr[r0 + i] = Tuple{(uint32_t)(v >> 32), (uint32_t)v};
+        }
+        __syncthreads();
+    }
+}
+
+// The first tuple of key `key` in the sorted runs of pr[0, nr) (runs of cap
+// tuples), read from global memory; false if none.
+__device__ __forceinline__ bool search_runs(const Tuple *pr, uint32_t nr, uint32_t cap, uint32_t key, uint32_t &rp) {
+    const unsigned long long target = (unsigned long long)key << 32;
+    for (uint32_t r0 = 0; r0 < nr; r0 += cap) {
+        uint32_t lo = r0, hi = min(nr, r0 + cap);
+        const uint32_t end = hi;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (pack_kp(pr[mid]) < target)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        if (lo < end && pr[lo].key == key) {
+            rp = pr[lo].pay;
+            return true;
+        }
+    }
+    return false;
+}
+
 // ---------------------------------------------------------- nested-loop join --
 // nested_loop_join.c:184-231 on B200. The R partition is counting-sorted in
 // shared memory into L <= 1024 sub-partitions (hash bits above the partition
@@ -1296,6 +1462,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
     WarpOut w{0u, 0u};
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0, lmask = 0;
+    bool in_smem = true;
+    const Tuple *pr_g = nullptr;
     Unit un;
     unit_claim_first(P, &s_next);
     while (unit_claim_next(P, n_units, &s_next, un)) {
@@ -1306,8 +1474,14 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
             cur_p = un.p;
             const RelDev &Rr = P.rel[2 * un.join];
             const uint32_t cap = J.table_slots;  // R tuples that fit
-            nr = min(Rr.total[un.p], cap);
-            if (threadIdx.x == 0 && Rr.total[un.p] > cap) atomicOr(&J.ctr->error, 1u);
+            nr = Rr.total[un.p];
+            pr_g = Rr.out + Rr.base[un.p];
+            in_smem = nr <= cap;  // else: sorted runs, searched in global memory
+            if (!in_smem) {
+                __syncthreads();
+                unit_prefetch_next_r(P, n_units, &s_next, un);
+                goto probe;
+            }
             uint32_t L = 1;
             while (L < 1024 && L * 16 < nr) L <<= 1;
             lmask = L - 1;
@@ -1331,7 +1505,20 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
             __syncthreads();  // the next unit's index is written
         }
         unit_prefetch_next_r(P, n_units, &s_next, un);
+    probe:
         const Tuple *ps = P.rel[2 * un.join + 1].out;
+        if (!in_smem) {  // an R partition beyond the shared-memory budget: its sorted runs
+            const uint32_t rcap = run_cap(J);
+            for (uint32_t base = un.s_begin + warp * 32; base < un.s_end; base += nwarps * 32) {
+                const uint32_t idx = base + lane;
+                const Tuple t = idx < un.s_end ? ps[idx] : Tuple{0u, 0u};
+                uint32_t rp = 0;
+                const bool hit = t.key != 0 && search_runs(pr_g, nr, rcap, t.key, rp);
+                warp_emit(o, w, t.key != 0, hit ? rp : t.key, t.pay);
+            }
+            __syncthreads();
+            continue;
+        }
         constexpr int U = 4;
         for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
             Tuple t[U];
@@ -1365,81 +1552,79 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
 }
 
 // ----------------------------------------------------------- sort-merge join --
-// mpsm_join_sort_probe.c:152-236 on B200. The R partition is bitonic-sorted by
-// key in shared memory, and every S tuple finds its key in the sorted run by a
-// lower-bound search (the merge step of the reference, done per tuple: the
-// output is a multiset, so S need not be sorted first -- sorting each warp's 32
-// S tuples with a shuffle network cost 30% of the join). A matched S tuple
-// becomes (R.payload, S.payload), an unmatched one stays as it is (S is
-// rewritten in place).
+// mpsm_join_sort_probe.c:152-236 on B200. The R partition, sorted once by
+// k_sort_runs, is copied into shared memory, and every S tuple finds its key in
+// it by a lower-bound search (the merge step of the reference, done per tuple:
+// the output is a multiset, so S need not be sorted first -- sorting each warp's
+// 32 S tuples with a shuffle network cost 30% of the join). A partition larger
+// than the shared-memory budget is searched run by run in global memory. A
+// matched S tuple becomes (R.payload, S.payload), an unmatched one stays as it
+// is (S is rewritten in place).
 __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
     extern __shared__ unsigned long long sorted[];
-    __shared__ unsigned s_slot;
+    __shared__ unsigned s_next;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
     const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
     WarpOut w{0u, 0u};
     OutCtx o{};
-    uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0;
+    uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0, cap = 1;
+    bool in_smem = true;
+    const Tuple *pr = nullptr;
+    const unsigned long long *keys = sorted;  // the sorted partition in shared memory
     Unit un;
-    // (no one-ahead claim: the sort, not the load, bounds this build)
-    while (next_unit(P, n_units, &s_slot, un)) {
+    unit_claim_first(P, &s_next);
+    while (unit_claim_next(P, n_units, &s_next, un)) {
         const JoinDev &J = P.join[un.join];
         if (un.join != cur_j || un.p != cur_p) {
             switch_join(P, un.join, cur_j, o, w);
             cur_p = un.p;
-            uint32_t cap = 1;  // largest power of two that fits the shared-memory budget
-            while (cap * 2 <= (uint32_t)J.table_slots) cap <<= 1;
+            cap = run_cap(J);
             const RelDev &Rr = P.rel[2 * un.join];
-            nr = min(Rr.total[un.p], cap);
-            if (threadIdx.x == 0 && Rr.total[un.p] > cap) atomicOr(&J.ctr->error, 1u);
-            uint32_t npad = 1;
-            while (npad < nr) npad <<= 1;
-            const Tuple *pr = Rr.out + Rr.base[un.p];
-            for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x)
-                sorted[i] = i < nr ? ((unsigned long long)pr[i].key << 32) | pr[i].pay : ~0ull;
-            __syncthreads();
-            for (uint32_t k = 2; k <= npad; k <<= 1) {
-                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
-                    for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x) {
-                        const uint32_t ixj = i ^ jj;
-                        if (ixj > i) {
-                            const unsigned long long a = sorted[i], b = sorted[ixj];
-                            if ((a > b) == ((i & k) == 0)) {
-                                sorted[i] = b;
-                                sorted[ixj] = a;
-                            }
-                        }
-                    }
-                    __syncthreads();
-                }
+            nr = Rr.total[un.p];
+            pr = Rr.out + Rr.base[un.p];
+            in_smem = nr <= cap;
+            keys = sorted;
+            if (in_smem && presorted(P, un.join, un.p)) {  // sorted once for all its units
+                for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) sorted[i] = pack_kp(pr[i]);
+            } else if (in_smem) {  // its only unit sorts it
+                uint32_t npad = 1;
+                while (npad < nr) npad <<= 1;
+                for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x) sorted[i] = i < nr ? pack_kp(pr[i]) : ~0ull;
+                __syncthreads();
+                keys = sort_smem(sorted, npad, (uint32_t)J.table_slots);
             }
         }
+        __syncthreads();  // the copy is complete and the next unit's index is written
+        unit_prefetch_next_r(P, n_units, &s_next, un);
         const Tuple *ps = P.rel[2 * un.join + 1].out;
         for (uint32_t base = un.s_begin + warp * 32; base < un.s_end; base += nwarps * 32) {
             const uint32_t idx = base + lane;
             const bool in = idx < un.s_end;
             Tuple t = in ? ps[idx] : Tuple{0u, 0u};
             const bool valid = in && t.key != 0;
-            const bool mine = valid;
             bool hit = false;
             uint32_t rp = 0;
-            if (mine && nr) {
-                const unsigned long long target = (unsigned long long)t.key << 32;
-                uint32_t lo = 0, hi = nr;
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (sorted[mid] < target)
-                        lo = mid + 1;
-                    else
-                        hi = mid;
-                }
-                if (lo < nr && (uint32_t)(sorted[lo] >> 32) == t.key) {
-                    hit = true;
-                    rp = (uint32_t)sorted[lo];
+            if (valid && nr) {
+                if (in_smem) {
+                    const unsigned long long target = (unsigned long long)t.key << 32;
+                    uint32_t lo = 0, hi = nr;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (keys[mid] < target)
+                            lo = mid + 1;
+                        else
+                            hi = mid;
+                    }
+                    if (lo < nr && (uint32_t)(keys[lo] >> 32) == t.key) {
+                        hit = true;
+                        rp = (uint32_t)keys[lo];
+                    }
+                } else {
+                    hit = search_runs(pr, nr, cap, t.key, rp);
                 }
             }
-            warp_emit(o, w, mine, hit ? rp : t.key, t.pay);
+            warp_emit(o, w, valid, hit ? rp : t.key, t.pay);
         }
         __syncthreads();
     }
@@ -1803,6 +1988,10 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
             if (P.total_coarse) k_items<<<(P.total_coarse + 7) / 8, 256, 0, st>>>(P);
             k_scatter2<<<pl->num_sms * kScatterBlocksPerSM, kScatterThreads, sizeof(TileSmem), st>>>(P);
         }
+        // R partitions searched by several sort-merge units (or too large for a
+        // CTA) sorted once; also on executions that keep R's partitions, whose
+        // units can differ from the previous execution's (sorting is idempotent)
+        if (P.alg == SPJ_ALG_SMJ || P.alg == SPJ_ALG_NL) k_sort_runs<<<P.total_jparts, kJoinThreads, jsm, st>>>(P);
         mark(3);
         k_units_count<<<(P.total_jparts + 255) / 256, 256, 0, st>>>(P);
         k_units_scan<<<1, 1024, 0, st>>>(P);
@@ -1836,7 +2025,8 @@ cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm)
                              (1 << kMaxRadixBits) * 4 + (int)sizeof(HeavySmem));
     if (e) return e;
     // the largest table any plan may use, so plans of different sizes coexist
-    for (const void *k : {(const void *)k_join_phj, (const void *)k_join_smj, (const void *)k_join_nl}) {
+    for (const void *k : {(const void *)k_join_phj, (const void *)k_join_smj, (const void *)k_join_nl,
+                          (const void *)k_sort_runs}) {
         cudaFuncAttributes fa;
         if ((e = cudaFuncGetAttributes(&fa, k))) return e;
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,

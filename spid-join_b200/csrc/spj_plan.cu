@@ -141,10 +141,15 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
             sh.bits = std::min(std::max(std::max(std::max(need, par), minb) + delta, 1), kMaxRadixBits);
         }
         if (d.table_slots <= 0 && !tuned_ts) {
-            // shrink the table to three times a generous bound on the largest partition
+            // shrink the table to three times a generous bound on the largest
+            // partition (the hash table at a load of 1/3); the sort-merge join
+            // wants twice the bound's power of two (its merge sort's two buffers)
             const double mean = (double)n_r / (double)(1ull << sh.bits);
             const double bound = mean + 6.0 * sqrt(mean) + 32.0;
-            const int want = (int)std::min<double>(max_slots, std::max(1024.0, 3.0 * bound));
+            double pow2 = 1.0;
+            while (pow2 < bound) pow2 *= 2.0;
+            const double sized = d.join_alg == SPJ_ALG_SMJ ? 2.0 * pow2 : 3.0 * bound;
+            const int want = (int)std::min<double>(max_slots, std::max(1024.0, sized));
             ts = std::min(ts, (want + 255) / 256 * 256);
             ts = std::max(ts, 1024);
         }
@@ -176,14 +181,16 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     // Heavy keys joined on the fly: S keys frequent in a sample of S are joined
     // during the first scatter pass (their R payloads found by the count pass
     // over R) and never partitioned. Automatic for the adaptive skew mode when S
-    // has at least 2^20 tuples: kept only when the heavy keys hold most of the
-    // sample; heavy_sample > 0 sets the sample size and keeps whatever heavy
-    // keys it finds (in either skew mode); -1 turns the path off.
+    // has at least 2^24 tuples (2^20 in a batch, whose joins are sampled by one
+    // launch; a join's own sampling launch costs about as much as the path saves
+    // below that): kept only when the heavy keys hold most of the sample;
+    // heavy_sample > 0 sets the sample size and keeps whatever heavy keys it
+    // finds (in either skew mode); -1 turns the path off.
     if (d.join_alg != SPJ_ALG_NPHJ && d.heavy_sample >= 0 && n_s > 0) {
         int64_t hs = 0;
         if (d.heavy_sample > 0) {
             hs = d.heavy_sample;
-        } else if (d.skew_mode == SPJ_SKEW_ADAPTIVE && n_s >= (1 << 20)) {
+        } else if (d.skew_mode == SPJ_SKEW_ADAPTIVE && n_s >= (alone ? (1 << 24) : (1 << 20))) {
             hs = kHeavySampleDefault;
             sh.heavy_auto = 1;
         }

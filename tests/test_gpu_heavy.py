@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("alg", [0, 2, 3])
 def test_heavy_keys_zipf_1_5_exact_and_counted(spj, oracle, alg):
     R, S, expect = spj.generate_host(1 << 18, 1 << 20, 1.5, seed=77)
-    res, logs = run_instance(spj, R, S, join_alg=alg)
+    res, logs = run_instance(spj, R, S, join_alg=alg, heavy_sample=1 << 14)
     out = res.pairs()
     assert out.shape[0] == S.shape[0] and oracle.checksum(out) == expect
     assert same_multiset(oracle, out, oracle.simple_join(R, S))
@@ -75,7 +75,7 @@ def test_automatic_mode_keeps_heavy_keys_only_under_strong_skew(spj):
     on for Zipf 1.5, off for Zipf 1.0 (where a filter lookup per tuple would
     cost more than the partitioning it saves) and for uniform keys."""
     for zipf, on in ((1.5, True), (1.0, False), (0.0, False)):
-        R, S, expect = spj.generate_host(1 << 20, 1 << 22, zipf, seed=80)
+        R, S, expect = spj.generate_host(1 << 20, 1 << 24, zipf, seed=80)
         res, logs = run_instance(spj, R, S)
         assert (logs["heavy_keys"] > 0) == on, zipf
 
@@ -108,7 +108,7 @@ def test_heavy_keys_with_host_slices(spj, oracle):
     """|S| >= 2^24 in host memory: S is joined in slices that reuse R's
     partitions and the heavy table of the first slice."""
     R, S, expect = spj.generate_host(1 << 20, 1 << 25, 1.5, seed=95)
-    res, logs = run_instance(spj, R, S)
+    res, logs = run_instance(spj, R, S, heavy_sample=1 << 14)
     out = res.pairs()
     assert out.shape[0] == S.shape[0] and oracle.checksum(out) == expect
     assert logs["heavy_keys"] > 0
