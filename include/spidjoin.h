@@ -195,16 +195,21 @@ void spj_plan_destroy(spj_plan_t *plan);
  * choice. No counterpart in the reference, whose partition counts follow fixed
  * formulas.
  * A class is (floor(log2 |R|), floor(log2(|S| / |R|)) clamped to [0, 6]);
- * radix_bits_delta offsets the planner's fan-out, table_slots and unit_tuples
- * replace its choices when non-zero. The table is filled by the autotuner
- * (spidjoin.autotune, which times candidates per class on the device) and is
- * process-wide; spj_tuning_set replaces it (n = 0 clears it). */
+ * radix_bits_delta offsets the planner's fan-out (and so the pass count: one
+ * scatter pass up to 2^8 partitions, two above), table_slots and unit_tuples
+ * replace its choices when non-zero, and join_alg (spj_join_alg + 1; 0 = the
+ * design's) picks the class's local-join algorithm among those with the
+ * design's output semantics: the hash joins PHJ and NPHJ, or sort-merge and
+ * nested loop. One batch may so mix algorithms. The table is filled by the
+ * autotuner (spidjoin.autotune, which times candidates per class on the device)
+ * and is process-wide; spj_tuning_set replaces it (n = 0 clears it). */
 typedef struct {
     int log2_r, log2_ratio;
     int radix_bits_delta; /* -4..4 */
     int table_slots;      /* 0 = planner */
     int unit_tuples;      /* 0 = planner */
-    int reserved[3];
+    int join_alg;         /* 0 = the design's; else spj_join_alg + 1 */
+    int reserved[2];
 } spj_tuning_t;
 int spj_tuning_set(const spj_tuning_t *entries, int n);
 /* Copies up to `capacity` entries; returns the table's size. */

@@ -125,11 +125,15 @@ struct Unit {
 };
 
 // Batch-wide queues (zeroed per execution).
+// The unit queue holds each local-join algorithm's units in one contiguous
+// range, [alg_begin[a], alg_begin[a + 1]), so every join kernel of a batch whose
+// joins use different algorithms claims only its own.
 struct BatchCtr {
     unsigned int unit_count, unit_next;
     unsigned int item_count, item_next;
     unsigned int error;
-    unsigned int pad[3];
+    unsigned int alg_begin[5];
+    unsigned int alg_next[4];
 };
 
 // Kernel-parameter view of a plan.
@@ -144,7 +148,7 @@ struct PlanDev {
     uint32_t total_chunks, total_parts, total_coarse, total_jparts;
     int max_bits;             // histogram shared memory
     int max_table_slots;      // join-kernel shared memory
-    int alg;                  // one local-join algorithm per batch
+    int alg_mask;             // 1 << spj_join_alg of every algorithm some join uses
     int any_two_pass;
     int any_heavy;            // some join samples heavy keys
     Unit *units;
@@ -172,6 +176,7 @@ struct JoinShape {
     unsigned long long gtable_slots = 0;
     uint32_t heavy_sample = 0;  // 0: no heavy-key path
     int heavy_auto = 0;
+    int alg = SPJ_ALG_PHJ;      // the join's local-join algorithm
 };
 
 }  // namespace spj
@@ -218,7 +223,9 @@ cudaError_t init_single(spj_plan *pl, cudaStream_t st, bool keep_r = false);
 // spj_plan_execute with keep_r (see launch_pipeline).
 int plan_execute(spj_plan *pl, const spj_kv_pair_t *r, const spj_kv_pair_t *s, spj_kv_pair_t *out, int64_t *n_out,
                  cudaStream_t st, bool keep_r);
-cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm);
+// alg_mask: 1 << spj_join_alg of each algorithm the plan's joins use; the CTAs
+// per SM that every one of those join kernels can keep resident.
+cudaError_t configure_kernels(int table_slots, int alg_mask, int *join_blocks_per_sm);
 int create_plan_stream(int J, const int64_t *n_r, const int64_t *n_s, const spj_design_t *design,
                        const spj_kv_pair_t *const *r, const spj_kv_pair_t *const *s, spj_kv_pair_t *const *out,
                        int64_t *const *n_out, cudaMemPool_t pool, cudaStream_t st, spj_plan_t **pout,

@@ -897,41 +897,63 @@ __global__ void k_units_count(PlanDev P) {
 }
 
 // Units, step 2: each join's units get a contiguous range of the queue, so a
-// CTA meets every join in one stretch (at most one output hole per warp and join).
+// CTA meets every join in one stretch (at most one output hole per warp and
+// join), and each local-join algorithm's joins come in one stretch of their own
+// (alg_begin), which that algorithm's kernel works through.
 __global__ void __launch_bounds__(1024) k_units_scan(PlanDev P) {
     __shared__ uint32_t warp_sums[32];
+    __shared__ uint32_t s_carry;
     const uint32_t J = P.njoin;
     const uint32_t per = (J + blockDim.x - 1) / blockDim.x;
     const uint32_t beg = threadIdx.x * per, end = min(J, beg + per);
-    uint32_t sum = 0;
-    for (uint32_t j = beg; j < end; j++) sum += P.join[j].ctr->units;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t incl = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += x;
-    }
-    if (lane == 31) warp_sums[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t w = warp_sums[lane];
-        uint32_t wi = w;
+    if (threadIdx.x == 0) s_carry = 0;
+    for (int A = 0; A < 4; A++) {
+        __syncthreads();
+        if (threadIdx.x == 0) P.bctr->alg_begin[A] = s_carry;
+        if (!(P.alg_mask & (1 << A))) continue;  // uniform: no join uses A
+        uint32_t sum = 0;
+        for (uint32_t j = beg; j < end; j++)
+            if (P.join[j].alg == A) sum += P.join[j].ctr->units;
+        uint32_t incl = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t x = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += x;
+            const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += x;
         }
-        warp_sums[lane] = wi - w;
-        if (lane == 31) P.bctr->unit_count = wi;
+        if (lane == 31) warp_sums[warp] = incl;
+        __syncthreads();
+        uint32_t total = 0;
+        if (warp == 0) {
+            const uint32_t w = warp_sums[lane];
+            uint32_t wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += x;
+            }
+            warp_sums[lane] = wi - w;
+            total = __shfl_sync(0xffffffffu, wi, 31);
+        }
+        __syncthreads();
+        uint32_t run = s_carry + warp_sums[warp] + incl - sum;
+        for (uint32_t j = beg; j < end; j++) {
+            if (P.join[j].alg != A) continue;
+            JoinCtr *c = P.join[j].ctr;
+            c->unit_base = run;
+            run += c->units;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += total;
     }
     __syncthreads();
-    uint32_t run = warp_sums[warp] + incl - sum;
+    if (threadIdx.x == 0) {
+        P.bctr->alg_begin[4] = s_carry;
+        P.bctr->unit_count = s_carry;
+    }
     for (uint32_t j = beg; j < end; j++) {
         const JoinDev &J = P.join[j];
         JoinCtr *c = J.ctr;
-        c->unit_base = run;
-        run += c->units;
         // the pairs of heavy keys, appended by the first scatter pass, end on a
         // whole output chunk, so every join chunk is aligned; the rest of their
         // last chunk is a hole for the fix-up
@@ -1146,9 +1168,18 @@ __device__ __forceinline__ bool probe_table(const unsigned long long *table, uin
     return false;
 }
 
-// Fetches the next unit for the CTA; returns false when the queue is empty.
-__device__ __forceinline__ bool next_unit(const PlanDev &P, unsigned n_units, unsigned *s_slot, Unit &un) {
-    if (threadIdx.x == 0) *s_slot = atomicAdd(&P.bctr->unit_next, 1u);
+// The unit range of local-join algorithm A (its units are contiguous in the queue).
+__device__ __forceinline__ unsigned units_end(const PlanDev &P, int A) {
+    return min(*(volatile unsigned *)&P.bctr->alg_begin[A + 1], P.max_units);
+}
+
+__device__ __forceinline__ unsigned claim_unit(const PlanDev &P, int A) {
+    return *(volatile unsigned *)&P.bctr->alg_begin[A] + atomicAdd(&P.bctr->alg_next[A], 1u);
+}
+
+// Fetches the next unit of algorithm A for the CTA; false when its range is done.
+__device__ __forceinline__ bool next_unit(const PlanDev &P, int A, unsigned n_units, unsigned *s_slot, Unit &un) {
+    if (threadIdx.x == 0) *s_slot = claim_unit(P, A);
     __syncthreads();
     const unsigned u = *s_slot;
     __syncthreads();
@@ -1162,17 +1193,18 @@ __device__ __forceinline__ bool next_unit(const PlanDev &P, unsigned n_units, un
 // towards L2, so that unit's build finds its tuples there. unit_claim_first
 // once, then unit_claim_next per unit; unit_prefetch_next_r after a barrier
 // that follows unit_claim_next (the next index is written by thread 0).
-__device__ __forceinline__ void unit_claim_first(const PlanDev &P, unsigned *s_next) {
-    if (threadIdx.x == 0) *s_next = atomicAdd(&P.bctr->unit_next, 1u);
+__device__ __forceinline__ void unit_claim_first(const PlanDev &P, int A, unsigned *s_next) {
+    if (threadIdx.x == 0) *s_next = claim_unit(P, A);
 }
 
-__device__ __forceinline__ bool unit_claim_next(const PlanDev &P, unsigned n_units, unsigned *s_next, Unit &un) {
+__device__ __forceinline__ bool unit_claim_next(const PlanDev &P, int A, unsigned n_units, unsigned *s_next,
+                                                Unit &un) {
     __syncthreads();
     const unsigned u = *s_next;
     __syncthreads();
     if (u >= n_units) return false;
     un = P.units[u];
-    if (threadIdx.x == 0) *s_next = atomicAdd(&P.bctr->unit_next, 1u);
+    if (threadIdx.x == 0) *s_next = claim_unit(P, A);
     return true;
 }
 
@@ -1204,13 +1236,13 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
     __shared__ unsigned s_next;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
-    const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
+    const unsigned n_units = units_end(P, SPJ_ALG_PHJ);
     WarpOut w{0u, 0u};
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu;
     Unit un;
-    unit_claim_first(P, &s_next);
-    while (unit_claim_next(P, n_units, &s_next, un)) {
+    unit_claim_first(P, SPJ_ALG_PHJ, &s_next);
+    while (unit_claim_next(P, SPJ_ALG_PHJ, n_units, &s_next, un)) {
         const JoinDev &J = P.join[un.join];
         if (un.join != cur_j || un.p != cur_p) {
             switch_join(P, un.join, cur_j, o, w);
@@ -1458,15 +1490,15 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
     Tuple *rs = reinterpret_cast<Tuple *>(smem_u64);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
-    const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
+    const unsigned n_units = units_end(P, SPJ_ALG_NL);
     WarpOut w{0u, 0u};
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0, lmask = 0;
     bool in_smem = true;
     const Tuple *pr_g = nullptr;
     Unit un;
-    unit_claim_first(P, &s_next);
-    while (unit_claim_next(P, n_units, &s_next, un)) {
+    unit_claim_first(P, SPJ_ALG_NL, &s_next);
+    while (unit_claim_next(P, SPJ_ALG_NL, n_units, &s_next, un)) {
         const JoinDev &J = P.join[un.join];
         const uint32_t bits = J.bits;
         if (un.join != cur_j || un.p != cur_p) {
@@ -1565,7 +1597,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
     __shared__ unsigned s_next;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
-    const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
+    const unsigned n_units = units_end(P, SPJ_ALG_SMJ);
     WarpOut w{0u, 0u};
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu, cur_p = 0xffffffffu, nr = 0, cap = 1;
@@ -1573,8 +1605,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
     const Tuple *pr = nullptr;
     const unsigned long long *keys = sorted;  // the sorted partition in shared memory
     Unit un;
-    unit_claim_first(P, &s_next);
-    while (unit_claim_next(P, n_units, &s_next, un)) {
+    unit_claim_first(P, SPJ_ALG_SMJ, &s_next);
+    while (unit_claim_next(P, SPJ_ALG_SMJ, n_units, &s_next, un)) {
         const JoinDev &J = P.join[un.join];
         if (un.join != cur_j || un.p != cur_p) {
             switch_join(P, un.join, cur_j, o, w);
@@ -1672,12 +1704,12 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
     __shared__ unsigned s_slot;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
-    const unsigned n_units = min(*(volatile unsigned *)&P.bctr->unit_count, P.max_units);
+    const unsigned n_units = units_end(P, SPJ_ALG_NPHJ);
     WarpOut w{0u, 0u};
     OutCtx o{};
     uint32_t cur_j = 0xffffffffu;
     Unit un;
-    while (next_unit(P, n_units, &s_slot, un)) {
+    while (next_unit(P, SPJ_ALG_NPHJ, n_units, &s_slot, un)) {
         switch_join(P, un.join, cur_j, o, w);
         const JoinDev &J = P.join[un.join];
         const unsigned long long *table = J.gtable;
@@ -1935,13 +1967,16 @@ cudaError_t init_single(spj_plan *pl, cudaStream_t st, bool keep_r) {
     const uint32_t f = 1u << h.dev.bits;
     const uint32_t f1 = h.dev.fine_bits ? 1u << (h.dev.bits - h.dev.fine_bits) : 0u;
     k_init_single<<<1, 32, 0, st>>>(pl->dev, h.rel[0], h.rel[1], h.dev, h.rel[0].nchunks, h.rel[1].nchunks, f, f1,
-                                    keep_r && pl->dev.alg != SPJ_ALG_NPHJ);
+                                    keep_r && h.dev.alg != SPJ_ALG_NPHJ);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
     PlanDev P = pl->dev;
-    if (keep_r && P.alg != SPJ_ALG_NPHJ) {
+    const int M = P.alg_mask;
+    const bool nphj = M & (1 << SPJ_ALG_NPHJ), part = M & ~(1 << SPJ_ALG_NPHJ);
+    keep_r = keep_r && part;  // a non-partitioned join has no partitions to keep
+    if (keep_r) {
         // one-join plan whose R partitions (out, hist offsets, totals) are still in
         // its buffers from its previous execution: count and scatter S only. The
         // base scan still runs over both relations (it rederives R's bases and
@@ -1961,26 +1996,23 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
     const size_t jsm = (size_t)P.max_table_slots * 8;
     const uint32_t J = P.njoin;
     mark(0);
-    if (P.alg == SPJ_ALG_NPHJ) {
-        k_nphj_clear<<<dim3(pl->num_sms * 2, J), 256, 0, st>>>(P);
-        mark(1);
-        mark(2);
-        k_nphj_build<<<dim3(pl->num_sms * 4, J), 256, 0, st>>>(P);
-        mark(3);
-        k_units_count<<<(P.total_jparts + 255) / 256, 256, 0, st>>>(P);
-        k_units_scan<<<1, 1024, 0, st>>>(P);
-        k_units<<<(P.total_jparts * 32 + 255) / 256, 256, 0, st>>>(P);
-        mark(4);
-        k_nphj_probe<<<pl->join_blocks, kJoinThreads, 0, st>>>(P);
-    } else {
+    if (part) {
         // heavy keys are sampled when R is partitioned; executions that keep R's
         // partitions keep its heavy table too
         if (P.any_heavy && !keep_r) k_heavy_sample<<<J, 1024, (size_t)kSampleSlots * 8, st>>>(P);
         k_hist<<<P.total_chunks, kHistThreads, ((size_t)4 << P.max_bits) + sizeof(HeavySmem), st>>>(P);
-        mark(1);
+    }
+    mark(1);
+    if (part) {
         k_colscan<<<(P.total_parts + 255) / 256, 256, 0, st>>>(P);
         k_basescan<<<P.nrel, 1024, 0, st>>>(P);
-        mark(2);
+    }
+    mark(2);
+    if (nphj) {  // the non-partitioned joins' global tables
+        k_nphj_clear<<<dim3(pl->num_sms * 2, J), 256, 0, st>>>(P);
+        k_nphj_build<<<dim3(pl->num_sms * 4, J), 256, 0, st>>>(P);
+    }
+    if (part) {
         k_scatter1<false><<<P.total_chunks, kScatterThreads, sizeof(TileSmem), st>>>(P);
         if (P.any_heavy)
             k_scatter1<true><<<P.total_chunks, kScatterThreads, sizeof(TileSmem) + sizeof(HeavySmem), st>>>(P);
@@ -1991,19 +2023,18 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
         // R partitions searched by several sort-merge units (or too large for a
         // CTA) sorted once; also on executions that keep R's partitions, whose
         // units can differ from the previous execution's (sorting is idempotent)
-        if (P.alg == SPJ_ALG_SMJ || P.alg == SPJ_ALG_NL) k_sort_runs<<<P.total_jparts, kJoinThreads, jsm, st>>>(P);
-        mark(3);
-        k_units_count<<<(P.total_jparts + 255) / 256, 256, 0, st>>>(P);
-        k_units_scan<<<1, 1024, 0, st>>>(P);
-        k_units<<<(P.total_jparts * 32 + 255) / 256, 256, 0, st>>>(P);
-        mark(4);
-        if (P.alg == SPJ_ALG_SMJ)
-            k_join_smj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
-        else if (P.alg == SPJ_ALG_NL)
-            k_join_nl<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
-        else
-            k_join_phj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
+        if (M & ((1 << SPJ_ALG_SMJ) | (1 << SPJ_ALG_NL))) k_sort_runs<<<P.total_jparts, kJoinThreads, jsm, st>>>(P);
     }
+    mark(3);
+    k_units_count<<<(P.total_jparts + 255) / 256, 256, 0, st>>>(P);
+    k_units_scan<<<1, 1024, 0, st>>>(P);
+    k_units<<<(P.total_jparts * 32 + 255) / 256, 256, 0, st>>>(P);
+    mark(4);
+    // one kernel per local-join algorithm in the plan, each over its own units
+    if (M & (1 << SPJ_ALG_PHJ)) k_join_phj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
+    if (M & (1 << SPJ_ALG_SMJ)) k_join_smj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
+    if (M & (1 << SPJ_ALG_NL)) k_join_nl<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
+    if (nphj) k_nphj_probe<<<pl->join_blocks, kJoinThreads, 0, st>>>(P);
     mark(5);
     k_fixup_prep<<<J, 1024, (size_t)kUpSlots * 2 * 8, st>>>(P);
     // gaps are spread over all warps of a join's blocks; a batch gives each join fewer blocks
@@ -2016,7 +2047,7 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
     return cudaGetLastError();
 }
 
-cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm) {
+cudaError_t configure_kernels(int table_slots, int alg_mask, int *join_blocks_per_sm) {
     cudaError_t e;
     int dev = 0, max_smem = 0;
     cudaGetDevice(&dev);
@@ -2051,12 +2082,18 @@ cudaError_t configure_kernels(int table_slots, int alg, int *join_blocks_per_sm)
     e = cudaFuncSetAttribute(k_fixup_prep, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kUpSlots * 2 * 8);
     if (e) return e;
-    const void *jk = alg == SPJ_ALG_SMJ    ? (const void *)k_join_smj
-                     : alg == SPJ_ALG_NL   ? (const void *)k_join_nl
-                     : alg == SPJ_ALG_NPHJ ? (const void *)k_nphj_probe
-                                           : (const void *)k_join_phj;
-    const size_t dyn = alg == SPJ_ALG_NPHJ ? 0 : (size_t)table_slots * 8;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(join_blocks_per_sm, jk, kJoinThreads, dyn);
+    const void *jk[4] = {(const void *)k_join_phj, (const void *)k_nphj_probe, (const void *)k_join_smj,
+                         (const void *)k_join_nl};
+    int best = 1 << 30;
+    for (int a = 0; a < 4; a++) {
+        if (!(alg_mask & (1 << a))) continue;
+        int n = 0;
+        const size_t dyn = a == SPJ_ALG_NPHJ ? 0 : (size_t)table_slots * 8;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, jk[a], kJoinThreads, dyn))) return e;
+        best = std::min(best, n);
+    }
+    *join_blocks_per_sm = best == (1 << 30) ? 0 : best;
+    return cudaSuccess;
 }
 
 cudaError_t launch_checksum(const spj_kv_pair_t *pairs, const int64_t *n_dev, uint64_t *sum_dev, int sms,

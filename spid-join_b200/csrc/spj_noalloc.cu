@@ -65,7 +65,7 @@ int setup_device(int dev, DeviceSetup **out) {
         e = cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         if (e != cudaSuccess) return cuda_error(e, "cudaDeviceGetAttribute");
         int per_sm = 0;
-        e = configure_kernels(kDefaultTableSlots, SPJ_ALG_PHJ, &per_sm);
+        e = configure_kernels(kDefaultTableSlots, 1 << SPJ_ALG_PHJ, &per_sm);
         if (e != cudaSuccess) return cuda_error(e, "configure kernels");
         s.scratch = ptr;
         s.sms = prop.multiProcessorCount;

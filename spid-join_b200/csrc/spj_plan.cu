@@ -112,11 +112,23 @@ const spj_tuning_t *find_tuning(int64_t n_r, int64_t n_s, spj_tuning_t *out) {
 JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, int max_slots, bool alone,
                      int64_t batch_tuples, const spj_tuning_t *tune) {
     JoinShape sh;
+    // the local-join algorithm: the design's, or the autotuner's choice for the
+    // size class among the algorithms with the same output (the hash joins drop
+    // unmatched S tuples, sort-merge and nested loop keep them)
+    int alg = d.join_alg;
+    if (tune && tune->join_alg > 0) {
+        const int ta = tune->join_alg - 1;
+        const bool drops = alg == SPJ_ALG_PHJ || alg == SPJ_ALG_NPHJ;
+        if (drops == (ta == SPJ_ALG_PHJ || ta == SPJ_ALG_NPHJ)) alg = ta;
+    }
+    sh.alg = alg;
     const bool tuned_ts = d.table_slots <= 0 && tune && tune->table_slots > 0;
+    // a tuned table stays within the default size: in a batch the largest table
+    // sets the shared memory, and so the CTAs per SM, of every join kernel
     int ts = d.table_slots > 0 ? std::min(d.table_slots, max_slots)
-             : tuned_ts        ? std::min(tune->table_slots, max_slots)
+             : tuned_ts        ? std::min(std::min(tune->table_slots, kDefaultTableSlots), max_slots)
                                : kDefaultTableSlots;
-    if (d.join_alg == SPJ_ALG_NPHJ) {
+    if (alg == SPJ_ALG_NPHJ) {
         sh.bits = 0;
         sh.fine_bits = 0;
         sh.table_slots = 2;
@@ -133,7 +145,7 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
             // (in a batch the other joins do).
             // (the sort-merge join sorts each R partition in shared memory: half
             // as large partitions keep its sort in a power of two below the table)
-            const uint64_t target = std::max<uint64_t>(1, (uint64_t)ts / (d.join_alg == SPJ_ALG_SMJ ? 6 : 3));
+            const uint64_t target = std::max<uint64_t>(1, (uint64_t)ts / (alg == SPJ_ALG_SMJ ? 6 : 3));
             const int need = ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + target - 1) / target));
             const int par = alone ? ceil_log2((uint64_t)8 * sms) : 0;
             const int minb = ceil_log2((uint64_t)64 * d.rank_num);
@@ -148,7 +160,7 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
             const double bound = mean + 6.0 * sqrt(mean) + 32.0;
             double pow2 = 1.0;
             while (pow2 < bound) pow2 *= 2.0;
-            const double sized = d.join_alg == SPJ_ALG_SMJ ? 2.0 * pow2 : 3.0 * bound;
+            const double sized = alg == SPJ_ALG_SMJ ? 2.0 * pow2 : 3.0 * bound;
             const int want = (int)std::min<double>(max_slots, std::max(1024.0, sized));
             ts = std::min(ts, (want + 255) / 256 * 256);
             ts = std::max(ts, 1024);
@@ -186,7 +198,7 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     // below that): kept only when the heavy keys hold most of the sample;
     // heavy_sample > 0 sets the sample size and keeps whatever heavy keys it
     // finds (in either skew mode); -1 turns the path off.
-    if (d.join_alg != SPJ_ALG_NPHJ && d.heavy_sample >= 0 && n_s > 0) {
+    if (alg != SPJ_ALG_NPHJ && d.heavy_sample >= 0 && n_s > 0) {
         int64_t hs = 0;
         if (d.heavy_sample > 0) {
             hs = d.heavy_sample;
@@ -217,13 +229,13 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
     const size_t o_pref = take((3 * (2 * J + 1) + J + 1) * 4);
     uint64_t max_units = 64, max_items = 1;
     uint32_t tot_chunks = 0, tot_parts = 0, tot_coarse = 0, tot_jparts = 0;
-    int max_bits = 0, max_ts = 2, two = 0, any_heavy = 0;
+    int max_bits = 0, max_ts = 2, two = 0, any_heavy = 0, alg_mask = 0;
     const uint32_t warps = (uint32_t)pl->join_blocks * (kJoinThreads / 32);
     std::vector<uint32_t> chunk_pref(2 * J + 1), part_pref(2 * J + 1), coarse_pref(2 * J + 1), jpart_pref(J + 1);
     for (uint32_t j = 0; j < J; j++) {
         JoinHost &h = pl->joins[j];
         const JoinShape &sh = pl->shapes[j];
-        const bool nphj = d.join_alg == SPJ_ALG_NPHJ;
+        const bool nphj = sh.alg == SPJ_ALG_NPHJ;
         const uint64_t F = nphj ? 1 : 1ull << sh.bits;
         const uint64_t f1 = (!nphj && sh.fine_bits) ? 1ull << (sh.bits - sh.fine_bits) : 0;
         JoinDev &jd = h.dev;
@@ -235,10 +247,10 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
         jd.bits = sh.bits;
         jd.fine_bits = nphj ? 0 : sh.fine_bits;
         jd.table_slots = sh.table_slots;
-        jd.alg = d.join_alg;
+        jd.alg = sh.alg;
         jd.skew_mode = d.skew_mode;
         jd.group = d.rank_set * d.bank_set;
-        jd.keep_unmatched = (d.join_alg == SPJ_ALG_SMJ || d.join_alg == SPJ_ALG_NL) ? 1 : 0;
+        jd.keep_unmatched = (sh.alg == SPJ_ALG_SMJ || sh.alg == SPJ_ALG_NL) ? 1 : 0;
         jd.unit_tuples = sh.unit_tuples;
         jd.item_target = sh.item_target;
         jd.out_chunk = sh.out_chunk;
@@ -296,6 +308,7 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
             jd.heavy = sh.heavy_sample ? (HeavyTab *)(a + o_hv) : nullptr;
         }
         any_heavy |= sh.heavy_sample ? 1 : 0;
+        alg_mask |= 1 << sh.alg;
         max_units += nphj ? (uint64_t)h.n_s / jd.unit_tuples + 64
                           : F * (uint64_t)std::max(jd.group, 1) + (uint64_t)h.n_s / jd.unit_tuples + F + 64;
         if (f1) max_items += (uint64_t)(sh.nchunks[0] + sh.nchunks[1]) * f1 + 2 * f1;
@@ -325,7 +338,7 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
         P.total_jparts = tot_jparts;
         P.max_bits = max_bits;
         P.max_table_slots = max_ts;
-        P.alg = d.join_alg;
+        P.alg_mask = alg_mask;
         P.any_two_pass = two;
         P.any_heavy = any_heavy;
         P.units = (Unit *)(a + o_units);
@@ -432,8 +445,9 @@ static int create_plan(int J, const int64_t *n_r, const int64_t *n_s, const spj_
                                    J > 1 ? find_tuning(n_r[j], n_s[j], &tn) : nullptr);
         ts_max = std::max(ts_max, pl->shapes[j].table_slots);
     }
-    int per_sm = 0;
-    cudaError_t ce = configure_kernels(ts_max, design->join_alg, &per_sm);
+    int per_sm = 0, alg_mask = 0;
+    for (const JoinShape &sh : pl->shapes) alg_mask |= 1 << sh.alg;
+    cudaError_t ce = configure_kernels(ts_max, alg_mask, &per_sm);
     if (ce != cudaSuccess || per_sm < 1) {
         delete pl;
         return ce != cudaSuccess ? cuda_error(ce, "configure kernels")
@@ -514,8 +528,9 @@ int create_plan_stream(int J, const int64_t *n_r, const int64_t *n_s, const spj_
         h.dev.out = reinterpret_cast<Tuple *>(out[j]);
         h.dev.n_out_user = reinterpret_cast<unsigned long long *>(n_out[j]);
     }
-    int per_sm = 0;
-    cudaError_t ce = configure_kernels(ts_max, design->join_alg, &per_sm);
+    int per_sm = 0, alg_mask = 0;
+    for (const JoinShape &sh : pl->shapes) alg_mask |= 1 << sh.alg;
+    cudaError_t ce = configure_kernels(ts_max, alg_mask, &per_sm);
     if (ce != cudaSuccess || per_sm < 1) {
         delete pl;
         return ce != cudaSuccess ? cuda_error(ce, "configure kernels") : set_error(SPJ_E_ARG, "table too large");
@@ -806,7 +821,7 @@ int spj_tuning_set(const spj_tuning_t *entries, int n) {
     for (int i = 0; i < n; i++) {
         const spj_tuning_t &t = entries[i];
         if (t.log2_r < 0 || t.log2_r > 32 || t.log2_ratio < 0 || t.log2_ratio > 6 || t.radix_bits_delta < -4 ||
-            t.radix_bits_delta > 4 || t.table_slots < 0 || t.unit_tuples < 0)
+            t.radix_bits_delta > 4 || t.table_slots < 0 || t.unit_tuples < 0 || t.join_alg < 0 || t.join_alg > 4)
             return set_error(SPJ_E_ARG, "tuning entry " + std::to_string(i) + " out of range");
     }
     std::lock_guard<std::mutex> lk(g_tuning_mu);

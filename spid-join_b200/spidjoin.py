@@ -71,7 +71,8 @@ class Stats(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("log2_r", ctypes.c_int), ("log2_ratio", ctypes.c_int), ("radix_bits_delta", ctypes.c_int),
-                ("table_slots", ctypes.c_int), ("unit_tuples", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+                ("table_slots", ctypes.c_int), ("unit_tuples", ctypes.c_int), ("join_alg", ctypes.c_int),
+                ("reserved", ctypes.c_int * 2)]
 
 
 class ServerStats(ctypes.Structure):
@@ -608,7 +609,7 @@ class DistributedJoin:
 
 
 # ------------------------------------------------------------- autotuning --
-TUNING_KEYS = ("log2_r", "log2_ratio", "radix_bits_delta", "table_slots", "unit_tuples")
+TUNING_KEYS = ("log2_r", "log2_ratio", "radix_bits_delta", "table_slots", "unit_tuples", "join_alg")
 
 
 def set_tuning(entries):
@@ -639,17 +640,22 @@ def load_tuning(path):
 def autotune(classes, zipf=1.0, reps=3, batch_tuples=1 << 26, max_joins=256, candidates=None, log=None):
     """Autotuner of the batch planner: for every size class (log2|R|, log2(|S|/|R|))
     it builds a batch of joins of that class (about `batch_tuples` tuples, from the
-    seeded device generator), times every candidate setting of the fan-out offset,
-    table size and work-unit size with CUDA events (a warm-up, then `reps` runs),
-    checks every join's count and checksum, and keeps the fastest. Returns the
-    table (the fields of spj_tuning_t plus the measured times); set_tuning()
-    installs it. Needs a GPU."""
+    seeded device generator), times every candidate setting with CUDA events (a
+    warm-up, then `reps` runs), checks every join's count and checksum, and keeps
+    the fastest. A candidate is (fan-out offset, table slots, work-unit tuples,
+    algorithm), the last as spj_tuning_t.join_alg (0 = the partitioned hash join;
+    2 = the non-partitioned one, which skips the partitioning passes; 3-tuples
+    mean 0); the fan-out offset also sets the pass count (one scatter pass up to
+    2^8 partitions). Returns the table (the fields of spj_tuning_t plus the
+    measured times); set_tuning() installs it. Needs a GPU."""
     import torch
     set_tuning([])  # measure against the planner's own choices
     if candidates is None:
-        # table sizes stay the planner's: in a mixed batch the largest table sets
-        # the shared memory (and so the CTAs per SM) of every join
-        candidates = [(dl, 0, ut) for dl in (0, -1, -2, 1) for ut in (0, 32768, 131072)]
+        # tables no larger than the default: in a mixed batch the largest table sets
+        # the shared memory (and so the CTAs per SM) of every join kernel
+        candidates = ([(dl, 0, ut, a) for a in (0, 2) for dl in (0, -1, 1) for ut in (0, 131072)] +
+                      [(0, 4096, 0, 0), (-1, 8192, 0, 0)])
+    candidates = [tuple(c) + (0,) * (4 - len(c)) for c in candidates]
     table = []
     for lr, lt in classes:
         n_r = 1 << lr
@@ -679,11 +685,12 @@ def autotune(classes, zipf=1.0, reps=3, batch_tuples=1 << 26, max_joins=256, can
         del outs
         sums = torch.zeros(J, dtype=torch.int64, device="cuda")
         best, default_ms = None, None
-        for dl, ts, ut in candidates:
+        for dl, ts, ut, ta in candidates:
             bits = base_bits + dl
-            if bits < 1 or bits > 15:
+            if bits < 1 or bits > 15 or (ta == 2 and (dl or ts)):
                 continue
-            design = make_design(rank_num=1, radix_bits=bits if dl else 0, table_slots=ts, unit_tuples=ut)
+            design = make_design(rank_num=1, radix_bits=bits if dl else 0, table_slots=ts, unit_tuples=ut,
+                                 join_alg=ta - 1 if ta else 0)
             try:
                 b = Batch([n_r] * J, [n_s] * J, design)
                 outs = [torch.empty((b.output_capacity(j), 2), dtype=torch.int32, device="cuda") for j in range(J)]
@@ -709,13 +716,13 @@ def autotune(classes, zipf=1.0, reps=3, batch_tuples=1 << 26, max_joins=256, can
             except SpjError:
                 continue
             if not ok:
-                raise SpjError(-5, f"autotune candidate {(dl, ts, ut)} gave a wrong result for class {(lr, lt)}")
-            if (dl, ts, ut) == (0, 0, 0):
+                raise SpjError(-5, f"autotune candidate {(dl, ts, ut, ta)} gave a wrong result for class {(lr, lt)}")
+            if (dl, ts, ut, ta) == (0, 0, 0, 0):
                 default_ms = ms
             if best is None or ms < best[0]:
-                best = (ms, dl, ts, ut)
+                best = (ms, dl, ts, ut, ta)
         entry = {"log2_r": lr, "log2_ratio": lt, "radix_bits_delta": best[1], "table_slots": best[2],
-                 "unit_tuples": best[3], "joins": J, "ms": best[0], "planner_ms": default_ms}
+                 "unit_tuples": best[3], "join_alg": best[4], "joins": J, "ms": best[0], "planner_ms": default_ms}
         if log:
             log(entry)
         table.append(entry)

@@ -101,8 +101,10 @@ def test_cli_without_gpu_fails_loudly():
 
 
 def test_tuning_table_roundtrip(spj):
-    entries = [{"log2_r": 20, "log2_ratio": 1, "radix_bits_delta": -1, "table_slots": 8192, "unit_tuples": 0},
-               {"log2_r": 14, "log2_ratio": 3, "radix_bits_delta": 1, "table_slots": 0, "unit_tuples": 32768}]
+    entries = [{"log2_r": 20, "log2_ratio": 1, "radix_bits_delta": -1, "table_slots": 8192, "unit_tuples": 0,
+                "join_alg": 0},
+               {"log2_r": 14, "log2_ratio": 3, "radix_bits_delta": 1, "table_slots": 0, "unit_tuples": 32768,
+                "join_alg": 2}]
     spj.set_tuning(entries)
     try:
         assert spj.get_tuning() == entries

@@ -136,3 +136,34 @@ def test_autotuned_batch_stays_exact(spj, oracle):
             assert oracle.checksum(results[0][j]) == exp[j] & (2**64 - 1)
     finally:
         spj.set_tuning([])
+
+
+@pytest.mark.parametrize("design_alg,table", [
+    (0, [{"log2_r": 12, "log2_ratio": 1, "join_alg": 2}, {"log2_r": 16, "log2_ratio": 2, "join_alg": 1}]),
+    (2, [{"log2_r": 12, "log2_ratio": 1, "join_alg": 4}, {"log2_r": 16, "log2_ratio": 2, "join_alg": 3}]),
+    (0, [{"log2_r": 12, "log2_ratio": 1, "join_alg": 3}]),  # another output semantics: ignored
+])
+def test_batch_mixes_local_join_algorithms(spj, oracle, design_alg, table):
+    """A tuning table can give size classes their own local-join algorithm (among
+    those with the design's output semantics): one batch then runs the hash and
+    non-partitioned hash joins, or sort-merge and nested loop, side by side, each
+    over its own range of work units; every join equals the oracle."""
+    rng = np.random.default_rng(77)
+    specs = [(1 << 12, 1 << 13, 1.0), (1 << 16, 1 << 18, 1.2), (70000, 150000, 0.0), (1 << 12, 9000, 0.5)]
+    data = []
+    for n_r, n_s, z in specs:
+        R, S, _ = spj.generate_host(n_r, n_s, z, seed=int(rng.integers(1 << 30)))
+        S[::7, 0] = 0xFFFFFFF0  # unmatched S tuples: dropped by the hash joins, kept by SMJ / NL
+        data.append((R, S))
+    import torch
+    R = [torch.from_numpy(r.view(np.int32)).cuda() for r, _ in data]
+    S = [torch.from_numpy(x.view(np.int32)).cuda() for _, x in data]
+    spj.set_tuning(table)
+    try:
+        results, _ = run_batch(spj, specs, spj.make_design(rank_num=1, join_alg=design_alg), R, S)
+    finally:
+        spj.set_tuning([])
+    for rep in results:
+        for j, (r, x) in enumerate(data):
+            want = oracle.simple_join(r, x, keep_unmatched=design_alg in (2, 3))
+            assert np.array_equal(oracle.sort_pairs(rep[j]), oracle.sort_pairs(want)), j
