@@ -57,6 +57,9 @@ struct join_design_t {
     int unit_tuples = 0;
     int heavy_sample = 0;
     int table_slots = 0;
+    // selections on R and S ahead of the join (src/dpu/include/select.h predicates)
+    spj_predicate_t select_r{SPJ_PRED_NONE, SPJ_PRED_EQ, 0u, 0u};
+    spj_predicate_t select_s{SPJ_PRED_NONE, SPJ_PRED_EQ, 0u, 0u};
 
     spj_design_t to_c() const {
         spj_design_t d;
@@ -74,6 +77,8 @@ struct join_design_t {
         d.unit_tuples = unit_tuples;
         d.heavy_sample = heavy_sample;
         d.table_slots = table_slots;
+        d.select_r = select_r;
+        d.select_s = select_s;
         return d;
     }
 };

@@ -59,6 +59,29 @@ enum spj_skew_mode {
                               reference's fixed rank-set x bank-set replication */
 };
 
+/* A selection applied to a relation before it is joined: the reference's
+ * TPC-H-style predicates (src/dpu/include/select.h: the comparison operators of
+ * PREDINT64, :30-37, and predi_btw's inclusive range, :44-47) on a tuple's key
+ * or payload, as unsigned 32-bit values (the reference compares its dates the
+ * same way, predd, :4-11). The join path evaluates them inside its first pass
+ * over each relation (count and first scatter, or the non-partitioned join's
+ * build and probe), so the filtered tuples are never written; spj_select
+ * applies one on its own. */
+enum spj_pred_field { SPJ_PRED_NONE = 0, SPJ_PRED_KEY = 1, SPJ_PRED_PAYLOAD = 2 };
+enum spj_pred_op {
+    SPJ_PRED_EQ = 0,      /* value == lo */
+    SPJ_PRED_LE = 1,      /* value <= lo */
+    SPJ_PRED_GE = 2,      /* value >= lo */
+    SPJ_PRED_LT = 3,      /* value < lo */
+    SPJ_PRED_GT = 4,      /* value > lo */
+    SPJ_PRED_BETWEEN = 5  /* lo <= value <= hi */
+};
+typedef struct {
+    int field;  /* enum spj_pred_field (SPJ_PRED_NONE: every tuple passes) */
+    int op;     /* enum spj_pred_op */
+    uint32_t lo, hi;
+} spj_predicate_t;
+
 /* join_design_t, include/idpHandler.hpp:131-145, followed by B200 tuning fields
  * (0 = chosen by the planner). rank_num, rank_set and bank_set keep the
  * reference's meaning as replication knobs: 64 * rank_num is the minimum
@@ -86,7 +109,8 @@ typedef struct {
                            off; > 0 = that many, kept whatever their share (any skew mode);
                            -1 = off */
     int table_slots;    /* shared-memory hash-table slots per CTA */
-    int reserved[7];
+    spj_predicate_t select_r, select_s; /* selections on R and S ahead of the join */
+    int reserved[4];
 } spj_design_t;
 
 /* Fills the reference's defaults (idpHandler.hpp:131-145) and automatic tuning. */
@@ -299,6 +323,13 @@ void spj_server_destroy(spj_server_t *server);
  * serialised by the caller. */
 int spj_join_noalloc(const spj_kv_pair_t *r, int64_t n_r, const spj_kv_pair_t *s, int64_t n_s, spj_kv_pair_t *out,
                      int64_t out_capacity, int64_t *n_out, void *stream);
+
+/* Selection (src/dpu/include/select.h): out (device, capacity n) receives the
+ * tuples of in[0, n) that pass `pred`, n_out (device int64) their count. The
+ * tuples of each block of the input keep their order; the blocks' order in the
+ * output is unspecified (a join consumes the result as a multiset). */
+int spj_select(const spj_kv_pair_t *in, int64_t n, const spj_predicate_t *pred, spj_kv_pair_t *out, int64_t *n_out,
+               void *stream);
 
 /* The split before the rank-to-rank exchange of a join sharded over `world`
  * GPUs (this rank is `me`): the B200 form of the reference's global partition

@@ -188,3 +188,22 @@ def refpipe_dpu_sizes(R, S, ranks=1, rank_sets=1, bank_set=1, nthreads=None):
     if rc:
         raise RuntimeError(ERRORS.get(rc, rc))
     return rs, ss
+
+
+PRED_NONE, PRED_KEY, PRED_PAYLOAD = 0, 1, 2
+PRED_EQ, PRED_LE, PRED_GE, PRED_LT, PRED_GT, PRED_BETWEEN = 0, 1, 2, 3, 4, 5
+
+
+def select(tuples, field=PRED_KEY, op=PRED_EQ, lo=0, hi=0):
+    """The tuples (in input order) whose key (field 1) or payload (field 2)
+    passes the predicate, restating the reference's selection predicates
+    (src/dpu/include/select.h: PREDINT64's operators ==, <=, >=, <, > at :30-37
+    and predi_btw's inclusive range at :44-47) on unsigned 32-bit values."""
+    t = _tuples(tuples)
+    if field == PRED_NONE:
+        return t.copy()
+    v = t[:, 0] if field == PRED_KEY else t[:, 1]
+    lo, hi = np.uint32(lo), np.uint32(hi)
+    keep = {PRED_EQ: v == lo, PRED_LE: v <= lo, PRED_GE: v >= lo, PRED_LT: v < lo, PRED_GT: v > lo,
+            PRED_BETWEEN: (lo <= v) & (v <= hi)}[op]
+    return t[keep]

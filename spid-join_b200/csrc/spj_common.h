@@ -58,6 +58,27 @@ SPJ_HD uint32_t join_hash2(uint32_t key) {
     return h;
 }
 
+// A selection on a tuple (spj_predicate_t): the comparisons of the reference's
+// TPC-H predicates (src/dpu/include/select.h:30-37, PREDINT64) and its inclusive
+// range (predi_btw, :44-47) on the key (field 1) or payload (field 2) as
+// unsigned 32-bit values; field 0 passes every tuple.
+struct Pred {
+    uint32_t field, op, lo, hi;
+};
+
+SPJ_HD bool pred_pass(const Pred &p, uint32_t key, uint32_t pay) {
+    if (p.field == 0) return true;
+    const uint32_t v = p.field == 1 ? key : pay;
+    switch (p.op) {
+        case 0: return v == p.lo;
+        case 1: return v <= p.lo;
+        case 2: return v >= p.lo;
+        case 3: return v < p.lo;
+        case 4: return v > p.lo;
+        default: return p.lo <= v && v <= p.hi;
+    }
+}
+
 // splitmix64 (Steele, Lea, Flood 2014): the counter-based mixer of the generator
 // and the finaliser of the order-independent output checksum.
 SPJ_HD uint64_t mix64(uint64_t z) {

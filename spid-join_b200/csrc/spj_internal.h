@@ -57,6 +57,7 @@ struct RelDev {
     uint32_t *chist;     // [nchunks][F1] counts of the coarse buckets (two-pass scatter)
     uint32_t *total;     // [F] tuples per partition
     uint32_t *base;      // [F] partition starts
+    Pred pred;           // selection ahead of the join (field 0: none)
 };
 
 // The heavy table of one join: written by the sampling kernel (keys), completed

@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(1024) k_heavy_sample(PlanDev P) {
             if (i < m) {
                 const uint64_t lo = (uint64_t)i * n / m, hi = (uint64_t)(i + 1) * n / m;
                 const uint64_t idx = lo + mix64(i * 0x9e3779b97f4a7c15ull + n) % (hi - lo);
-                key[k] = Rs.in[idx].key;
+                const Tuple t = Rs.in[idx];
+                key[k] = pred_pass(Rs.pred, t.key, t.pay) ? t.key : 0u;
             }
         }
 #pragma unroll
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P) {
     const uint32_t b = c * R.chunk;
     const uint32_t e = min(R.n, b + R.chunk);
     auto count = [&](uint32_t key, uint32_t pay) {
-        if (!key) return;
+        if (!key || !pred_pass(R.pred, key, pay)) return;
         if (hmode) {
             const int hs = heavy_find(HS, key);
             if (hs >= 0) {
@@ -454,7 +455,7 @@ template <bool kHot, bool kBulk, bool kHeavy = false, typename BucketFn>
 __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint32_t b, uint32_t e,
                                               Tuple *__restrict__ out, TileSmem &S, int nb, BucketFn bucket_of,
                                               uint32_t (&uses)[2], unsigned int *err,
-                                              const HeavyOut *hvo = nullptr) {
+                                              const HeavyOut *hvo = nullptr, const Pred pred = Pred{0u, 0u, 0u, 0u}) {
     constexpr int PER = kTile / kScatterThreads;
     constexpr uint32_t kBulkMin = 8;  // bulk-store bodies shorter than this go by ordinary stores
     uint2 *o2 = reinterpret_cast<uint2 *>(out);
@@ -468,6 +469,7 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
         // head: index b when odd; tail: index e-1 when e is odd, unless that is the head
         if ((head && (b & 1u)) || (!head && (e & 1u) && !((b & 1u) && e - 1 == b))) {
             Tuple t = in[idx];
+            if (!pred_pass(pred, t.key, t.pay)) t.key = 0;  // not selected
             int hs = -1;
             if (kHeavy && t.key) hs = heavy_find(*hvo->hs, t.key);
             if (hs >= 0) {
@@ -523,6 +525,7 @@ __device__ __forceinline__ bool scatter_range(const Tuple *__restrict__ in, uint
         for (int k = 0; k < PER; k++) {
             const uint32_t idx = threadIdx.x + k * kScatterThreads;
             v[k] = idx < nt ? S.inbuf[buf][idx] : Tuple{0u, 0u};
+            if (pred.field && !pred_pass(pred, v[k].key, v[k].pay)) v[k].key = 0;  // not selected
             if (kHeavy) {  // heavy key: rank among the tile's heavy pairs (one counter add per warp)
                 int hs = v[k].key ? heavy_find(*hvo->hs, v[k].key) : -1;
                 const bool isH = hs >= 0;
@@ -729,13 +732,15 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) k_scatte
     if (heavy) {
         const HeavyOut hvo{&HS, reinterpret_cast<uint2 *>(J.out), (uint32_t)J.out_cap, J.ctr, J.keep_unmatched};
         if (nb <= kBulkMaxBuckets)
-            scatter_range<false, true, kHeavyJoins>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo);
+            scatter_range<false, true, kHeavyJoins>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo,
+                                                    R.pred);
         else
-            scatter_range<false, false, kHeavyJoins>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo);
+            scatter_range<false, false, kHeavyJoins>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, &hvo,
+                                                     R.pred);
     } else if (nb <= kBulkMaxBuckets) {
-        scatter_range<false, true>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error);
+        scatter_range<false, true>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, nullptr, R.pred);
     } else {
-        scatter_range<false, false>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error);
+        scatter_range<false, false>(R.in, b0, e0, dst, S, nb, coarse, uses, &J.ctr->error, nullptr, R.pred);
     }
     bulk_wait_all();  // this thread's bulk stores are performed before the CTA retires
 }
@@ -1688,7 +1693,7 @@ __global__ void k_nphj_build(PlanDev P) {
     unsigned long long *table = J.gtable;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const Tuple t = r[i];
-        if (t.key == 0) continue;
+        if (t.key == 0 || !pred_pass(Rr.pred, t.key, t.pay)) continue;
         const unsigned long long ent = ((unsigned long long)t.pay << 32) | t.key;
         uint32_t s = join_hash2(t.key) & tmask;
         for (uint32_t step = 0; step <= tmask; step++) {
@@ -1714,7 +1719,8 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
         const JoinDev &J = P.join[un.join];
         const unsigned long long *table = J.gtable;
         const uint32_t tmask = (uint32_t)(J.gtable_slots - 1);
-        const Tuple *s = P.rel[2 * un.join + 1].in;
+        const RelDev &Rs = P.rel[2 * un.join + 1];
+        const Tuple *s = Rs.in;
         constexpr int U = 4;
         for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
             Tuple t[U];
@@ -1722,6 +1728,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
             for (int k = 0; k < U; k++) {
                 const uint32_t idx = base + k * 32 + lane;
                 t[k] = idx < un.s_end ? s[idx] : Tuple{0u, 0u};
+                if (!pred_pass(Rs.pred, t[k].key, t[k].pay)) t[k].key = 0;  // not selected
             }
             uint32_t sl[U];
             unsigned long long e[U];
@@ -1949,6 +1956,55 @@ __global__ void k_gen_s(GenSpec g, Zipf z, Perm pr, Perm prank, Tuple *s, unsign
     if (expect && (threadIdx.x & 31) == 0) atomicAdd(expect, acc);
 }
 
+// Selection: one CTA per 8192-tuple block; the block counts its selected
+// tuples with ballots, reserves their range of the output with one atomic and
+// writes them in input order (warp by warp, each warp's share placed by a scan
+// of the warps' counts).
+constexpr int kSelectBlock = 8192, kSelectThreads = 256;
+__global__ void __launch_bounds__(kSelectThreads) k_select(const Tuple *in, uint64_t n, Pred pred, Tuple *out,
+                                                            unsigned long long *n_out) {
+    __shared__ uint32_t wcount[kSelectThreads / 32], wbase[kSelectThreads / 32];
+    __shared__ unsigned long long s_base;
+    constexpr int PER = kSelectBlock / kSelectThreads;  // 32 tuples per thread, warp-strided
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint64_t b0 = (uint64_t)blockIdx.x * kSelectBlock; b0 < n; b0 += (uint64_t)gridDim.x * kSelectBlock) {
+        // warp w covers [b0 + w * 1024, b0 + (w + 1) * 1024): 32 rounds of 32 tuples
+        const uint64_t wb = b0 + (uint64_t)warp * (kSelectBlock / (kSelectThreads / 32));
+        uint32_t masks[PER];
+        uint32_t cnt = 0;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint64_t i = wb + (uint64_t)k * 32 + lane;
+            bool keep = false;
+            if (i < n) {
+                const Tuple t = in[i];
+                keep = pred_pass(pred, t.key, t.pay);
+            }
+            masks[k] = __ballot_sync(0xffffffffu, keep);
+            cnt += __popc(masks[k]);
+        }
+        if (lane == 0) wcount[warp] = cnt;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t run = 0;
+            for (int w = 0; w < kSelectThreads / 32; w++) {
+                wbase[w] = run;
+                run += wcount[w];
+            }
+            s_base = run ? atomicAdd(n_out, (unsigned long long)run) : 0ull;
+        }
+        __syncthreads();
+        unsigned long long pos = s_base + wbase[warp];
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint64_t i = wb + (uint64_t)k * 32 + lane;
+            if ((masks[k] >> lane) & 1u) out[pos + __popc(masks[k] & lanemask_lt())] = in[i];
+            pos += __popc(masks[k]);
+        }
+        __syncthreads();  // wcount / wbase / s_base are rewritten by the next block
+    }
+}
+
 __global__ void k_hist_single(const Tuple *t, uint64_t n, int bits, uint32_t *hist) {
     const uint32_t mask = (1u << bits) - 1;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -2114,6 +2170,18 @@ cudaError_t launch_generate(uint64_t seed, int64_t n_r, int64_t n_s, double zipf
     if (s && n_s > 0)
         k_gen_s<<<sms * 8, 256, 0, st>>>(g, z, pr, prank, reinterpret_cast<Tuple *>(s),
                                           reinterpret_cast<unsigned long long *>(expect));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_select(const spj_kv_pair_t *in, int64_t n, const spj_predicate_t &p, spj_kv_pair_t *out,
+                          int64_t *n_out, int sms, cudaStream_t st) {
+    cudaMemsetAsync(n_out, 0, 8, st);
+    if (n <= 0) return cudaGetLastError();
+    const uint64_t blocks = std::min<uint64_t>(((uint64_t)n + kSelectBlock - 1) / kSelectBlock, (uint64_t)sms * 8);
+    k_select<<<(unsigned)blocks, kSelectThreads, 0, st>>>(reinterpret_cast<const Tuple *>(in), (uint64_t)n,
+                                                         Pred{(uint32_t)p.field, (uint32_t)p.op, p.lo, p.hi},
+                                                         reinterpret_cast<Tuple *>(out),
+                                                         reinterpret_cast<unsigned long long *>(n_out));
     return cudaGetLastError();
 }
 

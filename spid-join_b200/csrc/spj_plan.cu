@@ -22,6 +22,8 @@ cudaError_t launch_generate(uint64_t seed, int64_t n_r, int64_t n_s, double zipf
                             spj_kv_pair_t *s, uint64_t *expect, int sms, cudaStream_t st);
 cudaError_t launch_hist_single(const spj_kv_pair_t *t, int64_t n, int bits, uint32_t *hist, int sms,
                                cudaStream_t st);
+cudaError_t launch_select(const spj_kv_pair_t *in, int64_t n, const spj_predicate_t &p, spj_kv_pair_t *out,
+                          int64_t *n_out, int sms, cudaStream_t st);
 
 static thread_local std::string g_last_error;
 
@@ -265,6 +267,8 @@ size_t layout_plan(spj_plan *pl, char *a, bool image) {
             rd = RelDev{};
             rd.in = bound_in;
             rd.n = (uint32_t)n[r];
+            const spj_predicate_t &sel = r == 0 ? d.select_r : d.select_s;
+            rd.pred = Pred{(uint32_t)sel.field, (uint32_t)sel.op, sel.lo, sel.hi};
             rd.chunk = sh.chunk[r];
             rd.nchunks = nphj ? 0 : sh.nchunks[r];
             rd.join = j;
@@ -409,6 +413,9 @@ static int validate_design(const spj_design_t *d) {
     if (d->radix_bits < 0 || d->radix_bits > kMaxRadixBits)
         return set_error(SPJ_E_ARG, "radix_bits must be in [0, 15]");
     if (d->table_slots < 0 || d->unit_tuples < 0) return set_error(SPJ_E_ARG, "negative tuning value");
+    for (const spj_predicate_t *p : {&d->select_r, &d->select_s})
+        if (p->field < SPJ_PRED_NONE || p->field > SPJ_PRED_PAYLOAD || p->op < SPJ_PRED_EQ || p->op > SPJ_PRED_BETWEEN)
+            return set_error(SPJ_E_ARG, "a selection needs field 0..2 (none, key, payload) and op 0..5");
     return SPJ_OK;
 }
 
@@ -745,6 +752,18 @@ int spj_partition_histogram(const spj_kv_pair_t *tuples, int64_t n, int bits, ui
     if (rc) return rc;
     cudaError_t e = launch_hist_single(tuples, n, bits, hist, sms, (cudaStream_t)stream);
     return e ? cuda_error(e, "histogram kernel") : SPJ_OK;
+}
+
+int spj_select(const spj_kv_pair_t *in, int64_t n, const spj_predicate_t *pred, spj_kv_pair_t *out, int64_t *n_out,
+               void *stream) {
+    if (!pred || !n_out || n < 0 || (n > 0 && (!in || !out))) return set_error(SPJ_E_ARG, "bad selection arguments");
+    if (pred->field < SPJ_PRED_NONE || pred->field > SPJ_PRED_PAYLOAD || pred->op < SPJ_PRED_EQ ||
+        pred->op > SPJ_PRED_BETWEEN)
+        return set_error(SPJ_E_ARG, "a selection needs field 0..2 (none, key, payload) and op 0..5");
+    int sms = 0, rc = device_sms(&sms, nullptr);
+    if (rc) return rc;
+    cudaError_t e = launch_select(in, n, *pred, out, n_out, sms, (cudaStream_t)stream);
+    return e ? cuda_error(e, "selection kernel") : SPJ_OK;
 }
 
 int spj_checksum_device(const spj_kv_pair_t *pairs, const int64_t *n_dev, uint64_t *sum_dev, void *stream) {

@@ -34,7 +34,7 @@ EXPORTS = (
     "spj_batch_create", "spj_batch_output_capacity", "spj_batch_bind", "spj_batch_execute", "spj_batch_stats",
     "spj_server_create", "spj_server_output_capacity", "spj_server_submit", "spj_server_wait", "spj_server_stats",
     "spj_server_reset_stats", "spj_server_destroy", "spj_server_hold", "spj_exchange_split",
-    "spj_tuning_set", "spj_tuning_get", "spj_exchange_count", "spj_exchange_scatter",
+    "spj_tuning_set", "spj_tuning_get", "spj_exchange_count", "spj_exchange_scatter", "spj_select",
 )
 
 
@@ -44,13 +44,30 @@ class SpjError(RuntimeError):
         self.code = code
 
 
+class Predicate(ctypes.Structure):
+    """spj_predicate_t: a selection on a tuple's key (field 1) or payload (field 2):
+    op 0 ==, 1 <=, 2 >=, 3 <, 4 > lo; 5 lo <= value <= hi (src/dpu/include/select.h)."""
+    _fields_ = [("field", ctypes.c_int), ("op", ctypes.c_int), ("lo", ctypes.c_uint32), ("hi", ctypes.c_uint32)]
+
+
+PRED_FIELD = {"none": 0, "key": 1, "payload": 2}
+PRED_OP = {"==": 0, "<=": 1, ">=": 2, "<": 3, ">": 4, "between": 5}
+
+
+def predicate(field="key", op="==", lo=0, hi=0):
+    """A Predicate from names: predicate("payload", "between", 10, 99)."""
+    return Predicate(PRED_FIELD[field] if isinstance(field, str) else field,
+                     PRED_OP[op] if isinstance(op, str) else op, lo, hi)
+
+
 class Design(ctypes.Structure):
     """spj_design_t = join_design_t (include/idpHandler.hpp:131-145) + B200 tuning."""
     _fields_ = [("input_size", ctypes.c_int64), ("rank_num", ctypes.c_int), ("zipf_factor", ctypes.c_int),
                 ("rs_ratio", ctypes.c_int), ("rank_set", ctypes.c_int), ("bank_set", ctypes.c_int),
                 ("tpch_example", ctypes.c_int), ("join_alg", ctypes.c_int), ("radix_bits", ctypes.c_int),
                 ("skew_mode", ctypes.c_int), ("unit_tuples", ctypes.c_int), ("heavy_sample", ctypes.c_int),
-                ("table_slots", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+                ("table_slots", ctypes.c_int), ("select_r", Predicate), ("select_s", Predicate),
+                ("reserved", ctypes.c_int * 4)]
 
 
 class Result(ctypes.Structure):
@@ -131,6 +148,7 @@ def lib():
                                         ctypes.POINTER(ctypes.c_uint64), i32]
         L.spj_generate_device.argtypes = [ctypes.c_uint64, i64, i64, ctypes.c_double, vp, vp, vp, vp]
         L.spj_join_noalloc.argtypes = [vp, i64, vp, i64, vp, i64, vp, vp]
+        L.spj_select.argtypes = [vp, i64, ctypes.POINTER(Predicate), vp, vp, vp]
         L.spj_batch_create.argtypes = [i32, vp, vp, ctypes.POINTER(Design), ctypes.POINTER(vp)]
         L.spj_batch_output_capacity.argtypes = [vp, i32]
         L.spj_batch_output_capacity.restype = i64
@@ -172,7 +190,7 @@ def make_design(**kw):
             v = ALG[v]
         if k not in {f[0] for f in Design._fields_}:
             raise KeyError(k)
-        setattr(d, k, int(v))
+        setattr(d, k, v if isinstance(v, Predicate) else int(v))
     return d
 
 

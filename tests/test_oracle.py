@@ -150,3 +150,18 @@ def test_threaded_join_and_sort_equal_single_threaded(oracle):
             assert np.array_equal(a, oracle.simple_join_mt(R, S, keep_unmatched=keep, nthreads=t))
     for t in (1, 5, 16):
         assert np.array_equal(oracle.sort_pairs(S), oracle.sort_pairs_mt(S, nthreads=t))
+
+
+def test_select_restates_the_reference_predicates(oracle):
+    rng = np.random.default_rng(21)
+    T = np.stack([rng.integers(0, 1000, 5000), rng.integers(0, 2**32, 5000)], 1).astype(np.uint32)
+    cmp = {0: lambda v, a, b: v == a, 1: lambda v, a, b: v <= a, 2: lambda v, a, b: v >= a,
+           3: lambda v, a, b: v < a, 4: lambda v, a, b: v > a, 5: lambda v, a, b: a <= v <= b}
+    for field in (1, 2):
+        for op in range(6):
+            lo = 500 if field == 1 else 2**31
+            hi = 700 if field == 1 else 2**32 - 5
+            want = [tuple(t) for t in T.tolist() if cmp[op](t[field - 1], lo, hi)]
+            got = oracle.select(T, field, op, lo, hi)
+            assert [tuple(t) for t in got.tolist()] == want, (field, op)
+    assert np.array_equal(oracle.select(T, 0), T)
