@@ -59,9 +59,9 @@ def launches_per_join(alg, radix_bits, single=True, heavy=False):
     return n + 10 + (2 if radix_bits > 8 else 0) + (2 if heavy else 0)
 
 
-def samples_heavy(args, n_s):
+def samples_heavy(args, n_s, alg=None):
     """Whether the plan samples heavy keys for this join (the planner's rule)."""
-    if args.alg == 1 or args.heavy < 0:
+    if args.alg == 1 or alg == 1 or args.heavy < 0:
         return False
     return args.heavy > 0 or (args.skew == 0 and n_s >= (1 << 24))
 
@@ -448,7 +448,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": desc, "n_r": n_r, "n_s": n_s, "zipf": zipf, "rank_num": ranks,
-                       "rank_set": rsets, "bank_set": bset, "join_alg": args.alg,
+                       "rank_set": rsets, "bank_set": bset, "join_alg": args.alg, "join_alg_run": st["join_alg"],
                        "skew_mode": "adaptive" if args.skew == 0 else "fixed",
                        "radix_bits": st["radix_bits"], "table_slots": st["table_slots"],
                        "l2": "inputs (8*(|R|+|S|) bytes) larger than the 126 MB L2; no flush",
@@ -460,7 +460,7 @@ def run_ours(args):
                                   "algorithmic_bytes": pipe_bytes, "formula": "24*(|R|+|S|) + 8*|out|"},
             "kernels_ms": kmean,
             "e2e": e2e, "cpu_baseline": cpu,
-            "gpu_launches": launches_per_join(args.alg, st["radix_bits"], heavy=samples_heavy(args, n_s)) * args.steps,
+            "gpu_launches": launches_per_join(st["join_alg"], st["radix_bits"], heavy=samples_heavy(args, n_s, st["join_alg"])) * args.steps,
             "clocks": leg["clocks"],
             "check": {"n_pairs": n_pairs, "checksum_ok": leg["ok"], "max_s_partition": st["max_s_partition"],
                       "units": st["units"], "heavy_keys": st["heavy_keys"], "heavy_tuples": st["heavy_tuples"]},

@@ -166,6 +166,7 @@ typedef struct {
     int64_t max_s_partition; /* largest S partition */
     int radix_bits;
     int table_slots;
+    int join_alg;            /* the local-join algorithm the plan runs (enum spj_join_alg) */
 } spj_stats_t;
 
 /* void RecordLogs(struct timespec start, int rank_group), include/join_internals.hpp:323:

@@ -130,6 +130,8 @@ extern "C" int spj_join_noalloc(const spj_kv_pair_t *r, int64_t n_r, const spj_k
     pl.joins[0].n_r = n_r;
     pl.joins[0].n_s = n_s;
     JoinShape sh = plan_shape(n_r, n_s, pl.design, ds->sms, ds->table_slots_max, true, 0, nullptr);
+    sh.alg = SPJ_ALG_PHJ;  // the partitioned hash join (its scratch fits the fixed region)
+    sh.gtable_slots = 0;
     sh.bits = std::min(std::max(ceil_log2((uint64_t)std::max<int64_t>(1, (n_r + 4095) / 4096)), 6), kMaxPassBits);
     sh.fine_bits = 0;
     {

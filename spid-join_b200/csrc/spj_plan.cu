@@ -118,6 +118,14 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     // size class among the algorithms with the same output (the hash joins drop
     // unmatched S tuples, sort-merge and nested loop keep them)
     int alg = d.join_alg;
+    // A hash join planned alone whose R's global table (2 slots of 8 bytes per R
+    // tuple, rounded to a power of two) fits in a quarter of the 126 MB L2 runs
+    // as the non-partitioned hash join: same output, no partitioning passes, and
+    // its probes hit L2 (|R| <= 2^20 here). Adaptive skew mode only: the rank-set
+    // and bank-set replication knobs of the fixed mode shape partitions.
+    if (alone && alg == SPJ_ALG_PHJ && d.skew_mode == SPJ_SKEW_ADAPTIVE && d.radix_bits <= 0 && n_r > 0 &&
+        n_r <= (1 << 20))
+        alg = SPJ_ALG_NPHJ;
     if (tune && tune->join_alg > 0) {
         const int ta = tune->join_alg - 1;
         const bool drops = alg == SPJ_ALG_PHJ || alg == SPJ_ALG_NPHJ;
@@ -213,6 +221,12 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     sh.unit_tuples = d.unit_tuples > 0                ? (uint32_t)d.unit_tuples
                      : (tune && tune->unit_tuples > 0) ? (uint32_t)tune->unit_tuples
                                                        : (uint32_t)kDefaultUnitTuples;
+    if (alg == SPJ_ALG_NPHJ && alone && d.unit_tuples <= 0) {
+        // the non-partitioned join's units are plain ranges of S: a join alone
+        // cuts S into about eight units per SM so that every SM probes
+        const int64_t u = (n_s + 8ll * sms - 1) / (8ll * sms);
+        sh.unit_tuples = (uint32_t)std::min<int64_t>(kDefaultUnitTuples, std::max<int64_t>(2048, u));
+    }
     return sh;
 }
 
@@ -633,6 +647,7 @@ static void fill_stats(const spj_plan *pl, const JoinCtr &c, spj_stats_t *out) {
     out->table_slots = pl->shapes[0].table_slots;
     out->heavy_keys = c.heavy_keys;
     out->heavy_tuples = (int64_t)c.heavy_tuples;
+    out->join_alg = pl->shapes[0].alg;
 }
 
 static int ctr_error(const spj_plan *pl, unsigned err, unsigned max_r) {
@@ -743,6 +758,7 @@ int spj_batch_stats(spj_plan_t *pl, int j, spj_stats_t *out) {
     fill_stats(pl, c, out);
     out->radix_bits = pl->shapes[j].bits;
     out->table_slots = pl->shapes[j].table_slots;
+    out->join_alg = pl->shapes[j].alg;
     return ctr_error(pl, c.error, c.max_r_part);
 }
 

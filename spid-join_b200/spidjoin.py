@@ -80,7 +80,8 @@ class Stats(ctypes.Structure):
                 ("finish_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("n_pairs", ctypes.c_int64), ("units", ctypes.c_int64), ("heavy_keys", ctypes.c_int64),
                 ("heavy_tuples", ctypes.c_int64), ("max_r_partition", ctypes.c_int64),
-                ("max_s_partition", ctypes.c_int64), ("radix_bits", ctypes.c_int), ("table_slots", ctypes.c_int)]
+                ("max_s_partition", ctypes.c_int64), ("radix_bits", ctypes.c_int), ("table_slots", ctypes.c_int),
+                ("join_alg", ctypes.c_int)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}

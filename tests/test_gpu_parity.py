@@ -42,11 +42,13 @@ def test_kat_main_cc(spj, oracle, case):
     assert sum(res.byte_sizes) == 8 * case["n_pairs"]
 
 
+@pytest.mark.parametrize("bits", [0, 11])  # 0: the planner's plan (non-partitioned for small R), 11: partitioned
 @pytest.mark.parametrize("zipf", [0.0, 1.0, 1.5])
 @pytest.mark.parametrize("n_r,ratio", [(1 << 10, 2), (1 << 16, 4), (100003, 3), (1 << 20, 2)])
-def test_generated_joins(spj, oracle, zipf, n_r, ratio):
+def test_generated_joins(spj, oracle, zipf, n_r, ratio, bits):
     R, S, expect = spj.generate_host(n_r, n_r * ratio, zipf, seed=n_r + int(10 * zipf))
-    res, logs = run_instance(spj, R, S)
+    res, logs = run_instance(spj, R, S, radix_bits=bits)
+    assert logs["join_alg"] == (1 if bits == 0 else 0)
     out = res.pairs()
     assert out.shape[0] == S.shape[0]
     assert oracle.checksum(out) == expect
@@ -58,7 +60,9 @@ def test_generated_joins(spj, oracle, zipf, n_r, ratio):
 def test_replication_groups_bit_exact(spj, oracle, layout):
     ranks, rsets, bset, mode = layout
     R, S, expect = spj.generate_host(1 << 17, 1 << 19, 1.5, seed=31)
-    res, logs = run_instance(spj, R, S, ranks=ranks, rank_sets=rsets, bank_set=bset, skew_mode=mode)
+    # an explicit fan-out keeps the partitioned join (the planner would run this
+    # small R without partitions)
+    res, logs = run_instance(spj, R, S, ranks=ranks, rank_sets=rsets, bank_set=bset, skew_mode=mode, radix_bits=11)
     out = res.pairs()
     assert out.shape[0] == S.shape[0] and oracle.checksum(out) == expect
 
@@ -72,21 +76,23 @@ def test_tuning_variants(spj, oracle, bits, slots):
     assert logs["radix_bits"] == bits
 
 
-def test_non_fk_and_key_zero(spj, oracle):
+@pytest.mark.parametrize("bits", [0, 9])
+def test_non_fk_and_key_zero(spj, oracle, bits):
     rng = np.random.default_rng(5)
     R = np.stack([rng.permutation(np.arange(1, 50001)), rng.integers(0, 2**32, 50000)], 1).astype(np.uint32)
     R[::97, 0] = 0
     S = np.stack([rng.integers(0, 100000, 300001), np.arange(300001)], 1).astype(np.uint32)
-    res, _ = run_instance(spj, R, S)
+    res, _ = run_instance(spj, R, S, radix_bits=bits)
     assert same_multiset(oracle, res.pairs(), oracle.simple_join(R, S))
 
 
-def test_duplicate_r_keys_one_match_each(spj, oracle):
+@pytest.mark.parametrize("bits", [0, 9])
+def test_duplicate_r_keys_one_match_each(spj, oracle, bits):
     rng = np.random.default_rng(6)
     keys = rng.integers(1, 2000, 40000)
     R = np.stack([keys, np.arange(40000)], 1).astype(np.uint32)
     S = np.stack([rng.integers(1, 4000, 100000), np.arange(100000)], 1).astype(np.uint32)
-    out = run_instance(spj, R, S)[0].pairs()
+    out = run_instance(spj, R, S, radix_bits=bits)[0].pairs()
     present = np.zeros(4001, bool)
     present[keys] = True
     assert out.shape[0] == int(present[S[:, 0]].sum())        # one match per S tuple with a key in R
@@ -94,12 +100,13 @@ def test_duplicate_r_keys_one_match_each(spj, oracle):
     assert np.array_equal(R[out[:, 0], 0], S[out[:, 1], 0])   # each pair joins equal keys
 
 
+@pytest.mark.parametrize("bits", [0, 9])
 @pytest.mark.parametrize("nr,ns", [(0, 10), (10, 0), (0, 0), (1, 1), (3, 5), (1, 100000), (100000, 1)])
-def test_edge_sizes(spj, oracle, nr, ns):
+def test_edge_sizes(spj, oracle, nr, ns, bits):
     rng = np.random.default_rng(nr * 7 + ns)
     R = np.stack([rng.permutation(np.arange(1, nr + 1)), np.arange(nr)], 1).astype(np.uint32).reshape(nr, 2)
     S = np.stack([rng.integers(1, max(nr, 1) + 1, ns), np.arange(ns)], 1).astype(np.uint32).reshape(ns, 2)
-    res, _ = run_instance(spj, R, S)
+    res, _ = run_instance(spj, R, S, radix_bits=bits)
     assert same_multiset(oracle, res.pairs(), oracle.simple_join(R, S))
 
 
@@ -160,11 +167,18 @@ def test_device_generator_matches_host(spj):
 ALGS = ["phj", "nphj", "smj", "nl"]
 
 
+def alg_design(alg):
+    """The design keys of a local-join algorithm: the hash join with an explicit
+    fan-out stays partitioned (the planner runs a small R alone without
+    partitions)."""
+    return dict(join_alg=alg, radix_bits=11) if alg == "phj" else dict(join_alg=alg)
+
+
 @pytest.mark.parametrize("alg", ALGS)
 @pytest.mark.parametrize("zipf", [0.0, 1.0, 1.5])
 def test_algorithms_on_fk_joins(spj, oracle, alg, zipf):
     R, S, expect = spj.generate_host(1 << 16, 1 << 18, zipf, seed=77 + int(zipf * 10))
-    res, _ = run_instance(spj, R, S, join_alg=alg)
+    res, _ = run_instance(spj, R, S, **alg_design(alg))
     out = res.pairs()
     assert out.shape[0] == S.shape[0] and oracle.checksum(out) == expect
     assert same_multiset(oracle, out, oracle.simple_join(R, S))
@@ -177,7 +191,7 @@ def test_algorithms_non_fk_semantics(spj, oracle, alg):
     R = np.stack([rng.permutation(np.arange(1, 30001)), rng.integers(0, 2**32, 30000)], 1).astype(np.uint32)
     R[::101, 0] = 0
     S = np.stack([rng.integers(0, 60000, 200003), np.arange(200003)], 1).astype(np.uint32)
-    out = run_instance(spj, R, S, join_alg=alg)[0].pairs()
+    out = run_instance(spj, R, S, **alg_design(alg))[0].pairs()
     keep = alg in ("smj", "nl")
     assert same_multiset(oracle, out, oracle.simple_join(R, S, keep_unmatched=keep))
 
@@ -189,7 +203,7 @@ def test_algorithms_duplicate_r_keys(spj, alg):
     rng.shuffle(keys)
     R = np.stack([keys, np.arange(30000)], 1).astype(np.uint32)
     S = np.stack([rng.integers(1, 3000, 90000), np.arange(90000)], 1).astype(np.uint32)
-    out = run_instance(spj, R, S, join_alg=alg)[0].pairs()
+    out = run_instance(spj, R, S, **alg_design(alg))[0].pairs()
     assert out.shape[0] == S.shape[0]  # every S key occurs in R here
     assert np.array_equal(np.sort(out[:, 1]), np.arange(90000, dtype=np.uint32))
     assert np.array_equal(R[out[:, 0], 0], S[out[:, 1], 0])
@@ -201,7 +215,7 @@ def test_config3_sweep_all_bit_exact(spj, oracle):
     all give the same multiset."""
     R, S, expect = spj.generate_host(1 << 17, 1 << 20, 1.5, seed=3)
     ref = oracle.sort_pairs(oracle.simple_join(R, S))
-    variants = [dict(join_alg=a) for a in ALGS]
+    variants = [alg_design(a) for a in ALGS]
     variants += [dict(join_alg="phj", skew_mode=1, ranks=g, rank_sets=g) for g in (1, 4, 16)]
     for v in variants:
         v = dict(v)
@@ -217,7 +231,7 @@ def test_algorithms_edge_sizes(spj, oracle, alg, nr, ns):
     rng = np.random.default_rng(nr * 13 + ns)
     R = np.stack([rng.permutation(np.arange(1, nr + 1)), np.arange(nr)], 1).astype(np.uint32).reshape(nr, 2)
     S = np.stack([rng.integers(1, nr + 3, ns), np.arange(ns)], 1).astype(np.uint32).reshape(ns, 2)
-    out = run_instance(spj, R, S, join_alg=alg)[0].pairs()
+    out = run_instance(spj, R, S, **alg_design(alg))[0].pairs()
     assert same_multiset(oracle, out, oracle.simple_join(R, S, keep_unmatched=alg in ("smj", "nl")))
 
 

@@ -36,7 +36,8 @@ def test_join_with_selections(spj, oracle, alg):
     R, S, _ = spj.generate_host(1 << 17, 1 << 21, 1.5, seed=6)
     pr = spj.predicate("key", "between", 1000, 90000)
     ps = spj.predicate("payload", "<", 1500000)
-    res, logs = run_instance(spj, R, S, join_alg=alg, select_r=pr, select_s=ps, heavy_sample=1 << 14)
+    res, logs = run_instance(spj, R, S, join_alg=alg, select_r=pr, select_s=ps, heavy_sample=1 << 14,
+                             radix_bits=11 if alg == 0 else 0)
     want = oracle.simple_join(oracle.select(R, 1, 5, 1000, 90000), oracle.select(S, 2, 3, 1500000),
                               keep_unmatched=alg in (2, 3))
     assert same_multiset(oracle, res.pairs(), want)
