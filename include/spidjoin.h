@@ -337,7 +337,9 @@ int spj_select(const spj_kv_pair_t *in, int64_t n, const spj_predicate_t *pred, 
  * scatter into per-rank packets ahead of its rotate-and-stream shuffle
  * (src/dpu/src/join/glb_partition_packet.c:420-464, src/queryHostFunc.cc:481-777).
  * The destination of a tuple is (glb_partition_hash(key) * world) >> 32, except
- * for heavy keys (heavy_keys: device uint32[n_heavy], sorted, n_heavy <= 256),
+ * for heavy keys (heavy_keys: device uint32[n_heavy], n_heavy <= 256, sorted
+ * ascending -- a caller precondition: the kernels binary-search the list, so an
+ * unsorted one routes heavy tuples as ordinary ones),
  * SPID-Join's skew handling across ranks: with heavy_mode 1 (for S) a heavy
  * key's tuples stay on `me`; with heavy_mode 2 (for R, whose heavy tuples the
  * caller replicates to every rank) they leave the exchange; heavy_mode 0

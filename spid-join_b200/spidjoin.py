@@ -522,7 +522,10 @@ class DistributedJoin:
 
     # ---- exchanges
     def _heavy_dev(self, heavy, device):
+        """The heavy keys as the device array the exchange kernels binary-search:
+        ascending unsigned order (the kernels require it), as int32 bit patterns."""
         import torch
+        heavy = sorted(int(h) & 0xFFFFFFFF for h in heavy)
         return torch.tensor([h - (1 << 32) if h >= (1 << 31) else h for h in heavy] or [0], dtype=torch.int32,
                             device=device)
 
