@@ -127,7 +127,8 @@ __device__ __forceinline__ int heavy_find(const HeavySmem &H, uint32_t key) {
 }
 
 // One CTA per join: samples heavy_sample S keys (one at a pseudo-random position
-// inside each of heavy_sample equal strides of S), counts them in a shared-memory
+// inside each of heavy_sample strides of floor(|S| / heavy_sample) tuples),
+// counts them in a shared-memory
 // table and keeps the keys seen at least T times, T = max(4, sample/16384)
 // doubled until at most kHeavyMax keys remain. Which keys are chosen changes only
 // the speed, never the result.
@@ -148,6 +149,7 @@ __global__ void __launch_bounds__(1024) k_heavy_sample(PlanDev P) {
     const RelDev &Rs = P.rel[2 * blockIdx.x + 1];
     const uint64_t n = Rs.n;
     const uint32_t m = (uint32_t)min((uint64_t)J.heavy_sample, n);
+    const uint64_t stride = m ? n / m : 1;  // one division; the sample's positions need none
     constexpr int U = 8;  // loads in flight per thread
     for (uint32_t i0 = threadIdx.x; i0 < m; i0 += U * blockDim.x) {
         uint32_t key[U];
@@ -156,8 +158,7 @@ __global__ void __launch_bounds__(1024) k_heavy_sample(PlanDev P) {
             const uint32_t i = i0 + k * blockDim.x;
             key[k] = 0;
             if (i < m) {
-                const uint64_t lo = (uint64_t)i * n / m, hi = (uint64_t)(i + 1) * n / m;
-                const uint64_t idx = lo + mix64(i * 0x9e3779b97f4a7c15ull + n) % (hi - lo);
+                const uint64_t idx = (uint64_t)i * stride + mulhi64(mix64(i * 0x9e3779b97f4a7c15ull + n), stride);
                 const Tuple t = Rs.in[idx];
                 key[k] = pred_pass(Rs.pred, t.key, t.pay) ? t.key : 0u;
             }
@@ -1050,18 +1051,17 @@ __device__ __forceinline__ void warp_emit(const OutCtx &o, WarpOut &w, bool has,
     } else {
         const uint32_t avail = w.end - w.cur;
         uint32_t nb = 0;
-        if ((threadIdx.x & 31) == 0) nb = (uint32_t)atomicAdd(&o.ctr->out_reserved, (unsigned long long)o.chunk);
+        if ((threadIdx.x & 31) == 0) {
+            nb = (uint32_t)atomicAdd(&o.ctr->out_reserved, (unsigned long long)o.chunk);
+            // a chunk beyond the capacity: its pairs are dropped and the join fails
+            if (nb + o.chunk > o.cap) atomicOr(&o.ctr->error, 2u);
+        }
         nb = __shfl_sync(0xffffffffu, nb, 0);
         pos = rank < avail ? w.cur + rank : nb + (rank - avail);
         w.cur = nb + (m - avail);
         w.end = nb + o.chunk;
     }
-    if (has) {
-        if (pos < o.cap)
-            reinterpret_cast<uint2 *>(o.out)[pos] = make_uint2(lv, rv);
-        else
-            atomicOr(&o.ctr->error, 2u);
-    }
+    if (has && pos < o.cap) reinterpret_cast<uint2 *>(o.out)[pos] = make_uint2(lv, rv);
 }
 
 // Records the unused tail of the warp's chunk as the warp's hole in join J.
@@ -1131,42 +1131,37 @@ __device__ __forceinline__ void build_table(const PlanDev &P, const JoinDev &J, 
 // Probe of a2a_srj_probe_inner_mt.c:101-168: stop at the key (hit) or at an empty
 // slot (miss). Slots are read in aligned pairs (one 16-byte shared load), which
 // halves the steps of the linear scan; when the home slot s is odd, slot s-1 of
-// the first pair lies before the probe sequence and is ignored. The scan is
-// bounded by the table size.
+// the first pair lies before the probe sequence and is ignored. The first pair
+// decides almost every probe at a load of 1/3: it is resolved with selects, and
+// only a probe that finds both slots taken by other keys enters the loop. The
+// scan is bounded by the table size. Key 0 (padding) must not hit: callers mask
+// the result with key != 0 (its probe stops at the first empty slot).
 __device__ __forceinline__ bool probe_table(const unsigned long long *table, uint32_t ts,
                                             uint32_t key, uint32_t &rpay) {
     const uint32_t s = slot_of(key, ts);
     const ulonglong2 *t2 = reinterpret_cast<const ulonglong2 *>(table);
     uint32_t p = s & ~1u;
-    {
-        const ulonglong2 e = t2[p >> 1];
-        if (p == s) {
-            if ((uint32_t)e.x == key) {
-                rpay = (uint32_t)(e.x >> 32);
-                return true;
-            }
-            if ((uint32_t)e.x == 0) return false;
-        }
-        if ((uint32_t)e.y == key) {
-            rpay = (uint32_t)(e.y >> 32);
-            return true;
-        }
-        if ((uint32_t)e.y == 0) return false;
-        p += 2;
-        if (p >= ts) p = 0;
-    }
+    const ulonglong2 e = t2[p >> 1];
+    const bool even = p == s;
+    const uint32_t kx = (uint32_t)e.x, ky = (uint32_t)e.y;
+    const bool hx = even && kx == key, ex = even && kx == 0;
+    const bool hy = ky == key, ey = ky == 0;
+    rpay = hx ? (uint32_t)(e.x >> 32) : (uint32_t)(e.y >> 32);
+    if (hx || ex || hy || ey) return hx || (!ex && hy);
+    p += 2;
+    if (p >= ts) p = 0;
     for (uint32_t step = 1; step < ts / 2; step++) {
-        const ulonglong2 e = t2[p >> 1];
-        if ((uint32_t)e.x == key) {
-            rpay = (uint32_t)(e.x >> 32);
+        const ulonglong2 f = t2[p >> 1];
+        if ((uint32_t)f.x == key) {
+            rpay = (uint32_t)(f.x >> 32);
             return true;
         }
-        if ((uint32_t)e.x == 0) return false;
-        if ((uint32_t)e.y == key) {
-            rpay = (uint32_t)(e.y >> 32);
+        if ((uint32_t)f.x == 0) return false;
+        if ((uint32_t)f.y == key) {
+            rpay = (uint32_t)(f.y >> 32);
             return true;
         }
-        if ((uint32_t)e.y == 0) return false;
+        if ((uint32_t)f.y == 0) return false;
         p += 2;
         if (p >= ts) p = 0;
     }
@@ -1273,7 +1268,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
 #pragma unroll
             for (int k = 0; k < U; k++) {
                 uint32_t rp = 0;
-                const bool hit = t[k].key != 0 && probe_table(table, ts, t[k].key, rp);
+                const bool hit = probe_table(table, ts, t[k].key, rp) && t[k].key != 0;
                 warp_emit(o, w, hit, rp, t[k].pay);
             }
         }
