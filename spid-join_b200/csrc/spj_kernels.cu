@@ -1095,8 +1095,9 @@ __device__ __forceinline__ uint32_t slot_of(uint32_t key, uint32_t ts) {
 // (a2a_srj_probe_inner_mt.c:136-148).
 __device__ __forceinline__ void build_table(const PlanDev &P, const JoinDev &J, uint32_t j, uint32_t p,
                                             unsigned long long *table) {
-    const uint32_t ts = J.table_slots;
-        for (uint32_t i = threadIdx.x; i < ts; i += blockDim.x) table[i] = 0ull;
+    const uint32_t ts = J.table_slots;  // even: cleared in 16-byte pairs
+    ulonglong2 *t2 = reinterpret_cast<ulonglong2 *>(table);
+    for (uint32_t i = threadIdx.x; i < ts / 2; i += blockDim.x) t2[i] = make_ulonglong2(0ull, 0ull);
     __syncthreads();
     const RelDev &Rr = P.rel[2 * j];
     const uint32_t nr = Rr.total[p];
@@ -1260,10 +1261,15 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_phj(PlanDev P) {
             const uint32_t nxt = base + nwarps * 32 * U + lane * 16;
             if (lane < 8 && nxt < un.s_end) prefetch_l2(ps + nxt);
             Tuple t[U];
+            if (base + 32 * U <= un.s_end) {  // a whole step: no bounds per tuple
 #pragma unroll
-            for (int k = 0; k < U; k++) {
-                const uint32_t idx = base + k * 32 + lane;
-                t[k] = idx < un.s_end ? ps[idx] : Tuple{0u, 0u};
+                for (int k = 0; k < U; k++) t[k] = ps[base + k * 32 + lane];
+            } else {
+#pragma unroll
+                for (int k = 0; k < U; k++) {
+                    const uint32_t idx = base + k * 32 + lane;
+                    t[k] = idx < un.s_end ? ps[idx] : Tuple{0u, 0u};
+                }
             }
 #pragma unroll
             for (int k = 0; k < U; k++) {
