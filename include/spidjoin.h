@@ -371,6 +371,41 @@ int spj_exchange_scatter(const spj_kv_pair_t *tuples, int64_t n, int world, int 
                          int n_heavy, int heavy_mode, spj_kv_pair_t *const *dest_bufs, const int64_t *dest_offsets,
                          int64_t *cursor, void *stream);
 
+/* -------------------------------------------------- sharded join (NCCL) ---- */
+/* The join sharded over the GPUs of one node, one process per GPU, driven from
+ * C: the B200 form of the reference's multi-rank join (src/queryHostFunc.cc:
+ * 481-777, the rotate-and-stream shuffle; rank sets for skew,
+ * glb_partition_count.c:317-318). Every rank owns a shard of R and of S. A call
+ * (collective: every rank calls it, in the same order) finds the heavy keys of S
+ * from a sample of every rank (a key whose estimated count reaches
+ * heavy_share * |S_total| / world, at most 256 keys), all-gathers the R tuples
+ * of those keys, sends every other tuple to rank (glb_partition_hash(key) *
+ * world) >> 32 over NCCL (spj_exchange_split + grouped send/receive), and joins
+ * what the rank received with a local plan. The union of the ranks' outputs is
+ * the join of the whole relations.
+ *
+ * NCCL (libnccl.so.2) is loaded at the first call that needs it; without it
+ * these return SPJ_E_UNSUPPORTED.
+ *
+ * spj_dist_unique_id: one rank makes the id (128 bytes) and hands it to the
+ * others (any side channel). spj_dist_create: collective; binds the calling
+ * thread's current CUDA device. spj_dist_set_heavy: mode 0 = no heavy keys,
+ * 1 = heavy keys with more than one rank (default), 2 = always; share (default
+ * 0.25) and sample (S keys a rank samples, default 65536) as above; every rank
+ * sets the same values. spj_dist_join: r, s device shards (16-byte aligned);
+ * *pairs receives a device pointer to this rank's *n_pairs output pairs, owned by
+ * the handle and valid until its next join or its destruction; synchronises with
+ * `stream`. spj_dist_heavy_keys: the heavy keys of the last join (returns their
+ * number, copies at most `capacity` of them). */
+typedef struct spj_dist spj_dist_t;
+int spj_dist_unique_id(void *id_out);
+int spj_dist_create(const void *unique_id, int world, int rank, const spj_design_t *design, spj_dist_t **out);
+int spj_dist_set_heavy(spj_dist_t *d, int mode, double heavy_share, int sample);
+int spj_dist_join(spj_dist_t *d, const spj_kv_pair_t *r, int64_t n_r, const spj_kv_pair_t *s, int64_t n_s,
+                  const spj_kv_pair_t **pairs, int64_t *n_pairs, void *stream);
+int spj_dist_heavy_keys(const spj_dist_t *d, uint32_t *keys, int capacity);
+void spj_dist_destroy(spj_dist_t *d);
+
 /* Histogram of glb_partition_hash(key) & (2^bits - 1) over a device column (key-0
  * tuples skipped): the B200 form of the global partition count kernel
  * (src/dpu/src/join/glb_partition_count.c:119-371, partition_type 0). hist is a

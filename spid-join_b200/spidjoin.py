@@ -35,6 +35,8 @@ EXPORTS = (
     "spj_server_create", "spj_server_output_capacity", "spj_server_submit", "spj_server_wait", "spj_server_stats",
     "spj_server_reset_stats", "spj_server_destroy", "spj_server_hold", "spj_exchange_split",
     "spj_tuning_set", "spj_tuning_get", "spj_exchange_count", "spj_exchange_scatter", "spj_select",
+    "spj_dist_unique_id", "spj_dist_create", "spj_dist_set_heavy", "spj_dist_join", "spj_dist_heavy_keys",
+    "spj_dist_destroy",
 )
 
 
@@ -169,6 +171,13 @@ def lib():
         L.spj_exchange_split.argtypes = [vp, i64, i32, i32, vp, i32, i32, vp, vp, vp]
         L.spj_exchange_count.argtypes = [vp, i64, i32, i32, vp, i32, i32, vp, vp]
         L.spj_exchange_scatter.argtypes = [vp, i64, i32, i32, vp, i32, i32, vp, vp, vp, vp]
+        L.spj_dist_unique_id.argtypes = [vp]
+        L.spj_dist_create.argtypes = [vp, i32, i32, ctypes.POINTER(Design), ctypes.POINTER(vp)]
+        L.spj_dist_set_heavy.argtypes = [vp, i32, ctypes.c_double, i32]
+        L.spj_dist_join.argtypes = [vp, vp, i64, vp, i64, ctypes.POINTER(vp), ctypes.POINTER(i64), vp]
+        L.spj_dist_heavy_keys.argtypes = [vp, vp, i32]
+        L.spj_dist_destroy.argtypes = [vp]
+        L.spj_dist_destroy.restype = None
         L.spj_tuning_set.argtypes = [ctypes.POINTER(Tuning), i32]
         L.spj_tuning_get.argtypes = [ctypes.POINTER(Tuning), i32]
         _lib = L
@@ -628,6 +637,81 @@ class DistributedJoin:
             p.close()
         self._plans = {}
         self._bufs = {}
+
+
+class _DeviceView:
+    """A (n, 2) int32 device array at a raw pointer, for torch.as_tensor."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n, 2), "typestr": "<i4", "data": (ptr, False), "version": 2,
+                                         "strides": None}
+
+
+class ShardedJoin:
+    """The sharded join run by the library itself (spj_dist_*): the same
+    protocol as DistributedJoin -- heavy keys from an all-gathered sample of
+    every rank's S, their R tuples replicated, every other tuple routed to rank
+    (glb_partition_hash(key) * world) >> 32 -- with NCCL driven from C, so a C or
+    C++ caller needs no Python. `group`: a torch.distributed group whose ranks
+    share the NCCL id (broadcast over it); or world/rank/unique_id given directly
+    (world 1 needs neither). heavy: 0 off, 1 with more than one rank, 2 always."""
+
+    def __init__(self, group=None, design=None, heavy=1, heavy_share=0.25, sample=1 << 16, world=None, rank=None,
+                 unique_id=None):
+        uid = ctypes.create_string_buffer(128)
+        if world is None:
+            import torch.distributed as dist
+            world, rank = (dist.get_world_size(group), dist.get_rank(group)) if dist.is_initialized() else (1, 0)
+        if unique_id is not None:
+            uid.raw = bytes(unique_id)
+        elif world == 1:
+            check(lib().spj_dist_unique_id(uid))
+        else:
+            import torch.distributed as dist
+            obj = [None]
+            if rank == 0:
+                check(lib().spj_dist_unique_id(uid))
+                obj = [uid.raw]
+            src = dist.get_global_rank(group, 0) if group is not None else 0
+            dist.broadcast_object_list(obj, src=src, group=group)
+            uid.raw = obj[0]
+        self.world, self.rank = int(world), int(rank)
+        self.design = design if design is not None else make_design()
+        self.h = ctypes.c_void_p()
+        check(lib().spj_dist_create(uid, self.world, self.rank, ctypes.byref(self.design), ctypes.byref(self.h)))
+        check(lib().spj_dist_set_heavy(self.h, int(heavy), float(heavy_share), int(sample)))
+
+    def run(self, R, S, stream=None):
+        """R, S: this rank's shards, (n, 2) int32 CUDA tensors. Returns (pairs, n):
+        this rank's part of the join, a (n, 2) int32 tensor that views the
+        handle's output (valid until the next run or close)."""
+        import torch
+        st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        pp, n = ctypes.c_void_p(), ctypes.c_int64()
+        check(lib().spj_dist_join(self.h, R.data_ptr() if R.shape[0] else None, R.shape[0],
+                                  S.data_ptr() if S.shape[0] else None, S.shape[0], ctypes.byref(pp),
+                                  ctypes.byref(n), st))
+        if n.value == 0:
+            return torch.empty((0, 2), dtype=torch.int32, device=R.device), 0
+        return torch.as_tensor(_DeviceView(pp.value, n.value), device=R.device), n.value
+
+    @property
+    def last_heavy(self):
+        k = lib().spj_dist_heavy_keys(self.h, None, 0)
+        buf = (ctypes.c_uint32 * max(k, 1))()
+        lib().spj_dist_heavy_keys(self.h, buf, k)
+        return [int(buf[i]) for i in range(k)]
+
+    def close(self):
+        if self.h:
+            lib().spj_dist_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ------------------------------------------------------------- autotuning --

@@ -43,6 +43,21 @@ def test_no_gpu_fails_loudly(spj):
         spj.Plan(100, 100)
     with pytest.raises(spj.SpjError, match="NODEVICE"):
         spj.Server(1 << 30)
+    with pytest.raises(spj.SpjError, match="NODEVICE"):  # checked before NCCL is loaded
+        spj.ShardedJoin(world=1, rank=0, unique_id=bytes(128))
+
+
+def test_sharded_join_argument_checks(spj):
+    L = spj.lib()
+    h = ctypes.c_void_p()
+    uid = ctypes.create_string_buffer(128)
+    d = spj.make_design()
+    for world, rank in [(0, 0), (2, 2), (2, -1), (1025, 0)]:
+        assert L.spj_dist_create(uid, world, rank, ctypes.byref(d), ctypes.byref(h)) == -1
+    assert L.spj_dist_create(None, 1, 0, ctypes.byref(d), ctypes.byref(h)) == -1
+    assert L.spj_dist_set_heavy(None, 1, 0.25, 1024) == -1
+    assert L.spj_dist_heavy_keys(None, None, 0) == 0
+    L.spj_dist_destroy(None)
 
 
 def test_bad_arguments(spj):

@@ -174,3 +174,41 @@ def test_exchange_split_routes_heavy_keys(spj, oracle, mode):
     for r in range(world):
         want = T[keep & (d == r)]
         assert np.array_equal(oracle.sort_pairs(got[off[r]:off[r + 1]]), oracle.sort_pairs(want))
+
+
+@pytest.mark.parametrize("heavy", [0, 2])
+def test_sharded_join_native_one_rank(spj, oracle, heavy):
+    # the library's own NCCL driver (spj_dist_*) on a one-rank communicator:
+    # heavy=2 runs the heavy-key sample, the replicated R rows and both
+    # exchange modes even with one rank; the pairs equal the oracle's join
+    import torch
+    n_r, n_s = 1 << 17, 1 << 20
+    R, S, expect = spj.generate_host(n_r, n_s, 1.5, seed=29)
+    sj = spj.ShardedJoin(world=1, rank=0, design=spj.make_design(rank_num=1), heavy=heavy)
+    dR = torch.from_numpy(R.view(np.int32)).cuda()
+    dS = torch.from_numpy(S.view(np.int32)).cuda()
+    want = oracle.sort_pairs(oracle.simple_join(R, S))
+    for _ in range(2):  # the second call reuses the handle's plan and buffers
+        pairs, n = sj.run(dR, dS)
+        got = pairs.cpu().numpy().view(np.uint32)
+        assert n == n_s and oracle.checksum(got) == expect
+        assert np.array_equal(oracle.sort_pairs(got), want)
+    assert (len(sj.last_heavy) >= 1) == (heavy == 2)
+    assert sj.last_heavy == sorted(sj.last_heavy)
+    sj.close()
+
+
+def test_sharded_join_native_ragged_and_empty(spj, oracle):
+    import torch
+    sj = spj.ShardedJoin(world=1, rank=0, heavy=2)
+    R, S, _ = spj.generate_host(1000, 7777, 1.2, seed=31)
+    S = S.copy()
+    S[::5, 0] = 0  # padding never joins
+    dR = torch.from_numpy(R.view(np.int32)).cuda()
+    dS = torch.from_numpy(S.view(np.int32)).cuda()
+    for r, s, hr, hs in ((dR, dS, R, S), (dR[:0], dS, R[:0], S), (dR, dS[:0], R, S[:0]), (dR[:0], dS[:0], R[:0], S[:0])):
+        pairs, n = sj.run(r, s)
+        want = oracle.sort_pairs(oracle.simple_join(hr, hs))
+        assert n == want.shape[0]
+        assert np.array_equal(oracle.sort_pairs(pairs.cpu().numpy().view(np.uint32)), want)
+    sj.close()
