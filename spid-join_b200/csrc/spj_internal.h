@@ -89,6 +89,7 @@ struct JoinCtr {
     unsigned int unit_fill;
     unsigned int heavy_keys;          // keys joined on the fly
     unsigned long long heavy_tuples;  // S tuples joined on the fly (pairs emitted by the scatter)
+    unsigned int probe_done;          // direct non-partitioned probe: CTAs finished
 };
 
 // Per-join constants and output state.

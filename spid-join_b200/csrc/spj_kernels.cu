@@ -1678,11 +1678,17 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
 __global__ void k_nphj_clear(PlanDev P) {
     const JoinDev &J = P.join[blockIdx.y];
     if (J.alg != SPJ_ALG_NPHJ) return;
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < J.gtable_slots;
+    ulonglong2 *t2 = reinterpret_cast<ulonglong2 *>(J.gtable);  // >= 1024 slots, a power of two
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < J.gtable_slots / 2;
          i += (unsigned long long)gridDim.x * blockDim.x)
-        J.gtable[i] = 0ull;
+        t2[i] = make_ulonglong2(0ull, 0ull);
 }
 
+// The build: every R tuple into the join's linear-probing table in HBM (mostly
+// L2-resident at the sizes the planner picks). Each thread inserts B tuples at
+// once: every round issues the compare-and-swap of each tuple not yet placed,
+// and a collision moves that tuple to its next slot, so a thread waits for the
+// longest of its B probe sequences, not for their sum.
 __global__ void k_nphj_build(PlanDev P) {
     const uint32_t j = blockIdx.y;
     const JoinDev &J = P.join[j];
@@ -1692,16 +1698,152 @@ __global__ void k_nphj_build(PlanDev P) {
     const uint32_t n = Rr.n;
     const uint32_t tmask = (uint32_t)(J.gtable_slots - 1);
     unsigned long long *table = J.gtable;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const Tuple t = r[i];
-        if (t.key == 0 || !pred_pass(Rr.pred, t.key, t.pay)) continue;
-        const unsigned long long ent = ((unsigned long long)t.pay << 32) | t.key;
-        uint32_t s = join_hash2(t.key) & tmask;
-        for (uint32_t step = 0; step <= tmask; step++) {
-            const unsigned long long prev = atomicCAS(&table[s], 0ull, ent);
-            if (prev == 0ull || (uint32_t)prev == t.key) break;
-            s = (s + 1) & tmask;
-            if (step == tmask) atomicOr(&J.ctr->error, 1u);
+    constexpr int B = 4;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += B * stride) {
+        unsigned long long ent[B];
+        uint32_t s[B];
+        unsigned pend = 0;
+#pragma unroll
+        for (int k = 0; k < B; k++) {
+            const uint32_t i = i0 + k * stride;
+            Tuple t = i < n ? r[i] : Tuple{0u, 0u};
+            if (t.key && !pred_pass(Rr.pred, t.key, t.pay)) t.key = 0;
+            ent[k] = ((unsigned long long)t.pay << 32) | t.key;
+            s[k] = join_hash2(t.key) & tmask;
+            if (t.key) pend |= 1u << k;
+        }
+        for (uint32_t round = 0; pend && round <= tmask; round++) {
+            unsigned long long prev[B];
+#pragma unroll
+            for (int k = 0; k < B; k++)
+                if ((pend >> k) & 1u) prev[k] = atomicCAS(&table[s[k]], 0ull, ent[k]);
+#pragma unroll
+            for (int k = 0; k < B; k++) {
+                if (!((pend >> k) & 1u)) continue;
+                if (prev[k] == 0ull || (uint32_t)prev[k] == (uint32_t)ent[k])
+                    pend &= ~(1u << k);  // placed, or the key is present already
+                else
+                    s[k] = (s[k] + 1) & tmask;
+            }
+        }
+        if (pend) atomicOr(&J.ctr->error, 1u);  // the table is full (cannot happen at load <= 1/2)
+    }
+}
+
+// Probes the U tuples t of a thread in the global table at once: every round
+// resolves or advances each unresolved probe, so the thread waits for its
+// longest probe sequence. Returns the mask of hits; e[k] is then the matching
+// entry (R payload << 32 | key). Key-0 tuples (padding, not selected) miss.
+template <int U>
+__device__ __forceinline__ unsigned nphj_probe_all(const unsigned long long *table, uint32_t tmask, const Tuple (&t)[U],
+                                                   unsigned long long (&e)[U]) {
+    uint32_t sl[U];
+    unsigned pend = 0, hit = 0;
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+        sl[k] = join_hash2(t[k].key) & tmask;
+        e[k] = t[k].key ? __ldg(&table[sl[k]]) : 0ull;
+        if (t[k].key) pend |= 1u << k;
+    }
+    for (uint32_t round = 0; pend && round <= tmask; round++) {
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            if (!((pend >> k) & 1u)) continue;
+            if ((uint32_t)e[k] == t[k].key) {
+                hit |= 1u << k;
+                pend &= ~(1u << k);
+            } else if ((uint32_t)e[k] == 0u) {
+                pend &= ~(1u << k);
+            } else {
+                sl[k] = (sl[k] + 1) & tmask;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++)
+            if ((pend >> k) & 1u) e[k] = __ldg(&table[sl[k]]);
+    }
+    return hit;
+}
+
+// Probe of a non-partitioned join planned alone: CTAs stride over tiles of
+// kJoinThreads * 4 S tuples with no work-unit list; each tile's pairs are
+// counted per warp, the CTA reserves their space with one atomic and writes
+// them densely, so the output has no holes and needs no fix-up. The last CTA to
+// finish publishes the pair count (n_out and the caller's device counter).
+// Pairs within the output are in no particular order (a join's output is a
+// multiset); which R tuple of a repeated key matches is the first inserted, as
+// in every hash join here.
+__global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe_direct(PlanDev P) {
+    constexpr int U = 4, NW = kJoinThreads / 32;
+    __shared__ uint32_t s_woff[NW];
+    __shared__ uint32_t s_wcnt[NW];
+    __shared__ unsigned long long s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const JoinDev &J = P.join[0];
+    const RelDev &Rs = P.rel[1];
+    const Tuple *s = Rs.in;
+    const uint32_t n = Rs.n;
+    const Pred pred = Rs.pred;
+    const unsigned long long *table = J.gtable;
+    const uint32_t tmask = (uint32_t)(J.gtable_slots - 1);
+    uint2 *out = reinterpret_cast<uint2 *>(J.out);
+    const unsigned long long cap = J.out_cap;
+    JoinCtr *ctr = J.ctr;
+    constexpr uint32_t T = kJoinThreads * U;
+    for (uint32_t t0 = blockIdx.x * T; t0 < n; t0 += gridDim.x * T) {
+        Tuple t[U];
+        unsigned long long e[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const uint32_t idx = t0 + k * kJoinThreads + threadIdx.x;
+            t[k] = idx < n ? s[idx] : Tuple{0u, 0u};
+            if (t[k].key && !pred_pass(pred, t[k].key, t[k].pay)) t[k].key = 0;  // not selected
+        }
+        const unsigned hit = nphj_probe_all<U>(table, tmask, t, e);
+        unsigned hits[U];
+        uint32_t cnt = 0;
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            hits[k] = __ballot_sync(0xffffffffu, (hit >> k) & 1u);
+            cnt += __popc(hits[k]);
+        }
+        if (lane == 0) s_wcnt[warp] = cnt;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t c = s_wcnt[lane];
+            uint32_t incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += x;
+            }
+            s_woff[lane] = incl - c;
+            if (lane == 31) s_base = incl ? atomicAdd(&ctr->out_reserved, (unsigned long long)incl) : 0ull;
+        }
+        __syncthreads();
+        unsigned long long pos = s_base + s_woff[warp];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            if ((hits[k] >> lane) & 1u) {
+                const unsigned long long p = pos + __popc(hits[k] & lanemask_lt());
+                if (p < cap)
+                    out[p] = make_uint2((uint32_t)(e[k] >> 32), t[k].pay);
+                else
+                    atomicOr(&ctr->error, 2u);
+            }
+            pos += __popc(hits[k]);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctr->probe_done, 1u) == gridDim.x - 1) {  // every other CTA has reserved its pairs
+            __threadfence();
+            const unsigned long long total = atomicAdd(&ctr->out_reserved, 0ull);
+            const unsigned long long nout = total < cap ? total : cap;
+            ctr->n_out = nout;
+            if (J.n_out_user) *J.n_out_user = nout;
         }
     }
 }
@@ -1722,7 +1864,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
         const uint32_t tmask = (uint32_t)(J.gtable_slots - 1);
         const RelDev &Rs = P.rel[2 * un.join + 1];
         const Tuple *s = Rs.in;
-        constexpr int U = 4;
+        constexpr int U = 2;
         for (uint32_t base = un.s_begin + warp * 32 * U; base < un.s_end; base += nwarps * 32 * U) {
             Tuple t[U];
 #pragma unroll
@@ -1731,33 +1873,10 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_nphj_probe(PlanDev P) {
                 t[k] = idx < un.s_end ? s[idx] : Tuple{0u, 0u};
                 if (!pred_pass(Rs.pred, t[k].key, t[k].pay)) t[k].key = 0;  // not selected
             }
-            uint32_t sl[U];
             unsigned long long e[U];
+            const unsigned hit = nphj_probe_all<U>(table, tmask, t, e);
 #pragma unroll
-            for (int k = 0; k < U; k++) {
-                sl[k] = join_hash2(t[k].key) & tmask;
-                e[k] = t[k].key ? __ldg(&table[sl[k]]) : 0ull;
-            }
-#pragma unroll
-            for (int k = 0; k < U; k++) {
-                bool hit = false;
-                uint32_t rp = 0;
-                if (t[k].key) {
-                    uint32_t sx = sl[k];
-                    unsigned long long ex = e[k];
-                    for (uint32_t step = 0; step <= tmask; step++) {
-                        if ((uint32_t)ex == t[k].key) {
-                            hit = true;
-                            rp = (uint32_t)(ex >> 32);
-                            break;
-                        }
-                        if ((uint32_t)ex == 0) break;
-                        sx = (sx + 1) & tmask;
-                        ex = __ldg(&table[sx]);
-                    }
-                }
-                warp_emit(o, w, hit, rp, t[k].pay);
-            }
+            for (int k = 0; k < U; k++) warp_emit(o, w, (hit >> k) & 1u, (uint32_t)(e[k] >> 32), t[k].pay);
         }
         __syncthreads();
     }
@@ -2033,6 +2152,8 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
     const int M = P.alg_mask;
     const bool nphj = M & (1 << SPJ_ALG_NPHJ), part = M & ~(1 << SPJ_ALG_NPHJ);
     keep_r = keep_r && part;  // a non-partitioned join has no partitions to keep
+    // a non-partitioned join alone probes S directly: no work units, no fix-up
+    const bool direct = nphj && !part && P.njoin == 1;
     if (keep_r) {
         // one-join plan whose R partitions (out, hist offsets, totals) are still in
         // its buffers from its previous execution: count and scatter S only. The
@@ -2067,7 +2188,7 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
     mark(2);
     if (nphj) {  // the non-partitioned joins' global tables
         k_nphj_clear<<<dim3(pl->num_sms * 2, J), 256, 0, st>>>(P);
-        k_nphj_build<<<dim3(pl->num_sms * 4, J), 256, 0, st>>>(P);
+        k_nphj_build<<<dim3(pl->num_sms * 8, J), 256, 0, st>>>(P);
     }
     if (part) {
         k_scatter1<false><<<P.total_chunks, kScatterThreads, sizeof(TileSmem), st>>>(P);
@@ -2083,19 +2204,26 @@ cudaError_t launch_pipeline(spj_plan *pl, cudaStream_t st, bool keep_r) {
         if (M & ((1 << SPJ_ALG_SMJ) | (1 << SPJ_ALG_NL))) k_sort_runs<<<P.total_jparts, kJoinThreads, jsm, st>>>(P);
     }
     mark(3);
-    k_units_count<<<(P.total_jparts + 255) / 256, 256, 0, st>>>(P);
-    k_units_scan<<<1, 1024, 0, st>>>(P);
-    k_units<<<(P.total_jparts * 32 + 255) / 256, 256, 0, st>>>(P);
+    if (!direct) {
+        k_units_count<<<(P.total_jparts + 255) / 256, 256, 0, st>>>(P);
+        k_units_scan<<<1, 1024, 0, st>>>(P);
+        k_units<<<(P.total_jparts * 32 + 255) / 256, 256, 0, st>>>(P);
+    }
     mark(4);
     // one kernel per local-join algorithm in the plan, each over its own units
     if (M & (1 << SPJ_ALG_PHJ)) k_join_phj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
     if (M & (1 << SPJ_ALG_SMJ)) k_join_smj<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
     if (M & (1 << SPJ_ALG_NL)) k_join_nl<<<pl->join_blocks, kJoinThreads, jsm, st>>>(P);
-    if (nphj) k_nphj_probe<<<pl->join_blocks, kJoinThreads, 0, st>>>(P);
+    if (direct)
+        k_nphj_probe_direct<<<pl->join_blocks, kJoinThreads, 0, st>>>(P);
+    else if (nphj)
+        k_nphj_probe<<<pl->join_blocks, kJoinThreads, 0, st>>>(P);
     mark(5);
-    k_fixup_prep<<<J, 1024, (size_t)kUpSlots * 2 * 8, st>>>(P);
-    // gaps are spread over all warps of a join's blocks; a batch gives each join fewer blocks
-    k_fixup_copy<<<dim3(std::max<uint32_t>(64, (kMaxHoles + 7) / 8 / J), J), 256, 0, st>>>(P);
+    if (!direct) {
+        k_fixup_prep<<<J, 1024, (size_t)kUpSlots * 2 * 8, st>>>(P);
+        // gaps are spread over all warps of a join's blocks; a batch gives each join fewer blocks
+        k_fixup_copy<<<dim3(std::max<uint32_t>(64, (kMaxHoles + 7) / 8 / J), J), 256, 0, st>>>(P);
+    }
     mark(6);
     if (ev) {
         pl->ring_next = (pl->ring_next + 1) % spj_plan::kRing;

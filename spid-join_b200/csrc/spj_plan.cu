@@ -119,12 +119,14 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     // unmatched S tuples, sort-merge and nested loop keep them)
     int alg = d.join_alg;
     // A hash join planned alone whose R's global table (2 slots of 8 bytes per R
-    // tuple, rounded to a power of two) fits in a quarter of the 126 MB L2 runs
-    // as the non-partitioned hash join: same output, no partitioning passes, and
-    // its probes hit L2 (|R| <= 2^20 here). Adaptive skew mode only: the rank-set
-    // and bank-set replication knobs of the fixed mode shape partitions.
+    // tuple, rounded to a power of two) fits in half of the 126 MB L2 runs as the
+    // non-partitioned hash join: same output, no partitioning passes, and its
+    // probes hit L2 (|R| <= 2^22 here; measured on B200 it beats the partitioned
+    // join there by 1.2-1.6x, and loses from 2^23 on). Adaptive skew mode only:
+    // the rank-set and bank-set replication knobs of the fixed mode shape
+    // partitions.
     if (alone && alg == SPJ_ALG_PHJ && d.skew_mode == SPJ_SKEW_ADAPTIVE && d.radix_bits <= 0 && n_r > 0 &&
-        n_r <= (1 << 20))
+        n_r <= (1 << 22))
         alg = SPJ_ALG_NPHJ;
     if (tune && tune->join_alg > 0) {
         const int ta = tune->join_alg - 1;

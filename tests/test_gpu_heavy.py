@@ -84,7 +84,8 @@ def test_automatic_mode_keeps_heavy_keys_only_under_strong_skew(spj):
     on for Zipf 1.5, off for Zipf 1.0 (where a filter lookup per tuple would
     cost more than the partitioning it saves) and for uniform keys."""
     for zipf, on in ((1.5, True), (1.0, False), (0.0, False)):
-        R, S, expect = spj.generate_host(1 << 21, 1 << 24, zipf, seed=80)
+        # |R| = 2^23: above the size the planner joins without partitions
+        R, S, expect = spj.generate_host(1 << 23, 1 << 24, zipf, seed=80)
         res, logs = _run_instance(spj, R, S)
         assert (logs["heavy_keys"] > 0) == on, zipf
 

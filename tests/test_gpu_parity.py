@@ -304,3 +304,32 @@ def test_oracle_generator_equals_device_generator(spj, oracle, n_r, n_s, seed):
     assert np.array_equal(dR.cpu().numpy().view(np.uint32), R)
     assert np.array_equal(dS.cpu().numpy().view(np.uint32), S)
     assert int(e.item()) & (2**64 - 1) == expect
+
+
+@pytest.mark.parametrize("n_r,alg_run", [(1 << 22, 1), ((1 << 22) + 1, 0)])
+def test_planner_non_partitioned_up_to_2_22(spj, oracle, n_r, alg_run):
+    """A hash join planned alone runs without partitions up to |R| = 2^22 (its
+    table fits half of L2), partitioned above; the direct probe (no work units,
+    dense output) gives the oracle's pairs, padding and misses included."""
+    import torch
+    n_s = (1 << 23) + 5
+    R, S, _ = spj.generate_host(n_r, n_s, 1.2, seed=71)
+    S = S.copy()
+    S[::101, 0] = 0                      # padding
+    S[5::103, 0] = np.uint32(0xFFFFFFF0)  # keys absent from R
+    plan = spj.Plan(n_r, n_s, spj.make_design(rank_num=1))
+    dR = torch.from_numpy(R.view(np.int32)).cuda()
+    dS = torch.from_numpy(S.view(np.int32)).cuda()
+    out = torch.empty((plan.output_capacity, 2), dtype=torch.int32, device="cuda")
+    n = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for _ in range(2):  # the second execution reuses the cleared table
+        n.zero_()
+        plan.execute(dR.data_ptr(), dS.data_ptr(), out.data_ptr(), n.data_ptr())
+        torch.cuda.synchronize()
+        st = plan.stats()
+        assert st["join_alg"] == alg_run
+        k = int(n.item())
+        assert k == st["n_pairs"]
+        got = out[:k].cpu().numpy().view(np.uint32)
+        assert same_multiset(oracle, got, oracle.simple_join_mt(R, S))
+    plan.close()
