@@ -1431,10 +1431,118 @@ __device__ __forceinline__ unsigned long long *sort_smem(unsigned long long *buf
     return buf;
 }
 
+// Bucket sort by key range, the usual sort of an R run (<= 4096 tuples, four
+// per thread): the run's smallest and largest key set the range, a counting pass
+// drops every tuple into one of nb ~ n/2 buckets by (key - min) scaled to the
+// range (monotone in the key: bucket order is key order), the buckets' offsets
+// come from one scan, and each bucket (about two tuples) is put in (key, payload)
+// order by one thread's insertion sort. The result is the same sequence as the
+// merge sort's, from four barriers instead of ten rounds; hash partitioning
+// spreads a partition's keys over their range, so buckets stay short. A bucket
+// longer than kBucketMaxLen (many repeats of a key, or keys clustered in a
+// small part of the range) makes the sort give up (nullptr, the same in every
+// thread) and the caller merge-sorts; `a` is left unchanged.
+constexpr uint32_t kBucketSortMax = 4096;  // tuples (four per thread of kJoinThreads)
+constexpr uint32_t kBucketMaxLen = 32;
+constexpr uint32_t kBucketsMax = 2048;
+
+struct BucketSmem {
+    uint32_t cnt[kBucketsMax + 1];  // bucket counts, then their exclusive offsets (cnt[nb] = n)
+    uint32_t kmin, kmax, fail;
+};
+
+__device__ __forceinline__ unsigned long long *bucket_sort_smem(const unsigned long long *a, unsigned long long *b,
+                                                               uint32_t n, BucketSmem &B) {
+    constexpr int PER = kBucketSortMax / kJoinThreads;
+    const int lane = threadIdx.x & 31;
+    uint32_t nb = 32;
+    while (nb < kBucketsMax && 2 * nb < n) nb <<= 1;
+    if (threadIdx.x == 0) {
+        B.kmin = 0xffffffffu;
+        B.kmax = 0u;
+        B.fail = 0u;
+    }
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) B.cnt[i] = 0u;
+    unsigned long long v[PER];
+    uint32_t lo = 0xffffffffu, hi = 0u;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        const uint32_t i = threadIdx.x + k * blockDim.x;
+        v[k] = i < n ? a[i] : 0ull;
+        if (i < n) {
+            lo = min(lo, (uint32_t)(v[k] >> 32));
+            hi = max(hi, (uint32_t)(v[k] >> 32));
+        }
+    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    __syncthreads();  // initial values written
+    if (lane == 0) {
+        atomicMin(&B.kmin, lo);
+        atomicMax(&B.kmax, hi);
+    }
+    __syncthreads();
+    const uint32_t kmin = B.kmin;
+    const unsigned long long range = (unsigned long long)B.kmax - kmin + 1;  // >= 1 when n > 0
+    // bucket = floor((key - kmin) * nb / range) < nb: exact when the range fits
+    // the buckets, else a multiply-high by floor(2^32 * nb / range) (< 2^32)
+    const bool direct = range <= nb;
+    const uint32_t mult = direct ? 0u : (uint32_t)(((unsigned long long)nb << 32) / range);
+    uint32_t br[PER];  // bucket << 16 | rank in the bucket
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        const uint32_t i = threadIdx.x + k * blockDim.x;
+        if (i < n) {
+            const uint32_t d = (uint32_t)(v[k] >> 32) - kmin;
+            const uint32_t bk = direct ? d : __umulhi(d, mult);
+            br[k] = (bk << 16) | atomicAdd(&B.cnt[bk], 1u);
+        }
+    }
+    __syncthreads();
+    warp0_scan1024(B.cnt, B.cnt, (int)nb);  // in place: each lane reads its counters before writing them
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        const uint32_t i = threadIdx.x + k * blockDim.x;
+        if (i < n) b[B.cnt[br[k] >> 16] + (br[k] & 0xffffu)] = v[k];
+    }
+    __syncthreads();
+    for (uint32_t bk = threadIdx.x; bk < nb; bk += blockDim.x) {
+        const uint32_t s0 = B.cnt[bk], e0 = B.cnt[bk + 1];
+        if (e0 - s0 > kBucketMaxLen) {
+            B.fail = 1u;
+        } else {
+            for (uint32_t i = s0 + 1; i < e0; i++) {  // insertion sort of b[s0, e0)
+                const unsigned long long x = b[i];
+                uint32_t j = i;
+                while (j > s0 && b[j - 1] > x) {
+                    b[j] = b[j - 1];
+                    j--;
+                }
+                b[j] = x;
+            }
+        }
+    }
+    __syncthreads();
+    return B.fail ? nullptr : b;
+}
+
+// Sorts an R run: buf[0, n) holds it and buf[n, npad) padding (~0ull); `room`
+// entries of shared memory from buf. Returns where the n sorted tuples are.
+__device__ __forceinline__ const unsigned long long *sort_run_smem(unsigned long long *buf, uint32_t n, uint32_t npad,
+                                                                   uint32_t room, BucketSmem &B) {
+    if (n >= 64 && n <= kBucketSortMax && 2 * npad <= room) {
+        const unsigned long long *r = bucket_sort_smem(buf, buf + npad, n, B);
+        if (r) return r;
+    }
+    return sort_smem(buf, npad, room);
+}
+
 // One CTA per flat partition: the partitions `presorted` names, sorted in runs
 // of run_cap tuples.
 __global__ void __launch_bounds__(kJoinThreads, 2) k_sort_runs(PlanDev P) {
     extern __shared__ unsigned long long sorted[];
+    __shared__ BucketSmem bsm;
     const uint32_t t = blockIdx.x;
     const uint32_t j = find_slot(P.jpart_prefix, P.njoin, t);
     const uint32_t p = t - P.jpart_prefix[j];
@@ -1450,7 +1558,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_sort_runs(PlanDev P) {
         while (npad < len) npad <<= 1;
         for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x) sorted[i] = i < len ? pack_kp(pr[r0 + i]) : ~0ull;
         __syncthreads();
-        const unsigned long long *res = sort_smem(sorted, npad, (uint32_t)J.table_slots);
+        const unsigned long long *res = sort_run_smem(sorted, len, npad, (uint32_t)J.table_slots, bsm);
         for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
             const unsigned long long v = res[i];
             pr[r0 + i] = Tuple{(uint32_t)(v >> 32), (uint32_t)v};
@@ -1601,6 +1709,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_nl(PlanDev P) {
 __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
     extern __shared__ unsigned long long sorted[];
     __shared__ unsigned s_next;
+    __shared__ BucketSmem bsm;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nwarps = kJoinThreads / 32;  // every join kernel runs kJoinThreads threads
     const unsigned n_units = units_end(P, SPJ_ALG_SMJ);
@@ -1630,7 +1739,7 @@ __global__ void __launch_bounds__(kJoinThreads, 2) k_join_smj(PlanDev P) {
                 while (npad < nr) npad <<= 1;
                 for (uint32_t i = threadIdx.x; i < npad; i += blockDim.x) sorted[i] = i < nr ? pack_kp(pr[i]) : ~0ull;
                 __syncthreads();
-                keys = sort_smem(sorted, npad, (uint32_t)J.table_slots);
+                keys = sort_run_smem(sorted, nr, npad, (uint32_t)J.table_slots, bsm);
             }
         }
         __syncthreads();  // the copy is complete and the next unit's index is written
