@@ -57,6 +57,24 @@ __device__ __forceinline__ uint32_t route_of(uint32_t key, const Route &rt, cons
     return dest_of(key, rt.world);
 }
 
+// Rank of the calling lane among the tuples of destination d in cnt[d]
+// (cnt[d] += the group's size). With few destinations most lanes of a warp share
+// one, so the lanes of a destination take consecutive ranks with one atomic per
+// group (its stores then coalesce) instead of one serialised atomic each; with
+// many destinations a plain atomic per lane is cheaper than the grouping.
+// Called by the active lanes only (`act` = their mask).
+__device__ __forceinline__ uint32_t rank_in(uint32_t *cnt, uint32_t d, unsigned act, bool grouped) {
+    if (!grouped) return atomicAdd(&cnt[d], 1u);
+    const unsigned peers = __match_any_sync(act, d);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&cnt[d], (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+constexpr uint32_t kGroupedWorld = 32;  // grouped ranking up to this many destinations
+
 __device__ __forceinline__ void load_heavy(const Route &rt, uint32_t *heavy_sm) {
     for (uint32_t i = threadIdx.x; i < rt.nheavy; i += blockDim.x) heavy_sm[i] = rt.heavy[i];
 }
@@ -70,13 +88,15 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_count(const Tuple *in, 
     load_heavy(rt, heavy_sm);
     for (uint32_t d = threadIdx.x; d < rt.world; d += blockDim.x) cnt[d] = 0;
     __syncthreads();
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
-         i += (unsigned long long)gridDim.x * blockDim.x) {
-        const Tuple t = in[i];
-        if (t.key) {
-            const uint32_t d = route_of(t.key, rt, heavy_sm);
-            if (d != kDrop) atomicAdd(&cnt[d], 1u);
-        }
+    const bool grouped = rt.world <= kGroupedWorld;
+    // whole warps iterate together (the grouping needs the warp's lanes)
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i0 = (unsigned long long)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const unsigned long long i = i0 + threadIdx.x;
+        const Tuple t = i < n ? in[i] : Tuple{0u, 0u};
+        const uint32_t d = t.key ? route_of(t.key, rt, heavy_sm) : kDrop;
+        const unsigned act = __ballot_sync(0xffffffffu, d != kDrop);
+        if (d != kDrop) rank_in(cnt, d, act, grouped);
     }
     __syncthreads();
     for (uint32_t d = threadIdx.x; d < rt.world; d += blockDim.x)
@@ -114,6 +134,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_scatter(const Tuple *in
     __shared__ unsigned long long base[kMaxWorld];
     __shared__ uint32_t heavy_sm[kMaxHeavy];
     const uint32_t world = rt.world;
+    const bool grouped = world <= kGroupedWorld;
     constexpr int PER = kSplitTile / kSplitThreads;
     load_heavy(rt, heavy_sm);
     for (unsigned long long t0 = (unsigned long long)blockIdx.x * kSplitTile; t0 < n;
@@ -126,11 +147,9 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_scatter(const Tuple *in
         for (int k = 0; k < PER; k++) {
             const unsigned long long i = t0 + threadIdx.x + (unsigned long long)k * kSplitThreads;
             v[k] = i < n ? in[i] : Tuple{0u, 0u};
-            dr[k] = 0xffffffffu;
-            if (v[k].key) {
-                const uint32_t d = route_of(v[k].key, rt, heavy_sm);
-                if (d != kDrop) dr[k] = (d << 16) | atomicAdd(&cnt[d], 1u);
-            }
+            const uint32_t d = v[k].key ? route_of(v[k].key, rt, heavy_sm) : kDrop;
+            const unsigned act = __ballot_sync(0xffffffffu, d != kDrop);
+            dr[k] = d != kDrop ? (d << 16) | rank_in(cnt, d, act, grouped) : 0xffffffffu;
         }
         __syncthreads();
         for (uint32_t d = threadIdx.x; d < world; d += blockDim.x)
