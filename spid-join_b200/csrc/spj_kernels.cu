@@ -254,18 +254,28 @@ __global__ void __launch_bounds__(kHistThreads) k_hist(PlanDev P) {
         const uint4 *in2 = reinterpret_cast<const uint4 *>(R.in);
         const uint32_t b2i = b >> 1, e2 = e >> 1;
         constexpr int U = 4;
+        // software-pipelined: the next group's loads are in flight while this
+        // group is counted
+        uint4 v[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const uint32_t j = b2i + threadIdx.x + k * blockDim.x;
+            v[k] = j < e2 ? __ldcs(in2 + j) : make_uint4(0, 0, 0, 0);
+        }
         for (uint32_t i = b2i + threadIdx.x; i < e2; i += U * blockDim.x) {
-            uint4 v[U];
+            uint4 nx[U];
 #pragma unroll
             for (int k = 0; k < U; k++) {
-                uint32_t j = i + k * blockDim.x;
-                v[k] = j < e2 ? __ldcs(in2 + j) : make_uint4(0, 0, 0, 0);
+                const uint32_t j = i + (U + k) * blockDim.x;
+                nx[k] = j < e2 ? __ldcs(in2 + j) : make_uint4(0, 0, 0, 0);
             }
 #pragma unroll
             for (int k = 0; k < U; k++) {
                 count(v[k].x, v[k].y);
                 count(v[k].z, v[k].w);
             }
+#pragma unroll
+            for (int k = 0; k < U; k++) v[k] = nx[k];
         }
         if ((e & 1u) && threadIdx.x == 0) {
             const Tuple t = R.in[e - 1];
