@@ -1,0 +1,2 @@
+/* <barrier.h> of the DPU runtime: see dpu_host.h. */
+#include "dpu_host.h"

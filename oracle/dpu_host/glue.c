@@ -1,0 +1,97 @@
+/* glue.c -- the runner's view of one reference kernel's __host variables: its
+ * argument struct set field by field from the runner's integer list (the struct
+ * itself comes from the reference's include/argument.h), and its results read
+ * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BUILD or
+ * -DGLUE_PROBE. Test infrastructure of the oracle only. */
+#include <stdbool.h>
+#include <stdint.h>
+
+#include "dpu_host.h"
+#include "argument.h"
+
+extern dpu_results_t dpu_results;
+
+static int errors_out(int64_t *o) {
+    o[0] = dpu_results.ERROR_TYPE_0;
+    o[1] = dpu_results.ERROR_TYPE_1;
+    o[2] = dpu_results.ERROR_TYPE_2;
+    o[3] = dpu_results.ERROR_TYPE_3;
+    return 4;
+}
+
+#if defined(GLUE_COUNT)
+/* src/dpu/src/join/glb_partition_count.c */
+extern glb_partition_count_arg param_glb_partition_count;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 12) return -1;
+    glb_partition_count_arg *p = &param_glb_partition_count;
+    p->input_type = (int32_t)a[0];
+    p->partition_type = (int32_t)a[1];
+    p->input_offset = (int32_t)a[2];
+    p->elem_num = (int32_t)a[3];
+    p->partition_info_start_byte = (int32_t)a[4];
+    p->histogram_start_byte = (int32_t)a[5];
+    p->partition_num = (int32_t)a[6];
+    p->bankgroup = (int32_t)a[7];
+    p->num_rankgroup = (int32_t)a[8];
+    p->num_rank_in_rankgroup = (int32_t)a[9];
+    p->join_type = (int32_t)a[10];
+    p->hist_interval = (int32_t)a[11];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
+
+#elif defined(GLUE_BUILD)
+/* src/dpu/src/join/a2a_srj_build.c */
+extern hash_phj_build_arg param_phj_build_hash_table;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 7) return -1;
+    hash_phj_build_arg *p = &param_phj_build_hash_table;
+    p->parted_R_offset = (uint32_t)a[0];
+    p->parted_Tid_R_offset = (uint32_t)a[1];
+    p->HT_offset = (uint32_t)a[2];
+    p->parted_R_info_offset = (uint32_t)a[3];
+    p->partition_num = (uint32_t)a[4];
+    p->R_num = (uint32_t)a[5];
+    p->compressed_key = (uint32_t)a[6];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
+
+#elif defined(GLUE_PROBE)
+/* src/dpu/src/join/a2a_srj_probe_inner_mt.c */
+extern hash_phj_probe_arg param_phj_probe_hash_table_inner;
+extern hash_phj_probe_return_arg param_hash_phj_probe_return;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 11) return -1;
+    hash_phj_probe_arg *p = &param_phj_probe_hash_table_inner;
+    p->parted_S_offset = (int32_t)a[0];
+    p->parted_Tid_S_offset = (int32_t)a[1];
+    p->HT_offset = (int32_t)a[2];
+    p->parted_S_info_offset = (int32_t)a[3];
+    p->Result_offset = (int32_t)a[4];
+    p->partition_num = (int32_t)a[5];
+    p->S_num = (int32_t)a[6];
+    p->rank_id = (int32_t)a[7];
+    p->dpu_id = (int32_t)a[8];
+    p->key_table_type = (int32_t)a[9];
+    p->probe_type = (int32_t)a[10];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) {
+    if (cap < 6) return 0;
+    errors_out(o);
+    o[4] = param_hash_phj_probe_return.result_size;
+    o[5] = param_hash_phj_probe_return.miss_count;
+    return 6;
+}
+
+#else
+#error "define GLUE_COUNT, GLUE_BUILD or GLUE_PROBE"
+#endif

@@ -58,6 +58,12 @@ def lib():
         L.orc_generate.restype = i32
         L.orc_generate.argtypes = [ctypes.c_uint64, i64, i64, ctypes.c_double, vp, vp,
                                    ctypes.POINTER(ctypes.c_uint64), i32]
+        L.orc_local_partitions.restype = i64
+        L.orc_local_partitions.argtypes = [i64]
+        L.orc_local_partition.restype = i32
+        L.orc_local_partition.argtypes = [vp, i64, i64, vp, vp]
+        L.orc_dpu_phj.restype = i64
+        L.orc_dpu_phj.argtypes = [vp, i64, vp, i64, vp]
         L.orc_refpipe_dpu_sizes.restype = i32
         L.orc_refpipe_dpu_sizes.argtypes = [vp, i64, vp, i64, i32, i32, i32, i32, vp, vp]
         _lib = L
@@ -188,6 +194,34 @@ def refpipe_dpu_sizes(R, S, ranks=1, rank_sets=1, bank_set=1, nthreads=None):
     if rc:
         raise RuntimeError(ERRORS.get(rc, rc))
     return rs, ss
+
+
+def local_partitions(n_r):
+    """The local partition count one DPU uses for n_r R tuples (2^bitlen(n_r / 1935))."""
+    return int(lib().orc_local_partitions(int(n_r)))
+
+
+def local_partition(tuples, L):
+    """(grouped, offsets): the tuples grouped by local_partition_hash & (L-1),
+    input order kept within a group, and the L+1 group starts."""
+    t = _tuples(tuples)
+    out = np.empty_like(t)
+    off = np.zeros(L + 1, dtype=np.int64)
+    rc = lib().orc_local_partition(_ptr(t), t.shape[0], L, _ptr(out), _ptr(off))
+    if rc:
+        raise RuntimeError(ERRORS.get(rc, rc))
+    return out, off
+
+
+def dpu_phj(R, S):
+    """One DPU's hash join as the oracle restates it: local partitions, a
+    4096-slot linear-probe table per partition, first match per S tuple."""
+    R, S = _tuples(R), _tuples(S)
+    out = np.empty((max(S.shape[0], 1), 2), dtype=np.uint32)
+    m = lib().orc_dpu_phj(_ptr(R), R.shape[0], _ptr(S), S.shape[0], _ptr(out))
+    if m < 0:
+        raise RuntimeError(ERRORS.get(m, m))
+    return out[:m]
 
 
 PRED_NONE, PRED_KEY, PRED_PAYLOAD = 0, 1, 2

@@ -436,6 +436,42 @@ static int dpu_phj(const orc_tuple *r, int64_t nr, const orc_tuple *s, int64_t n
     return rc_err;
 }
 
+/* The local partition count of dpu_phj for nr R tuples. */
+int64_t orc_local_partitions(int64_t nr)
+{
+    int64_t temp = nr / 1935, L = 1;
+    while (temp > 0) { temp >>= 1; L <<= 1; }
+    return L;
+}
+
+/* The layout dpu_phj joins: t grouped by local_partition_hash & (L-1), input
+ * order kept within a group; off[0..L] receives the group starts (L a power of
+ * two). Exported for the checks against the reference's own build and probe
+ * kernels, which take their input in this layout. */
+int orc_local_partition(const orc_tuple *t, int64_t n, int64_t L, orc_tuple *out, int64_t *off)
+{
+    if (L < 1 || (L & (L - 1)) || n < 0) return ORC_E_ARG;
+    const uint32_t mask = (uint32_t)(L - 1);
+    memset(off, 0, (size_t)(L + 1) * sizeof(int64_t));
+    for (int64_t i = 0; i < n; i++) off[(orc_local_partition_hash(t[i].key) & mask) + 1]++;
+    for (int64_t l = 0; l < L; l++) off[l + 1] += off[l];
+    int64_t *cur = (int64_t *)malloc((size_t)L * sizeof(int64_t));
+    if (!cur) return ORC_E_NOMEM;
+    memcpy(cur, off, (size_t)L * sizeof(int64_t));
+    for (int64_t i = 0; i < n; i++) out[cur[orc_local_partition_hash(t[i].key) & mask]++] = t[i];
+    free(cur);
+    return ORC_OK;
+}
+
+/* One DPU's hash join as dpu_phj restates it: the pairs written to out (room
+ * for ns) or an ORC_E_ code. */
+int64_t orc_dpu_phj(const orc_tuple *r, int64_t nr, const orc_tuple *s, int64_t ns, orc_tuple *out)
+{
+    int64_t m = 0;
+    const int rc = dpu_phj(r, nr, s, ns, out, &m);
+    return rc ? rc : m;
+}
+
 static int cmp_key_stable(const void *a, const void *b)
 {
     const orc_tuple *x = (const orc_tuple *)a, *y = (const orc_tuple *)b;

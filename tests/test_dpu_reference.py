@@ -1,0 +1,78 @@
+"""The oracle against the reference's own DPU join kernels, compiled from the
+reference tree as plain C and run on the host (oracle/dpu_ref.py,
+oracle/dpu_host/): the global partition count of src/dpu/src/join/
+glb_partition_count.c and the hash build and probe of a2a_srj_build.c and
+a2a_srj_probe_inner_mt.c must give what the oracle's restatement gives on the
+same inputs. The runners exist only where the reference tree was present when
+the oracle was built; elsewhere these tests are skipped."""
+import numpy as np
+import pytest
+
+import dpu_ref
+
+pytestmark = pytest.mark.skipif(not dpu_ref.available(), reason="reference DPU kernels not built here")
+
+
+def _tuples(rng, n, key_hi=2**32):
+    return np.stack([rng.integers(0, key_hi, n), np.arange(n)], 1).astype(np.uint32).reshape(n, 2)
+
+
+@pytest.mark.parametrize("n", [1, 255, 256, 50001])
+@pytest.mark.parametrize("P,type_,rank_sets,ranks_per_set",
+                         [(64, 0, 1, 1), (1024, 0, 1, 1), (2048, 0, 1, 1), (256, 1, 4, 1), (512, 1, 2, 4),
+                          (1024, 1, 16, 1)])
+def test_partition_count_kernel(oracle, n, P, type_, rank_sets, ranks_per_set):
+    rng = np.random.default_rng(n * 31 + P)
+    T = _tuples(rng, n)
+    T[::37, 0] = 0  # padding is not counted
+    hist, start = dpu_ref.partition_count(T, P, type_, rank_sets, ranks_per_set)
+    want = oracle.partition_count(T, P, type_, rank_sets, ranks_per_set)
+    assert np.array_equal(hist, want)
+    assert np.array_equal(start, (np.cumsum(want) - want).astype(np.uint32))
+    assert int(hist.sum()) == int((T[:, 0] != 0).sum())
+
+
+def _join_both(oracle, R, S):
+    L = oracle.local_partitions(R.shape[0])
+    rg, ro = oracle.local_partition(R, L)
+    sg, so = oracle.local_partition(S, L)
+    return dpu_ref.hash_join(rg, ro, sg, so), oracle.dpu_phj(R, S)
+
+
+@pytest.mark.parametrize("n_r,n_s", [(1, 3), (1935, 4000), (20000, 70000), (1 << 15, 1 << 17)])
+def test_hash_build_probe_kernels_fk(oracle, n_r, n_s):
+    """Unique R keys; S mixes matching keys, keys absent from R and padding:
+    one pair per matching S tuple, (R payload, S payload), nothing else."""
+    rng = np.random.default_rng(n_r + n_s)
+    keys = rng.permutation(np.arange(1, 4 * n_r + 2))[:n_r]
+    R = np.stack([keys, rng.integers(0, 2**32, n_r)], 1).astype(np.uint32)
+    hit = rng.random(n_s) < 0.8
+    S = np.stack([np.where(hit, keys[rng.integers(0, n_r, n_s)], rng.integers(4 * n_r + 2, 2**32, n_s)),
+                  np.arange(n_s)], 1).astype(np.uint32)
+    S[::53, 0] = 0
+    got, restated = _join_both(oracle, R, S)
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(restated))
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
+
+
+def test_hash_build_probe_kernels_generated(oracle):
+    """One DPU's share of the benchmark relations (Zipf 1.0)."""
+    R, S, expect = oracle.generate(1 << 15, 1 << 18, 1.0, seed=0x5EED5EED)
+    got, restated = _join_both(oracle, R, S)
+    assert got.shape == (S.shape[0], 2) and oracle.checksum(got) == expect
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(restated))
+
+
+def test_hash_build_probe_kernels_repeated_r_keys(oracle):
+    """Repeated R keys: the kernels keep every copy and the probe stops at the
+    first one on the key's probe sequence, so each S tuple with a key in R
+    yields exactly one pair joining equal keys, as in the restatement (which
+    copy is first depends on the tasklets' order)."""
+    rng = np.random.default_rng(9)
+    keys = rng.integers(1, 3000, 12000)
+    R = np.stack([keys, np.arange(12000)], 1).astype(np.uint32)
+    S = np.stack([rng.integers(1, 6000, 40000), np.arange(40000)], 1).astype(np.uint32)
+    got, restated = _join_both(oracle, R, S)
+    assert got.shape == restated.shape
+    assert np.array_equal(np.sort(got[:, 1]), np.sort(restated[:, 1]))  # the same S tuples matched
+    assert np.array_equal(R[got[:, 0], 0], S[got[:, 1], 0])              # each pair joins equal keys
