@@ -1,8 +1,8 @@
 /* glue.c -- the runner's view of one reference kernel's __host variables: its
  * argument struct set field by field from the runner's integer list (the struct
  * itself comes from the reference's include/argument.h), and its results read
- * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BUILD or
- * -DGLUE_PROBE. Test infrastructure of the oracle only. */
+ * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BUILD,
+ * -DGLUE_PROBE or -DGLUE_NL. Test infrastructure of the oracle only. */
 #include <stdbool.h>
 #include <stdint.h>
 
@@ -92,6 +92,24 @@ int dpu_host_get_results(int64_t *o, int cap) {
     return 6;
 }
 
+#elif defined(GLUE_NL)
+/* src/dpu/src/join/nested_loop_join.c */
+extern nested_loop_join_arg param_nested_loop_join;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 6) return -1;
+    nested_loop_join_arg *p = &param_nested_loop_join;
+    p->R_packet_start_byte = (int32_t)a[0];
+    p->S_packet_start_byte = (int32_t)a[1];
+    p->R_num_packets = (int32_t)a[2];
+    p->S_num_packets = (int32_t)a[3];
+    p->packet_size = (int32_t)a[4];
+    p->result_start_byte = (int32_t)a[5];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
+
 #else
-#error "define GLUE_COUNT, GLUE_BUILD or GLUE_PROBE"
+#error "define GLUE_COUNT, GLUE_BUILD, GLUE_PROBE or GLUE_NL"
 #endif

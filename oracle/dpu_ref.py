@@ -1,13 +1,14 @@
 """The reference's own DPU join kernels, run on the host.
 
 Test infrastructure only (tests/ imports it, nothing else): ``make -C oracle
-ref`` compiles src/dpu/src/join/glb_partition_count.c, a2a_srj_build.c and
-a2a_srj_probe_inner_mt.c of yonsei-hpcp/spid-join from the reference tree, each
-with its hash.c and the host stand-in for the DPU runtime in oracle/dpu_host/,
-into oracle/_ref/dpu_{count,build,probe}. One call of a runner is one DPU launch
-of 12 tasklets over one MRAM image; this module lays the image out, passes the
-kernel's arguments and reads its results back, so that the oracle's
-restatement of those kernels can be checked against the kernels themselves.
+ref`` compiles glb_partition_count.c, a2a_srj_build.c, a2a_srj_probe_inner_mt.c
+and nested_loop_join.c (src/dpu/src/join/ of yonsei-hpcp/spid-join) from the
+reference tree, each with the reference's hash.c and the host stand-in for the
+DPU runtime in oracle/dpu_host/, into oracle/_ref/dpu_{count,build,probe,nl}.
+One call of a runner is one DPU launch of 12 tasklets over one MRAM image; this
+module lays the image out, passes the kernel's arguments and reads its results
+back, so that the oracle's restatement of those kernels can be checked against
+the kernels themselves.
 """
 import os
 import struct
@@ -16,7 +17,7 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k) for k in ("count", "build", "probe")}
+RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k) for k in ("count", "build", "probe", "nl")}
 TASKLETS = 12              # NR_TASKLETS of every join kernel
 TABLE_BYTES = 32768        # one local partition's hash table (a2a_srj_build.c: 4096 x 8 B)
 JOIN_TYPE_EQUI = 1         # include/argument.h
@@ -109,3 +110,21 @@ def hash_join(r_grouped, r_off, s_grouped, s_off):
         raise RuntimeError(f"dpu_probe reported errors {res[:4]}")
     m = int(res[4])
     return img[res_at:res_at + 8 * m].view(np.uint32).reshape(m, 2).copy()
+
+
+def nested_loop(R, S):
+    """nested_loop_join.c on one DPU: S rewritten in place, each S tuple whose
+    key equals an R key taking that R tuple's payload as its key (R in order,
+    blocks of 256 tuples, three blocks at a time), the others unchanged.
+    Returns the n_s rewritten S tuples. Quadratic: keep the relations small."""
+    R = np.ascontiguousarray(R, dtype=np.uint32).reshape(-1, 2)
+    S = np.ascontiguousarray(S, dtype=np.uint32).reshape(-1, 2)
+    n_r, n_s = R.shape[0], S.shape[0]
+    r_at = 0
+    s_at = _align(n_r * 8, 3 * 2048) + 3 * 2048  # whole groups of three R blocks are read
+    res_at = s_at + _align(n_s * 8, 12 * 2048) + 12 * 2048
+    mram = np.zeros(res_at + _align(n_s * 8, 12 * 2048) + 12 * 2048, dtype=np.uint8)
+    _put(mram, r_at, R)
+    _put(mram, s_at, S)
+    _, img = launch("nl", [r_at, s_at, n_r, n_s, 8, res_at], mram)
+    return img[res_at:res_at + 8 * n_s].view(np.uint32).reshape(n_s, 2).copy()

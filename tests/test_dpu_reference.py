@@ -76,3 +76,35 @@ def test_hash_build_probe_kernels_repeated_r_keys(oracle):
     assert got.shape == restated.shape
     assert np.array_equal(np.sort(got[:, 1]), np.sort(restated[:, 1]))  # the same S tuples matched
     assert np.array_equal(R[got[:, 0], 0], S[got[:, 1], 0])              # each pair joins equal keys
+
+
+@pytest.mark.parametrize("n_r,n_s", [(1, 5), (256, 257), (700, 3000), (2000, 2500)])
+def test_nested_loop_kernel(oracle, n_r, n_s):
+    """nested_loop_join.c rewrites S in place: a matched tuple becomes (R
+    payload, S payload) from the first equal R key in R order, an unmatched one
+    stays. With R payloads that are no R key, that is the oracle's nested-loop
+    output, in S order; repeated R keys included."""
+    rng = np.random.default_rng(n_r * 3 + n_s)
+    keys = rng.integers(1, 3 * n_r + 2, n_r)  # repeats allowed
+    R = np.stack([keys, rng.integers(2**31, 2**32, n_r)], 1).astype(np.uint32)
+    S = np.stack([np.where(rng.random(n_s) < 0.7, keys[rng.integers(0, n_r, n_s)],
+                           rng.integers(3 * n_r + 2, 2**31, n_s)), np.arange(n_s)], 1).astype(np.uint32)
+    got = dpu_ref.nested_loop(R, S)
+    assert np.array_equal(got, oracle.simple_join(R, S, keep_unmatched=True))
+
+
+def test_nested_loop_kernel_rewrites_again(oracle):
+    """The quirk the oracle's restatement leaves out (and says so): the kernel
+    keeps comparing a rewritten key with the later R blocks, so when a matched
+    R tuple's payload equals a key further down R the S tuple is rewritten a
+    second time. Only those S tuples differ from the single rewrite."""
+    R = np.zeros((1000, 2), dtype=np.uint32)
+    R[:, 0] = np.arange(1, 1001)
+    R[:, 1] = np.arange(1, 1001) + 5000
+    R[3] = (4, 999)      # block 0: payload 999 is the key of R[998], three blocks later
+    R[998] = (999, 77)
+    S = np.array([[4, 0], [5, 1], [999, 2]], dtype=np.uint32)
+    got = dpu_ref.nested_loop(R, S)
+    want = oracle.simple_join(R, S, keep_unmatched=True)
+    assert want.tolist() == [[999, 0], [5005, 1], [77, 2]]
+    assert got.tolist() == [[77, 0], [5005, 1], [77, 2]]
