@@ -333,3 +333,55 @@ def test_planner_non_partitioned_up_to_2_22(spj, oracle, n_r, alg_run):
         got = out[:k].cpu().numpy().view(np.uint32)
         assert same_multiset(oracle, got, oracle.simple_join_mt(R, S))
     plan.close()
+
+
+def _join_hash2_np(keys):
+    """join_hash2 of the reference (src/dpu/src/hash.c:85-112), vectorised."""
+    k = np.asarray(keys, dtype=np.uint64)
+    m = np.uint64(0xFFFFFFFF)
+    h = np.zeros_like(k)
+    for b in range(4):
+        h = (h + ((k >> np.uint64(8 * b)) & np.uint64(0xFF))) & m
+        h = (h + (h << np.uint64(10))) & m
+        h = h ^ (h >> np.uint64(6))
+    h = (h + (h << np.uint64(3))) & m
+    h = h ^ (h >> np.uint64(11))
+    h = (h + (h << np.uint64(15))) & m
+    return h.astype(np.uint32)
+
+
+def test_non_partitioned_clustered_keys(spj, oracle):
+    """Every R key of a non-partitioned join alone has its home slot in the
+    first quarter of the table (12000 keys for 8192 slots), so the linear probe
+    runs far past the home slots and wraps their cluster into the rest of the
+    table; the join must still equal the oracle's, repeated keys and misses
+    included."""
+    import torch
+    cand = np.arange(1, 200000, dtype=np.uint32)
+    assert oracle.hashes(cand[:4])[:, 3].tolist() == _join_hash2_np(cand[:4]).tolist()
+    home = _join_hash2_np(cand) & np.uint32((1 << 15) - 1)  # the planner's table: 2^15 slots for 12000 R
+    keys = cand[(home >> 13) == 0][:12000]
+    assert keys.shape[0] == 12000
+    rng = np.random.default_rng(17)
+    R = np.stack([keys, rng.choice(2**31, 12000, replace=False)], 1).astype(np.uint32)  # distinct payloads
+    R[::50, 0] = R[1::50, 0]  # some repeated keys (one match per S tuple)
+    S = np.stack([np.concatenate([keys[rng.integers(0, 12000, 30000)], rng.integers(200000, 2**31, 5000)]),
+                  np.arange(35000)], 1).astype(np.uint32)
+    plan = spj.Plan(R.shape[0], S.shape[0], spj.make_design(rank_num=1))
+    dR = torch.from_numpy(R.view(np.int32)).cuda()
+    dS = torch.from_numpy(S.view(np.int32)).cuda()
+    out = torch.empty((plan.output_capacity, 2), dtype=torch.int32, device="cuda")
+    n = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        plan.execute(dR.data_ptr(), dS.data_ptr(), out.data_ptr(), n.data_ptr())
+        torch.cuda.synchronize()
+        assert plan.stats()["join_alg"] == 1
+        got = out[:int(n.item())].cpu().numpy().view(np.uint32)
+        want = oracle.simple_join(R, S)
+        assert got.shape == want.shape
+        assert np.array_equal(np.sort(got[:, 1]), np.sort(want[:, 1]))  # the same S tuples matched
+        by_pay = np.argsort(R[:, 1])                                     # R payloads are distinct
+        r_of = by_pay[np.searchsorted(R[by_pay, 1], got[:, 0])]
+        assert np.array_equal(R[r_of, 1], got[:, 0])                     # the pair's R payload exists
+        assert np.array_equal(R[r_of, 0], S[got[:, 1], 0])               # and joins equal keys
+    plan.close()
