@@ -51,7 +51,21 @@ def test_noalloc_matches_plan_execute_on_consecutive_calls(spj, oracle):
         got = _noalloc_join(spj, dR, dS, n_r, n_s)
         assert got.shape == want.shape == (n_s, 2)
         assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(want))
+        assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
         assert oracle.checksum(got) == expect
+
+
+def test_noalloc_non_fk_against_oracle(spj, oracle):
+    """S keys absent from R, padding (key 0) in both relations, repeated S keys:
+    the pairs equal the oracle's independent join."""
+    rng = np.random.default_rng(23)
+    n_r, n_s = 300000, (1 << 21) - 5
+    R = np.stack([rng.permutation(np.arange(1, 2 * n_r + 1))[:n_r], rng.integers(0, 2**32, n_r)],
+                 1).astype(np.uint32)
+    R[::101, 0] = 0
+    S = np.stack([rng.integers(0, 3 * n_r, n_s), np.arange(n_s)], 1).astype(np.uint32)
+    got = _noalloc_join(spj, _device(R), _device(S), n_r, n_s)
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
 
 
 def test_noalloc_rejects_sizes_over_its_limit(spj):
