@@ -15,6 +15,10 @@ Workloads: c1, c2 (default), c3, their uniform/skewed twins, c4 (batched), c5
 (served stream); `--alg` picks the local join (0 hash, 1 non-partitioned hash,
 2 sort-merge, 3 nested loop), `--groups G` the replication groups (-r G -R G
 -B 1), `--skew 1` fixed instead of adaptive replication.
+The default c2 line also carries three comparisons on the same GPU, every leg
+checked (`--no-extra` skips them): `skew` (the c2 shape uniform against Zipf
+1.5), `batched` (config 4 as one batch against one plan per join) and
+`sort_merge` (config 3 with the sort-merge against the hash local join).
 `--impl reference` times the reference's algorithm restated on the host cores
 (the oracle's pipeline restatement; the UPMEM original cannot run here).
 """
@@ -428,8 +432,8 @@ def run_ours(args):
     del hR, hS
 
     # the north-star comparisons on the same GPU: the C2 shape at Zipf 1.5
-    # against uniform, and the batched form of config 4 against one plain join
-    # per join (every join checked)
+    # against uniform, the batched form of config 4 against one plain join per
+    # join (every join checked), and config 3's sort-merge against its hash join
     extra = {}
     if rank == 0 and ws == 1 and args.workload == "c2" and not args.no_extra:
         k = max(3, min(args.steps, 10))
@@ -444,6 +448,21 @@ def run_ours(args):
             "heavy_keys": {"uniform": uni["stats"]["heavy_keys"], "zipf_1_5": z15["stats"]["heavy_keys"]},
             "clocks": {"uniform": uni["clocks"], "zipf_1_5": z15["clocks"]}}
         extra["batched"] = batched_compare(spj, args, steps=max(3, min(args.steps, 5)), warmup=3)
+        # config 3 with the sort-merge local join against the hash join (both checked)
+        import copy
+        n3r, n3s, z3, lay3, _ = WORKLOADS["c3"]
+        legs = {}
+        for name, alg in (("hash", 0), ("sort_merge", 2)):
+            a = copy.copy(args)
+            a.alg = alg
+            legs[name] = device_join_leg(spj, n3r, n3s, z3, lay3, a, k, 3, SEED + 13, True)
+        extra["sort_merge"] = {
+            "workload": f"|R|=2^26 |S|=2^29 Zipf {z3:g}, -r {lay3[0]} -R {lay3[1]} -B {lay3[2]}: sort-merge vs hash join",
+            "hash_ms": legs["hash"]["ms_step"], "sort_merge_ms": legs["sort_merge"]["ms_step"],
+            "sort_merge_vs_hash": legs["sort_merge"]["ms_step"] / legs["hash"]["ms_step"], "target": "<= 1.3",
+            "steps": k, "checked": legs["hash"]["ok"] and legs["sort_merge"]["ok"],
+            "join_alg_run": {n: legs[n]["stats"]["join_alg"] for n in legs},
+            "kernels_ms": {n: legs[n]["kmean"] for n in legs}, "clocks": {n: legs[n]["clocks"] for n in legs}}
 
     if rank == 0:
         line = {
