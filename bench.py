@@ -15,10 +15,11 @@ Workloads: c1, c2 (default), c3, their uniform/skewed twins, c4 (batched), c5
 (served stream); `--alg` picks the local join (0 hash, 1 non-partitioned hash,
 2 sort-merge, 3 nested loop), `--groups G` the replication groups (-r G -R G
 -B 1), `--skew 1` fixed instead of adaptive replication.
-The default c2 line also carries three comparisons on the same GPU, every leg
+The default c2 line also carries, measured on the same GPU with every leg
 checked (`--no-extra` skips them): `skew` (the c2 shape uniform against Zipf
-1.5), `batched` (config 4 as one batch against one plan per join) and
-`sort_merge` (config 3 with the sort-merge against the hash local join).
+1.5), `batched` (config 4 as one batch against one plan per join), `c1` (the
+reference driver's own config 1) and `sort_merge` (config 3 with the sort-merge
+against the hash local join).
 `--impl reference` times the reference's algorithm restated on the host cores
 (the oracle's pipeline restatement; the UPMEM original cannot run here).
 """
@@ -456,6 +457,15 @@ def run_ours(args):
             a = copy.copy(args)
             a.alg = alg
             legs[name] = device_join_leg(spj, n3r, n3s, z3, lay3, a, k, 3, SEED + 13, True)
+        # config 1, the reference driver's own case (-s 1048576 -t 2), as the planner runs it
+        n1r, n1s, z1, lay1, _ = WORKLOADS["c1"]
+        c1 = device_join_leg(spj, n1r, n1s, z1, lay1, args, max(20, args.steps), 5, SEED + 14, True)
+        b1 = 24 * (n1r + n1s) + 8 * c1["n_pairs"]
+        extra["c1"] = {"workload": WORKLOADS["c1"][4], "ms_per_step": c1["ms_step"],
+                       "value": (n1r + n1s) / (c1["ms_step"] / 1e3), "unit": "tuples/s", "checked": c1["ok"],
+                       "join_alg_run": c1["stats"]["join_alg"],
+                       "pipeline_roofline": {"frac": b1 / (c1["ms_step"] / 1e3) / 1e9 / peak, "peak": peak},
+                       "kernels_ms": c1["kmean"], "clocks": c1["clocks"]}
         extra["sort_merge"] = {
             "workload": f"|R|=2^26 |S|=2^29 Zipf {z3:g}, -r {lay3[0]} -R {lay3[1]} -B {lay3[2]}: sort-merge vs hash join",
             "hash_ms": legs["hash"]["ms_step"], "sort_merge_ms": legs["sort_merge"]["ms_step"],
