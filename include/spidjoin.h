@@ -396,7 +396,13 @@ int spj_exchange_scatter(const spj_kv_pair_t *tuples, int64_t n, int world, int 
  * *pairs receives a device pointer to this rank's *n_pairs output pairs, owned by
  * the handle and valid until its next join or its destruction; synchronises with
  * `stream`. spj_dist_heavy_keys: the heavy keys of the last join (returns their
- * number, copies at most `capacity` of them). */
+ * number, copies at most `capacity` of them).
+ *
+ * Failures: a call that fails on one rank returns there, while the other ranks
+ * may already wait in a collective of the same call, and NCCL has no timeout of
+ * its own. spj_dist_abort (from any thread, e.g. a watchdog that learns of the
+ * failure) aborts the rank's communicator: its pending collectives end with an
+ * error, later joins return SPJ_E_STATE, and the handle can only be destroyed. */
 typedef struct spj_dist spj_dist_t;
 int spj_dist_unique_id(void *id_out);
 int spj_dist_create(const void *unique_id, int world, int rank, const spj_design_t *design, spj_dist_t **out);
@@ -404,6 +410,7 @@ int spj_dist_set_heavy(spj_dist_t *d, int mode, double heavy_share, int sample);
 int spj_dist_join(spj_dist_t *d, const spj_kv_pair_t *r, int64_t n_r, const spj_kv_pair_t *s, int64_t n_s,
                   const spj_kv_pair_t **pairs, int64_t *n_pairs, void *stream);
 int spj_dist_heavy_keys(const spj_dist_t *d, uint32_t *keys, int capacity);
+int spj_dist_abort(spj_dist_t *d);
 void spj_dist_destroy(spj_dist_t *d);
 
 /* Histogram of glb_partition_hash(key) & (2^bits - 1) over a device column (key-0

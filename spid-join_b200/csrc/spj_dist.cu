@@ -45,6 +45,7 @@ struct Nccl {
     ncclResult_t (*GetUniqueId)(ncclUniqueId *) = nullptr;
     ncclResult_t (*CommInitRank)(ncclComm_t *, int, ncclUniqueId, int) = nullptr;
     ncclResult_t (*CommDestroy)(ncclComm_t) = nullptr;
+    ncclResult_t (*CommAbort)(ncclComm_t) = nullptr;
     ncclResult_t (*AllGather)(const void *, void *, size_t, ncclDataType_t, ncclComm_t, cudaStream_t) = nullptr;
     ncclResult_t (*Send)(const void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
     ncclResult_t (*Recv)(void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
@@ -72,6 +73,7 @@ Nccl &nccl() {
         n.GetUniqueId = (decltype(n.GetUniqueId))sym("ncclGetUniqueId");
         n.CommInitRank = (decltype(n.CommInitRank))sym("ncclCommInitRank");
         n.CommDestroy = (decltype(n.CommDestroy))sym("ncclCommDestroy");
+        n.CommAbort = (decltype(n.CommAbort))sym("ncclCommAbort");
         n.AllGather = (decltype(n.AllGather))sym("ncclAllGather");
         n.Send = (decltype(n.Send))sym("ncclSend");
         n.Recv = (decltype(n.Recv))sym("ncclRecv");
@@ -368,6 +370,7 @@ int spj_dist_join(spj_dist_t *d, const spj_kv_pair_t *r, int64_t n_r, const spj_
                   const spj_kv_pair_t **pairs, int64_t *n_pairs, void *stream) {
     if (!d || !pairs || !n_pairs || n_r < 0 || n_s < 0 || (n_r && !r) || (n_s && !s))
         return set_error(SPJ_E_ARG, "bad sharded-join arguments");
+    if (!d->comm) return set_error(SPJ_E_STATE, "the communicator was aborted");
     if (((uintptr_t)r & 15) || ((uintptr_t)s & 15)) return set_error(SPJ_E_ARG, "shards must be 16-byte aligned");
     if (n_r >= kMaxTuples || n_s >= kMaxTuples) return set_error(SPJ_E_ARG, "shard sizes must stay below 2^32 - 2^24");
     cudaStream_t st = (cudaStream_t)stream;
@@ -416,6 +419,14 @@ int spj_dist_join(spj_dist_t *d, const spj_kv_pair_t *r, int64_t n_r, const spj_
     *pairs = outp;
     *n_pairs = n;
     return SPJ_OK;
+}
+
+int spj_dist_abort(spj_dist_t *d) {
+    if (!d) return set_error(SPJ_E_ARG, "NULL handle");
+    if (!d->comm) return SPJ_OK;  // aborted already
+    const ncclResult_t r = nccl().CommAbort(d->comm);
+    d->comm = nullptr;
+    return r == ncclSuccess ? SPJ_OK : nccl_error(r, "ncclCommAbort");
 }
 
 int spj_dist_heavy_keys(const spj_dist_t *d, uint32_t *keys, int capacity) {

@@ -36,7 +36,7 @@ EXPORTS = (
     "spj_server_reset_stats", "spj_server_destroy", "spj_server_hold", "spj_exchange_split",
     "spj_tuning_set", "spj_tuning_get", "spj_exchange_count", "spj_exchange_scatter", "spj_select",
     "spj_dist_unique_id", "spj_dist_create", "spj_dist_set_heavy", "spj_dist_join", "spj_dist_heavy_keys",
-    "spj_dist_destroy",
+    "spj_dist_destroy", "spj_dist_abort",
 )
 
 
@@ -176,6 +176,7 @@ def lib():
         L.spj_dist_set_heavy.argtypes = [vp, i32, ctypes.c_double, i32]
         L.spj_dist_join.argtypes = [vp, vp, i64, vp, i64, ctypes.POINTER(vp), ctypes.POINTER(i64), vp]
         L.spj_dist_heavy_keys.argtypes = [vp, vp, i32]
+        L.spj_dist_abort.argtypes = [vp]
         L.spj_dist_destroy.argtypes = [vp]
         L.spj_dist_destroy.restype = None
         L.spj_tuning_set.argtypes = [ctypes.POINTER(Tuning), i32]
@@ -694,6 +695,11 @@ class ShardedJoin:
         if n.value == 0:
             return torch.empty((0, 2), dtype=torch.int32, device=R.device), 0
         return torch.as_tensor(_DeviceView(pp.value, n.value), device=R.device), n.value
+
+    def abort(self):
+        """Aborts the communicator (callable from another thread): this rank's
+        pending collectives end with an error; the handle can then only be closed."""
+        check(lib().spj_dist_abort(self.h))
 
     @property
     def last_heavy(self):

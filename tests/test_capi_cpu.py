@@ -57,6 +57,7 @@ def test_sharded_join_argument_checks(spj):
     assert L.spj_dist_create(None, 1, 0, ctypes.byref(d), ctypes.byref(h)) == -1
     assert L.spj_dist_set_heavy(None, 1, 0.25, 1024) == -1
     assert L.spj_dist_heavy_keys(None, None, 0) == 0
+    assert L.spj_dist_abort(None) == -1
     L.spj_dist_destroy(None)
 
 
