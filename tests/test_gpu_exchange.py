@@ -212,3 +212,20 @@ def test_sharded_join_native_ragged_and_empty(spj, oracle):
         assert n == want.shape[0]
         assert np.array_equal(oracle.sort_pairs(pairs.cpu().numpy().view(np.uint32)), want)
     sj.close()
+
+
+def test_sharded_join_native_abort(spj):
+    """After spj_dist_abort the handle refuses joins (SPJ_E_STATE) and can still
+    be destroyed; a world of one has no peer to wait for."""
+    import torch
+    sj = spj.ShardedJoin(world=1, rank=0)
+    R, S, _ = spj.generate_host(4096, 8192, 0.0, seed=3)
+    dR = torch.from_numpy(R.view(np.int32)).cuda()
+    dS = torch.from_numpy(S.view(np.int32)).cuda()
+    _, n = sj.run(dR, dS)
+    assert n == 8192
+    sj.abort()
+    sj.abort()  # a second abort is a no-op
+    with pytest.raises(spj.SpjError, match="STATE"):
+        sj.run(dR, dS)
+    sj.close()
