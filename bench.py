@@ -432,7 +432,7 @@ def run_ours(args):
         del R, S
     del hR, hS
 
-    # the north-star comparisons on the same GPU: the C2 shape at Zipf 1.5
+    # the target comparisons on the same GPU: the C2 shape at Zipf 1.5
     # against uniform, the batched form of config 4 against one plain join per
     # join (every join checked), and config 3's sort-merge against its hash join
     extra = {}
