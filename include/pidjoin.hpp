@@ -154,12 +154,40 @@ public:
     // StartJoin). With caller_owned, each rank's pairs are copied into its own
     // aligned_alloc'd buffer that the caller releases with free(), as the
     // reference hands out its result buffers (src/queryHostFunc.cc:1089).
-    ResultBuffers_t FinishJoin(bool caller_owned = false) {
+    //
+    // With dpu_blocks (implies caller_owned), each rank's buffer has the
+    // reference's transfer layout instead (src/queryHostFunc.cc:1058-1126 over
+    // the blocks src/dpu/src/join/finish_join.c:99-129 pads): 64 blocks of one
+    // size, each holding its pairs followed by (0,0) padding, and the byte size
+    // reported is that of the 64 padded blocks. The rank's pairs are dealt to
+    // the blocks in order and evenly (block b takes pairs / 64 of them, one more
+    // for the first pairs % 64 blocks; blocks hold ceil(pairs / 64)): this join
+    // has no DPUs, so which pair lands in which block carries no meaning. As in
+    // the reference, a (0,0) pair of the join itself cannot be told from padding.
+    ResultBuffers_t FinishJoin(bool caller_owned = false, bool dpu_blocks = false) {
         check(spj_finish(h_, &last_), "FinishJoin");
         ResultBuffers_t out;
         for (int r = 0; r < last_.num_rank; r++) {
-            const int64_t bytes = 8 * (last_.rank_offsets[r + 1] - last_.rank_offsets[r]);
+            const int64_t n = last_.rank_offsets[r + 1] - last_.rank_offsets[r];
+            const int64_t bytes = 8 * n;
             kv_pair_t *src = const_cast<kv_pair_t *>(last_.pairs) + last_.rank_offsets[r];
+            if (dpu_blocks) {
+                constexpr int64_t kBlocks = 64;  // DPUs per rank (NUM_DPU_RANK)
+                const int64_t per = (n + kBlocks - 1) / kBlocks;
+                const int64_t padded = kBlocks * per * 8;
+                kv_pair_t *dst = (kv_pair_t *)aligned_alloc(64, (size_t)((padded + 63) / 64 * 64 + 64));
+                if (!dst) throw Error(SPJ_E_NOMEM, "FinishJoin: result buffer allocation failed");
+                memset(dst, 0, (size_t)padded);
+                const int64_t base = n / kBlocks, extra = n % kBlocks;
+                for (int64_t b = 0, lo = 0; b < kBlocks; b++) {
+                    const int64_t cnt = base + (b < extra ? 1 : 0);
+                    if (cnt) memcpy(dst + b * per, src + lo, (size_t)cnt * 8);
+                    lo += cnt;
+                }
+                out.first.push_back(dst);
+                out.second.push_back(padded);
+                continue;
+            }
             if (caller_owned) {
                 kv_pair_t *dst = (kv_pair_t *)aligned_alloc(64, (size_t)((bytes + 63) / 64 * 64 + 64));
                 if (!dst) throw Error(SPJ_E_NOMEM, "FinishJoin: result buffer allocation failed");

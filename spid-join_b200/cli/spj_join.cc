@@ -2,15 +2,18 @@
 // reference's driver (test/join/main.cc:73-118):
 //   -s input_size (|R|)  -r rank_num  -z zipf_factor (Zipf exponent x 100)
 //   -t rs_ratio (|S|/|R|)  -R rank_set  -B bank_set
-// plus -a algorithm (phj|nphj|smj|nl), -n repetitions and -S seed. -h, -p and
-// -f take an argument and are ignored, as in the reference.
+// plus -a algorithm (phj|nphj|smj|nl), -n repetitions, -S seed, -o (result
+// buffers owned by the caller) and -P (the reference's padded per-rank layout of
+// 64 DPU blocks; implies -o). -h, -p and -f take an argument and are ignored, as
+// in the reference.
 //
 // With -z 0 the relations are the reference driver's (test/join/main.cc:33-43):
 // R[i] = (i+1, i+3) and S[i] = (i/ratio + 1, i/ratio + 3). With -z > 0 the
 // reference reads pre-generated files; here S keys are drawn Zipf(z/100) over
 // a seeded shuffle of R's keys by spj_generate_host. The output is checked by
-// count and by the order-independent 64-bit checksum; the exit status is 0
-// when it matches, 1 when it does not and 2 on an error.
+// count and by the order-independent 64-bit checksum (with -P over the non-(0,0)
+// pairs, which needs an output without a (0,0) pair of its own, as -z 0's is);
+// the exit status is 0 when it matches, 1 when it does not and 2 on an error.
 #include <getopt.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -31,9 +34,15 @@ static uint64_t splitmix64(uint64_t x) {
     return x ^ (x >> 31);
 }
 
-static uint64_t pair_sum(const kv_pair_t *p, int64_t n) {
+static uint64_t pair_sum(const kv_pair_t *p, int64_t n, bool skip_zero, int64_t *counted) {
     uint64_t s = 0;
-    for (int64_t i = 0; i < n; i++) s += splitmix64((uint64_t)p[i].lvalue << 32 | p[i].rvalue);
+    int64_t c = 0;
+    for (int64_t i = 0; i < n; i++) {
+        if (skip_zero && p[i].lvalue == 0 && p[i].rvalue == 0) continue;  // block padding
+        s += splitmix64((uint64_t)p[i].lvalue << 32 | p[i].rvalue);
+        c++;
+    }
+    *counted = c;
     return s;
 }
 
@@ -44,14 +53,15 @@ int main(int argc, char **argv) {
     std::string alg = "phj";
     int reps = 1;
     bool owned = false;  // -o: result buffers owned by the caller, as the reference hands them out
+    bool padded = false; // -P: the reference's transfer layout, 64 zero-padded DPU blocks per rank
     uint64_t seed = 0x5EED5EEDull;
     if (argc < 2) {
         fprintf(stderr, "usage: %s -s |R| [-r ranks] [-z zipf*100] [-t |S|/|R|] [-R rank_set] [-B bank_set] "
-                        "[-a phj|nphj|smj|nl] [-n reps] [-S seed] [-o]\n", argv[0]);
+                        "[-a phj|nphj|smj|nl] [-n reps] [-S seed] [-o] [-P]\n", argv[0]);
         return 0;
     }
     int opt;
-    while ((opt = getopt(argc, argv, "s:r:z:t:R:B:h:p:f:a:n:S:o")) != -1) {
+    while ((opt = getopt(argc, argv, "s:r:z:t:R:B:h:p:f:a:n:S:oP")) != -1) {
         switch (opt) {
             case 's': d.input_size = atoll(optarg); break;
             case 'r': d.rank_num = atoi(optarg); break;
@@ -63,6 +73,7 @@ int main(int argc, char **argv) {
             case 'n': reps = atoi(optarg); break;
             case 'S': seed = strtoull(optarg, nullptr, 0); break;
             case 'o': owned = true; break;
+            case 'P': padded = owned = true; break;
             default: break;
         }
     }
@@ -102,14 +113,17 @@ int main(int argc, char **argv) {
             struct timespec start;
             clock_gettime(CLOCK_MONOTONIC, &start);
             join_instance.StartJoin(d);
-            ResultBuffers_t res = join_instance.FinishJoin(owned);
+            ResultBuffers_t res = join_instance.FinishJoin(owned, padded);
             join_instance.RecordLogs(start, 0);
-            int64_t n = 0;
+            int64_t n = 0, bytes = 0;
             uint64_t sum = 0;
             for (size_t r = 0; r < res.first.size(); r++) {
-                n += res.second[r] / 8;
-                sum += pair_sum(res.first[r], res.second[r] / 8);
+                int64_t c = 0;
+                sum += pair_sum(res.first[r], res.second[r] / 8, padded, &c);
+                n += c;
+                bytes += res.second[r];
             }
+            if (padded) printf("padded layout: %lld bytes in %zu ranks of 64 blocks\n", (long long)bytes, res.first.size());
             const bool ok = n == n_s && sum == expect;
             printf("check: %s pairs=%lld expected=%lld checksum=%016llx expected=%016llx\n", ok ? "ok" : "MISMATCH",
                    (long long)n, (long long)n_s, (unsigned long long)sum, (unsigned long long)expect);

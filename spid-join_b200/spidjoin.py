@@ -232,6 +232,21 @@ class ResultBuffers:
         return np.concatenate(self.buffers) if self.buffers else np.zeros((0, 2), np.uint32)
 
 
+def _dpu_blocks(pairs, blocks=64):
+    """One rank's pairs in the reference's transfer layout: `blocks` blocks of
+    ceil(n / blocks) pairs, the pairs dealt evenly in order, (0, 0) padding."""
+    n = pairs.shape[0]
+    per = -(-n // blocks)
+    out = np.zeros((blocks * per, 2), dtype=np.uint32)
+    base, extra = divmod(n, blocks)
+    lo = 0
+    for b in range(blocks):
+        cnt = base + (1 if b < extra else 0)
+        out[b * per:b * per + cnt] = pairs[lo:lo + cnt]
+        lo += cnt
+    return out
+
+
 class JoinInstance:
     """pidjoin::JoinInstance on one B200 (include/join_internals.hpp:301-323)."""
 
@@ -262,7 +277,10 @@ class JoinInstance:
     def StartJoin(self, design=None):
         check(lib().spj_start(self._h, ctypes.byref(design) if design is not None else None))
 
-    def FinishJoin(self, copy=True):
+    def FinishJoin(self, copy=True, dpu_blocks=False):
+        """Per-rank buffers. dpu_blocks: the reference's transfer layout, 64
+        blocks of ceil(pairs / 64) per rank, the rank's pairs dealt evenly in
+        order, each block padded with (0, 0) (as pidjoin.hpp's FinishJoin)."""
         res = Result()
         check(lib().spj_finish(self._h, ctypes.byref(res)))
         n = res.n_pairs
@@ -275,6 +293,9 @@ class JoinInstance:
             flat = flat.copy()
         offs = [res.rank_offsets[i] for i in range(res.num_rank + 1)]
         bufs = [flat[offs[i]:offs[i + 1]] for i in range(res.num_rank)]
+        if dpu_blocks:
+            bufs = [_dpu_blocks(b) for b in bufs]
+            return ResultBuffers(bufs, [8 * b.shape[0] for b in bufs])
         return ResultBuffers(bufs, [8 * (offs[i + 1] - offs[i]) for i in range(res.num_rank)])
 
     def RecordLogs(self, print_=False):

@@ -385,3 +385,31 @@ def test_non_partitioned_clustered_keys(spj, oracle):
         assert np.array_equal(R[r_of, 1], got[:, 0])                     # the pair's R payload exists
         assert np.array_equal(R[r_of, 0], S[got[:, 1], 0])               # and joins equal keys
     plan.close()
+
+
+def test_finish_join_dpu_block_layout(spj, oracle):
+    """FinishJoin(dpu_blocks=True): per rank 64 blocks of one size with (0, 0)
+    padding, the reference's transfer layout; its non-padding pairs are the
+    join (the reference driver's inputs have no (0, 0) pair of their own)."""
+    R, S = main_cc_tables(100003, 3)
+    inst = spj.JoinInstance(4, 2, 2)
+    inst.LoadColumn(R, R.shape[0], "left")
+    inst.LoadColumn(S, S.shape[0], "right")
+    d = spj.make_design(rank_num=4, rank_set=2)
+    inst.PrepareJoin(d)
+    inst.StartJoin(d)
+    plain = inst.FinishJoin()
+    inst.StartJoin(d)
+    res = inst.FinishJoin(dpu_blocks=True)
+    inst.close()
+    assert len(res.buffers) == 4
+    # which pairs a rank holds differs between executions (the output order is
+    # free); each rank's count does not
+    for buf, size, ref in zip(res.buffers, res.byte_sizes, plain.buffers):
+        assert size == 8 * buf.shape[0] and buf.shape[0] % 64 == 0
+        assert buf.shape[0] // 64 == -(-ref.shape[0] // 64)
+        blocks = buf.reshape(64, -1, 2)
+        filled = ((blocks[:, :, 0] != 0) | (blocks[:, :, 1] != 0)).sum(1)
+        assert filled.sum() == ref.shape[0] and filled.max() - filled.min() <= 1  # dealt evenly
+    got = np.concatenate([b[(b[:, 0] != 0) | (b[:, 1] != 0)] for b in res.buffers])
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
