@@ -41,3 +41,19 @@ def test_sort_merge_sorted_once_exact(spj, oracle, zipf):
         out = res.pairs()
         assert oracle.checksum(out) == expect
         assert same_multiset(oracle, out, oracle.simple_join(R, S, keep_unmatched=True))
+
+
+def test_sort_merge_bucket_sort_fallback(spj, oracle):
+    """A run's bucket sort spreads its keys over [min, max]; one key near 2^32 in
+    a partition of small keys puts nearly all of them in the first bucket, which
+    makes that run fall back to the merge sort. Runs with and without the
+    fallback give the oracle's keep-unmatched join exactly."""
+    rng = np.random.default_rng(29)
+    n_small = 1 << 18
+    keys = rng.permutation(np.arange(1, n_small + 1)).astype(np.uint64)
+    far = (np.uint64(2**32) - np.arange(1, 4097, dtype=np.uint64))  # one far key in most partitions
+    R = np.stack([np.concatenate([keys, far]), np.arange(n_small + far.size)], 1).astype(np.uint32)
+    sk = np.concatenate([rng.integers(1, 2 * n_small, 1 << 20), far[rng.integers(0, far.size, 1 << 14)]])
+    S = np.stack([sk, np.arange(sk.size)], 1).astype(np.uint32)
+    res, _ = run_instance(spj, R, S, join_alg=2, heavy_sample=-1)
+    assert same_multiset(oracle, res.pairs(), oracle.simple_join(R, S, keep_unmatched=True))
