@@ -38,3 +38,13 @@ def test_cli_padded_layout_sizes():
     assert m, p.stdout
     total, ranks = int(m.group(1)), int(m.group(2))
     assert ranks == 4 and total % 512 == 0 and 8 * n_s <= total < 8 * n_s + ranks * 64 * 8
+
+
+def test_sharded_join_from_cpp():
+    """spj_dist_check: the sharded join's C sequence (NCCL id, create, heavy keys,
+    join twice, destroy) from a C++ program with no Python, on one rank; the
+    pairs match the generator's count and checksum."""
+    exe = os.path.join(os.path.dirname(CLI), "spj_dist_check")
+    p = subprocess.run([exe, str(1 << 18), str(1 << 21), "1.5"], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert p.stdout.count("check: ok") == 2 and "heavy_keys=0" not in p.stdout
