@@ -757,6 +757,41 @@ def batched_compare(spj, args, steps, warmup):
     bad = wrong(plain_outs, n_out)
     if bad:
         raise SystemExit(f"plain join check failed for {bad} joins")
+
+    # plain, back to back: every join's plan created first, then the J executions
+    # on one stream between two events, so the gaps between the joins count too
+    seq = {"how": "one pre-created plan per join, the J executions back to back on one stream, CUDA events "
+                  "around the sequence"}
+    plans = []
+    try:
+        for n_r, n_s, _ in specs:
+            plans.append(spj.Plan(n_r, n_s, design))
+        souts = [outs[j] if outs[j].shape[0] >= plans[j].output_capacity else plain_outs[j] for j in range(J)]
+
+        def run_all():
+            for j in range(J):
+                plans[j].execute(R[j].data_ptr(), S[j].data_ptr(), souts[j].data_ptr(), n_out[j:j + 1].data_ptr(), 0)
+
+        n_out.zero_()
+        run_all()
+        torch.cuda.synchronize()
+        bad = wrong(souts, n_out)
+        if bad:
+            raise SystemExit(f"plain back-to-back check failed for {bad} joins")
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 3
+        a.record()
+        for _ in range(reps):
+            run_all()
+        b.record()
+        torch.cuda.synchronize()
+        seq_ms = a.elapsed_time(b) / reps
+        seq.update({"value": tot / (seq_ms / 1e3), "ms_per_step": seq_ms, "batched_vs_this": seq_ms / ms_batched})
+    except spj.SpjError as e:  # the plans of all joins at once may not fit
+        seq["skipped"] = str(e)
+    finally:
+        for pl in plans:
+            pl.close()
     pipe_bytes = sum(24 * (a + b) + 8 * b for a, b, _ in specs)
     peak, peak_kind = peaks()
     del outs, plain_outs, R, S
@@ -767,6 +802,7 @@ def batched_compare(spj, args, steps, warmup):
             "value": tot / (ms_batched / 1e3), "ms_per_step": ms_batched, "steps": steps,
             "plain": {"value": tot / (plain_ms / 1e3), "ms_per_step": plain_ms,
                       "how": "one pre-created plan per join, CUDA-event device time per execution, summed"},
+            "plain_back_to_back": seq,
             "batched_vs_plain": plain_ms / ms_batched, "target": ">= 3",
             "pipeline_roofline": {"achieved": pipe_bytes / (ms_batched / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                                   "frac": pipe_bytes / (ms_batched / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
