@@ -49,11 +49,16 @@ __device__ __forceinline__ uint32_t find_slot(const uint32_t *prefix, uint32_t n
     return lo;
 }
 
-// Writes the descriptors of a one-join plan from kernel parameters (no host copy).
-// With keep_r, R owns no chunk, partition or coarse bucket of the count and
-// scatter grids (its partitions are reused), and every CTA of them maps to S.
+// Writes the descriptors of a one-join plan from kernel parameters (no host copy)
+// and zeroes the execution's counters (the batch counters and the join's, which
+// lie next to each other: ctr_words 32-bit words), so an execution needs no
+// separate memset. With keep_r, R owns no chunk, partition or coarse bucket of
+// the count and scatter grids (its partitions are reused), and every CTA of them
+// maps to S.
 __global__ void k_init_single(PlanDev P, RelDev r0, RelDev r1, JoinDev j0, uint32_t nch0, uint32_t nch1, uint32_t f,
-                              uint32_t f1, bool keep_r) {
+                              uint32_t f1, bool keep_r, uint32_t ctr_words) {
+    uint32_t *ctr = reinterpret_cast<uint32_t *>(P.bctr);
+    for (uint32_t i = threadIdx.x; i < ctr_words; i += blockDim.x) ctr[i] = 0u;
     if (threadIdx.x != 0) return;
     P.rel[0] = r0;
     P.rel[1] = r1;
@@ -2265,8 +2270,10 @@ cudaError_t init_single(spj_plan *pl, cudaStream_t st, bool keep_r) {
     const JoinHost &h = pl->joins[0];
     const uint32_t f = 1u << h.dev.bits;
     const uint32_t f1 = h.dev.fine_bits ? 1u << (h.dev.bits - h.dev.fine_bits) : 0u;
+    static_assert((sizeof(BatchCtr) + sizeof(JoinCtr)) % 4 == 0, "counters in whole words");
     k_init_single<<<1, 32, 0, st>>>(pl->dev, h.rel[0], h.rel[1], h.dev, h.rel[0].nchunks, h.rel[1].nchunks, f, f1,
-                                    keep_r && h.dev.alg != SPJ_ALG_NPHJ);
+                                    keep_r && h.dev.alg != SPJ_ALG_NPHJ,
+                                    (uint32_t)((sizeof(BatchCtr) + sizeof(JoinCtr)) / 4));
     return cudaGetLastError();
 }
 

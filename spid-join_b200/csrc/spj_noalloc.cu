@@ -155,12 +155,10 @@ extern "C" int spj_join_noalloc(const spj_kv_pair_t *r, int64_t n_r, const spj_k
     if (!h.rel[1].in) h.rel[1].in = h.rel[1].out;
 
     cudaStream_t st = (cudaStream_t)stream;
-    // descriptors written by a kernel from its parameters (no host copy)
+    // descriptors written by a kernel from its parameters (no host copy); the
+    // same kernel zeroes the counters, which the region keeps from the last call
     e = init_single(&pl, st);
     if (e != cudaSuccess) return cuda_error(e, "descriptor kernel");
-    // the region keeps the previous call's contents: the counters must start at zero
-    e = cudaMemsetAsync(pl.dev.bctr, 0, sizeof(BatchCtr) + sizeof(JoinCtr), st);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(counters)");
     e = launch_pipeline(&pl, st);
     if (e != cudaSuccess) return cuda_error(e, "join kernels");
     k_noalloc_status<<<1, 1, 0, st>>>(pl.dev.jctr, reinterpret_cast<long long *>(n_out));

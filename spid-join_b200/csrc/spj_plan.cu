@@ -614,9 +614,8 @@ int plan_execute(spj_plan *pl, const spj_kv_pair_t *r, const spj_kv_pair_t *s, s
     h.rel[1].in = s ? reinterpret_cast<const Tuple *>(s) : reinterpret_cast<const Tuple *>(out);
     h.dev.out = reinterpret_cast<Tuple *>(out);
     h.dev.n_out_user = reinterpret_cast<unsigned long long *>(n_out);
-    cudaError_t e = init_single(pl, st, keep_r);
+    cudaError_t e = init_single(pl, st, keep_r);  // also zeroes the counters
     if (e != cudaSuccess) return cuda_error(e, "descriptor kernel");
-    SPJ_CUDA(cudaMemsetAsync(pl->dev.bctr, 0, sizeof(BatchCtr) + sizeof(JoinCtr), st));
     e = launch_pipeline(pl, st, keep_r);
     if (e != cudaSuccess) return cuda_error(e, "join kernels");
     return SPJ_OK;
