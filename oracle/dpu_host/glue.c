@@ -2,7 +2,7 @@
  * argument struct set field by field from the runner's integer list (the struct
  * itself comes from the reference's include/argument.h), and its results read
  * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BUILD,
- * -DGLUE_PROBE or -DGLUE_NL. Test infrastructure of the oracle only. */
+ * -DGLUE_PROBE, -DGLUE_NL or -DGLUE_LP. Test infrastructure of the oracle only. */
 #include <stdbool.h>
 #include <stdint.h>
 
@@ -110,6 +110,37 @@ int dpu_host_set_args(const int64_t *a, int n) {
 
 int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
 
+#elif defined(GLUE_LP)
+/* src/dpu/src/join/a2a_packetwise_srj_local_partition.c */
+extern packetwise_hash_local_partitioning_arg param_packetwise_local_hash_partitioning;
+extern packetwise_hash_local_partitioning_return_arg param_packetwise_local_hash_partitioning_return;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 12) return -1;
+    packetwise_hash_local_partitioning_arg *p = &param_packetwise_local_hash_partitioning;
+    p->packet_start_byte = (int32_t)a[0];
+    p->generated_local_tid_start_byte = (int32_t)a[1];
+    p->partitioned_result_start_byte = (int32_t)a[2];
+    p->result_partition_info_start_byte = (int32_t)a[3];
+    p->do_calculate_partition_num = (int32_t)a[4];
+    p->shift_val = (int32_t)a[5];
+    p->total_rank = (int32_t)a[6];
+    p->num_packets = (int32_t)a[7];
+    p->tuple_size = (int32_t)a[8];
+    p->packet_size = (int32_t)a[9];
+    p->rank_id = (int32_t)a[10];
+    p->dpu_id = (int32_t)a[11];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) {
+    if (cap < 6) return 0;
+    errors_out(o);
+    o[4] = param_packetwise_local_hash_partitioning_return.elem_num;
+    o[5] = param_packetwise_local_hash_partitioning_return.partition_num;
+    return 6;
+}
+
 #else
-#error "define GLUE_COUNT, GLUE_BUILD, GLUE_PROBE or GLUE_NL"
+#error "define GLUE_COUNT, GLUE_BUILD, GLUE_PROBE, GLUE_NL or GLUE_LP"
 #endif

@@ -1,10 +1,11 @@
 """The reference's own DPU join kernels, run on the host.
 
 Test infrastructure only (tests/ imports it, nothing else): ``make -C oracle
-ref`` compiles glb_partition_count.c, a2a_srj_build.c, a2a_srj_probe_inner_mt.c
-and nested_loop_join.c (src/dpu/src/join/ of yonsei-hpcp/spid-join) from the
-reference tree, each with the reference's hash.c and the host stand-in for the
-DPU runtime in oracle/dpu_host/, into oracle/_ref/dpu_{count,build,probe,nl}.
+ref`` compiles glb_partition_count.c, a2a_packetwise_srj_local_partition.c,
+a2a_srj_build.c, a2a_srj_probe_inner_mt.c and nested_loop_join.c
+(src/dpu/src/join/ of yonsei-hpcp/spid-join) from the reference tree, each with
+the reference's hash.c and the host stand-in for the DPU runtime in
+oracle/dpu_host/, into oracle/_ref/dpu_{count,lp,build,probe,nl}.
 One call of a runner is one DPU launch of 12 tasklets over one MRAM image; this
 module lays the image out, passes the kernel's arguments and reads its results
 back, so that the oracle's restatement of those kernels can be checked against
@@ -17,7 +18,7 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k) for k in ("count", "build", "probe", "nl")}
+RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k) for k in ("count", "build", "probe", "nl", "lp")}
 TASKLETS = 12              # NR_TASKLETS of every join kernel
 TABLE_BYTES = 32768        # one local partition's hash table (a2a_srj_build.c: 4096 x 8 B)
 JOIN_TYPE_EQUI = 1         # include/argument.h
@@ -128,3 +129,28 @@ def nested_loop(R, S):
     _put(mram, s_at, S)
     _, img = launch("nl", [r_at, s_at, n_r, n_s, 8, res_at], mram)
     return img[res_at:res_at + 8 * n_s].view(np.uint32).reshape(n_s, 2).copy()
+
+
+def local_partition(tuples, partitions=0):
+    """a2a_packetwise_srj_local_partition.c on one DPU holding `tuples` (key-0
+    tuples are gaps and are dropped): (grouped tuples, L + 1 partition starts,
+    L). partitions = 0 lets the kernel choose L = 2^bitlen(n / 1935) from its
+    non-gap tuples, as it does for R; S passes R's L. At most 512 partitions
+    (the kernel writes its start offsets back correctly up to that many)."""
+    t = np.ascontiguousarray(tuples, dtype=np.uint32).reshape(-1, 2)
+    n = t.shape[0]
+    if partitions > 512:
+        raise ValueError("at most 512 local partitions")
+    res_at = _align(n * 8) + 2048
+    info_at = res_at + _align(n * 8) + 2048
+    mram = np.zeros(info_at + 32768 + 2048, dtype=np.uint8)
+    _put(mram, 0, t)
+    res, img = launch("lp", [0, 0, res_at, info_at, partitions, 0, 1, n, 8, 8, 0, 0], mram)
+    if any(res[:4]):
+        raise RuntimeError(f"dpu_lp reported errors {res[:4]}")
+    m, L = int(res[4]), int(res[5])
+    if L > 512:
+        raise RuntimeError("more than 512 local partitions")
+    starts = img[info_at:info_at + 4 * L].view(np.uint32).astype(np.int64)
+    grouped = img[res_at:res_at + 8 * m].view(np.uint32).reshape(m, 2).copy()
+    return grouped, np.append(starts, m), L

@@ -1,9 +1,11 @@
 """The oracle against the reference's own DPU join kernels, compiled from the
 reference tree as plain C and run on the host (oracle/dpu_ref.py,
 oracle/dpu_host/): the global partition count of src/dpu/src/join/
-glb_partition_count.c and the hash build and probe of a2a_srj_build.c and
-a2a_srj_probe_inner_mt.c must give what the oracle's restatement gives on the
-same inputs. The runners exist only where the reference tree was present when
+glb_partition_count.c, the local partitioning of
+a2a_packetwise_srj_local_partition.c, the hash build and probe of
+a2a_srj_build.c and a2a_srj_probe_inner_mt.c and the nested loop of
+nested_loop_join.c must give what the oracle's restatement gives on the same
+inputs. The runners exist only where the reference tree was present when
 the oracle was built; elsewhere these tests are skipped."""
 import numpy as np
 import pytest
@@ -108,3 +110,37 @@ def test_nested_loop_kernel_rewrites_again(oracle):
     want = oracle.simple_join(R, S, keep_unmatched=True)
     assert want.tolist() == [[999, 0], [5005, 1], [77, 2]]
     assert got.tolist() == [[77, 0], [5005, 1], [77, 2]]
+
+
+@pytest.mark.parametrize("n,gap", [(1, 0), (1936, 0), (30000, 41), (200000, 7)])
+def test_local_partition_kernel(oracle, n, gap):
+    """a2a_packetwise_srj_local_partition.c: L = 2^bitlen(n / 1935) from the
+    non-gap tuples, the start offsets and every partition's tuples equal the
+    oracle's local partitioning (the order inside a partition is the tasklets')."""
+    rng = np.random.default_rng(n + gap)
+    T = np.stack([rng.permutation(np.arange(1, 4 * n + 2))[:n], rng.integers(0, 2**32, n)], 1).astype(np.uint32)
+    if gap:
+        T[::gap, 0] = 0  # key 0: gaps between packets, dropped
+    got, starts, L = dpu_ref.local_partition(T)
+    nz = T[T[:, 0] != 0]
+    assert L == oracle.local_partitions(nz.shape[0])
+    want, off = oracle.local_partition(nz, L)
+    assert np.array_equal(starts, off)
+    for p in range(L):
+        assert np.array_equal(oracle.sort_pairs(got[starts[p]:starts[p + 1]]),
+                              oracle.sort_pairs(want[off[p]:off[p + 1]]))
+
+
+def test_reference_kernels_chained_join(oracle):
+    """One DPU's hash join by the reference's kernels alone: local partitioning
+    of R (which picks L) and of S (with R's L), then build and probe. The pairs
+    equal the oracle's per-DPU join and its independent join."""
+    R, S, _ = oracle.generate(60000, 240000, 1.0, seed=7)
+    S = S.copy()
+    S[::97, 0] = 0  # gaps in S's packets
+    rg, ro, L = dpu_ref.local_partition(R)
+    sg, so, Ls = dpu_ref.local_partition(S, partitions=L)
+    assert Ls == L
+    got = dpu_ref.hash_join(rg, ro, sg, so)
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.dpu_phj(R, S)))
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
