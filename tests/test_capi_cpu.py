@@ -130,3 +130,20 @@ def test_tuning_table_roundtrip(spj):
     finally:
         spj.set_tuning([])
     assert spj.get_tuning() == []
+
+
+@pytest.mark.parametrize("n", [0, 1, 63, 64, 65, 130])
+def test_dpu_block_layout(spj, n):
+    """The reference's transfer layout of one rank's pairs: 64 blocks of
+    ceil(n / 64) pairs, the pairs dealt evenly in order (block sizes differ by
+    at most one), each block padded with (0, 0)."""
+    pairs = (np.arange(2 * n, dtype=np.uint32).reshape(n, 2) + 1)
+    out = spj._dpu_blocks(pairs)
+    per = -(-n // 64)
+    assert out.shape == (64 * per, 2)
+    blocks = out.reshape(64, per, 2) if per else out.reshape(64, 0, 2)
+    filled = (blocks[:, :, 0] != 0).sum(1)
+    assert filled.sum() == n and (filled.max() - filled.min() <= 1 if n else True)
+    assert np.array_equal(np.concatenate([blocks[b, :filled[b]] for b in range(64)]), pairs)  # order kept
+    for b in range(64):
+        assert not blocks[b, filled[b]:].any()  # padding is (0, 0)
