@@ -2,7 +2,8 @@
  * argument struct set field by field from the runner's integer list (the struct
  * itself comes from the reference's include/argument.h), and its results read
  * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BUILD,
- * -DGLUE_PROBE, -DGLUE_NL or -DGLUE_LP. Test infrastructure of the oracle only. */
+ * -DGLUE_PROBE, -DGLUE_NL, -DGLUE_LP, -DGLUE_SMP or -DGLUE_SMJ. Test
+ * infrastructure of the oracle only. */
 #include <stdbool.h>
 #include <stdint.h>
 
@@ -141,6 +142,53 @@ int dpu_host_get_results(int64_t *o, int cap) {
     return 6;
 }
 
+#elif defined(GLUE_SMP)
+/* src/dpu/src/join/mpsm_join_local_partition.c */
+extern sort_merge_partitioning_arg param_sort_merge_partitioning;
+extern sort_merge_probe_return_arg param_sort_merge_probe_return;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 8) return -1;
+    sort_merge_partitioning_arg *p = &param_sort_merge_partitioning;
+    p->elem_range = (int32_t)a[0];
+    p->num_packets = (int32_t)a[1];
+    p->packet_size = (int32_t)a[2];
+    p->hist_interval = (int32_t)a[3];
+    p->r_packet_start_byte = (int32_t)a[4];
+    p->r_sorted_start_byte = (int32_t)a[5];
+    p->histogram_addr_start_byte = (int32_t)a[6];
+    p->data_skewness = (int32_t)a[7];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) {
+    if (cap < 5) return 0;
+    errors_out(o);
+    o[4] = param_sort_merge_probe_return.result_size;
+    return 5;
+}
+
+#elif defined(GLUE_SMJ)
+/* src/dpu/src/join/mpsm_join_sort_probe.c */
+extern sort_merge_sort_probe_arg param_sort_merge_sort_probe;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 9) return -1;
+    sort_merge_sort_probe_arg *p = &param_sort_merge_sort_probe;
+    p->elem_range = (int32_t)a[0];
+    p->hist_interval = (int32_t)a[1];
+    p->r_sorted_start_byte = (int32_t)a[2];
+    p->s_sorted_start_byte = (int32_t)a[3];
+    p->r_histogram_start_byte = (int32_t)a[4];
+    p->s_histogram_start_byte = (int32_t)a[5];
+    p->result_probe_start_byte = (int32_t)a[6];
+    p->r_total_bytes = (int32_t)a[7];
+    p->s_total_bytes = (int32_t)a[8];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
+
 #else
-#error "define GLUE_COUNT, GLUE_BUILD, GLUE_PROBE, GLUE_NL or GLUE_LP"
+#error "define GLUE_COUNT, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP or GLUE_SMJ"
 #endif

@@ -2,10 +2,11 @@
 
 Test infrastructure only (tests/ imports it, nothing else): ``make -C oracle
 ref`` compiles glb_partition_count.c, a2a_packetwise_srj_local_partition.c,
-a2a_srj_build.c, a2a_srj_probe_inner_mt.c and nested_loop_join.c
-(src/dpu/src/join/ of yonsei-hpcp/spid-join) from the reference tree, each with
-the reference's hash.c and the host stand-in for the DPU runtime in
-oracle/dpu_host/, into oracle/_ref/dpu_{count,lp,build,probe,nl}.
+a2a_srj_build.c, a2a_srj_probe_inner_mt.c, nested_loop_join.c,
+mpsm_join_local_partition.c and mpsm_join_sort_probe.c (src/dpu/src/join/ of
+yonsei-hpcp/spid-join) from the reference tree, each with the reference's
+hash.c and the host stand-in for the DPU runtime in oracle/dpu_host/, into
+oracle/_ref/dpu_{count,lp,build,probe,nl,smp,smj}.
 One call of a runner is one DPU launch of 12 tasklets over one MRAM image; this
 module lays the image out, passes the kernel's arguments and reads its results
 back, so that the oracle's restatement of those kernels can be checked against
@@ -18,7 +19,7 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k) for k in ("count", "build", "probe", "nl", "lp")}
+RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k) for k in ("count", "build", "probe", "nl", "lp", "smp", "smj")}
 TASKLETS = 12              # NR_TASKLETS of every join kernel
 TABLE_BYTES = 32768        # one local partition's hash table (a2a_srj_build.c: 4096 x 8 B)
 JOIN_TYPE_EQUI = 1         # include/argument.h
@@ -154,3 +155,105 @@ def local_partition(tuples, partitions=0):
     starts = img[info_at:info_at + 4 * L].view(np.uint32).astype(np.int64)
     grouped = img[res_at:res_at + 8 * m].view(np.uint32).reshape(m, 2).copy()
     return grouped, np.append(starts, m), L
+
+
+def range_buckets(elem_range, hist_interval):
+    """The number of key-range buckets both sort-merge kernels use:
+    elem_range / hist_interval + 1 (mpsm_join_local_partition.c:137,
+    mpsm_join_sort_probe.c:281); bucket of a key = min(key / hist_interval,
+    buckets - 1)."""
+    return int(elem_range) // int(hist_interval) + 1
+
+
+def probed_buckets(elem_range, hist_interval):
+    """Which buckets mpsm_join_sort_probe.c joins (boolean mask). It reads the
+    bucket starts in blocks of 512 and walks parts 0..510 of each full block
+    (:297) and parts 0..remains-2 of the last (:395), because a part's size is
+    start[part+1] - start[part] within the block: bucket 511 of every full
+    block and the last bucket are never probed, and their output slots are not
+    written."""
+    B = range_buckets(elem_range, hist_interval)
+    loops, remains = divmod(B, 512)
+    b = np.arange(B)
+    return (b < loops * 512) & (b % 512 != 511) | (b >= loops * 512) & (b - loops * 512 < remains - 1)
+
+
+def range_partition(tuples, elem_range, hist_interval):
+    """mpsm_join_local_partition.c on one DPU holding `tuples` (key-0 tuples
+    are gaps and are dropped): (tuples grouped by key-range bucket, the B
+    bucket starts the kernel writes, the non-gap count it returns). Within a
+    bucket the order is whichever the tasklets' scatter gave."""
+    t = np.ascontiguousarray(tuples, dtype=np.uint32).reshape(-1, 2)
+    n = t.shape[0]
+    B = range_buckets(elem_range, hist_interval)
+    if hist_interval < 1 or not 1 <= B <= 8190:
+        # the kernel's histogram is 8192 words and holds B + 1 of them
+        raise ValueError("1 <= elem_range / hist_interval + 1 <= 8190")
+    sorted_at = _align(n * 8) + 2048
+    hist_at = sorted_at + _align(n * 8) + 2048
+    mram = np.zeros(hist_at + _align(B * 4) + 2048, dtype=np.uint8)
+    _put(mram, 0, t)
+    res, img = launch("smp", [elem_range, n, 8, hist_interval, 0, sorted_at, hist_at, 0], mram)
+    if any(res[:4]):
+        raise RuntimeError(f"dpu_smp reported errors {res[:4]}")
+    m = int(res[4])
+    grouped = img[sorted_at:sorted_at + 8 * n].view(np.uint32).reshape(n, 2).copy()
+    starts = img[hist_at:hist_at + 4 * B].view(np.uint32).astype(np.int64)
+    return grouped, starts, m
+
+
+def sort_merge(R, S, elem_range, hist_interval):
+    """mpsm_join_local_partition.c on R and on S, then mpsm_join_sort_probe.c,
+    on one DPU. Each probed S tuple becomes (payload of the R tuple with its
+    key, S payload). Returns (rows of the probed buckets in the order the
+    kernel wrote them, S tuples of the buckets it leaves unprobed).
+
+    The inputs must keep the kernels on their working path:
+      - every key of a probed S bucket is in R (the probe stops its tasklet at
+        the first S key R lacks, :226-229, and the others then wait at a
+        barrier that never completes);
+      - at most 127 tuples of R and of S per bucket (the merge sort writes one
+        tuple past a full 128-tuple buffer, :199-202);
+      - no probed bucket with S tuples holds exactly one tuple of R or of S
+        (the merge sort of one tuple never writes its output buffer, :153-208,
+        so the probe would read that buffer's stale contents);
+      - B % 512 is 0 or 1, or the last block's B % 512 - 1 buckets are a
+        multiple of 12 and all hold S tuples (its loop waits at a barrier once
+        per bucket it joins, :477, so every tasklet must join as many)."""
+    R = np.ascontiguousarray(R, dtype=np.uint32).reshape(-1, 2)
+    S = np.ascontiguousarray(S, dtype=np.uint32).reshape(-1, 2)
+    B = range_buckets(elem_range, hist_interval)
+    bucket = lambda k: np.minimum(k.astype(np.int64) // hist_interval, B - 1)  # noqa: E731
+    rk, sk = R[:, 0][R[:, 0] != 0], S[:, 0][S[:, 0] != 0]
+    probed = probed_buckets(elem_range, hist_interval)
+    if max(np.bincount(bucket(rk), minlength=B).max(initial=0),
+           np.bincount(bucket(sk), minlength=B).max(initial=0)) > 127:
+        raise ValueError("more than 127 tuples in a bucket")
+    if not np.isin(sk[probed[bucket(sk)]], rk).all():
+        raise ValueError("an S key of a probed bucket is not in R")
+    r_n, s_n = np.bincount(bucket(rk), minlength=B), np.bincount(bucket(sk), minlength=B)
+    if ((s_n > 0) & probed & ((s_n == 1) | (r_n == 1))).any():
+        raise ValueError("a probed bucket holds exactly one tuple of R or of S")
+    tail = B % 512
+    if tail > 1:
+        s_tail = np.bincount(bucket(sk), minlength=B)[B - tail:B - 1]
+        if (tail - 1) % 12 or not s_tail.all():
+            raise ValueError("the last histogram block must hold 12k buckets with S tuples, plus one")
+    r_grp, r_start, n_r = range_partition(R, elem_range, hist_interval)
+    s_grp, s_start, n_s = range_partition(S, elem_range, hist_interval)
+    r_at = 0
+    s_at = _align(n_r * 8) + 2048
+    rh_at = s_at + _align(n_s * 8) + 2048
+    sh_at = rh_at + _align(B * 4) + 2048
+    res_at = sh_at + _align(B * 4) + 2048
+    mram = np.zeros(res_at + _align(n_s * 8) + 2048, dtype=np.uint8)
+    _put(mram, r_at, r_grp[:n_r])
+    _put(mram, s_at, s_grp[:n_s])
+    _put(mram, rh_at, r_start.astype(np.uint32))
+    _put(mram, sh_at, s_start.astype(np.uint32))
+    res, img = launch("smj", [elem_range, hist_interval, r_at, s_at, rh_at, sh_at, res_at, 8 * n_r, 8 * n_s], mram)
+    if any(res[:4]):
+        raise RuntimeError(f"dpu_smj reported errors {res[:4]}")
+    out = img[res_at:res_at + 8 * n_s].view(np.uint32).reshape(n_s, 2)
+    keep = probed[bucket(s_grp[:n_s, 0])]
+    return out[keep].copy(), s_grp[:n_s][~keep].copy()

@@ -64,6 +64,8 @@ def lib():
         L.orc_local_partition.argtypes = [vp, i64, i64, vp, vp]
         L.orc_dpu_phj.restype = i64
         L.orc_dpu_phj.argtypes = [vp, i64, vp, i64, vp]
+        L.orc_dpu_smj.restype = i64
+        L.orc_dpu_smj.argtypes = [vp, i64, vp, i64, vp]
         L.orc_refpipe_dpu_sizes.restype = i32
         L.orc_refpipe_dpu_sizes.argtypes = [vp, i64, vp, i64, i32, i32, i32, i32, vp, vp]
         _lib = L
@@ -219,6 +221,18 @@ def dpu_phj(R, S):
     R, S = _tuples(R), _tuples(S)
     out = np.empty((max(S.shape[0], 1), 2), dtype=np.uint32)
     m = lib().orc_dpu_phj(_ptr(R), R.shape[0], _ptr(S), S.shape[0], _ptr(out))
+    if m < 0:
+        raise RuntimeError(ERRORS.get(m, m))
+    return out[:m]
+
+
+def dpu_smj(R, S):
+    """One DPU's sort-merge join as the oracle restates it: S sorted by key,
+    each S tuple whose key R holds taking the first such R tuple's payload as
+    its key, the others unchanged (all n_s rows)."""
+    R, S = _tuples(R), _tuples(S)
+    out = np.empty((max(S.shape[0], 1), 2), dtype=np.uint32)
+    m = lib().orc_dpu_smj(_ptr(R), R.shape[0], _ptr(S), S.shape[0], _ptr(out))
     if m < 0:
         raise RuntimeError(ERRORS.get(m, m))
     return out[:m]

@@ -21,6 +21,7 @@
  *   hash build ............ src/dpu/src/join/a2a_srj_build.c:202-296
  *   hash probe ............ src/dpu/src/join/a2a_srj_probe_inner_mt.c:101-168
  *   sort-merge ............ src/dpu/src/join/mpsm_join_sort_probe.c:152-236
+ *                           (range buckets: mpsm_join_local_partition.c:137,203-207)
  *   nested loop ........... src/dpu/src/join/nested_loop_join.c:184-231
  *
  * The CRC table is generated from the reflected CRC-32 polynomial 0xEDB88320; the
@@ -506,6 +507,15 @@ static int dpu_smj(const orc_tuple *r, int64_t nr, const orc_tuple *s, int64_t n
     free(rs);
     *nout = ns;
     return ORC_OK;
+}
+
+/* One DPU's sort-merge join as dpu_smj restates it: all n_s S tuples, sorted by
+ * key, matched ones carrying their R payload as key. Returns n_s or an error. */
+int64_t orc_dpu_smj(const orc_tuple *r, int64_t nr, const orc_tuple *s, int64_t ns, orc_tuple *out)
+{
+    int64_t m = 0;
+    const int rc = dpu_smj(r, nr, s, ns, out, &m);
+    return rc ? rc : m;
 }
 
 /* Per-DPU nested loop (nested_loop_join.c:184-231): every S tuple is compared

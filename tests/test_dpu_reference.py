@@ -3,9 +3,10 @@ reference tree as plain C and run on the host (oracle/dpu_ref.py,
 oracle/dpu_host/): the global partition count of src/dpu/src/join/
 glb_partition_count.c, the local partitioning of
 a2a_packetwise_srj_local_partition.c, the hash build and probe of
-a2a_srj_build.c and a2a_srj_probe_inner_mt.c and the nested loop of
-nested_loop_join.c must give what the oracle's restatement gives on the same
-inputs. The runners exist only where the reference tree was present when
+a2a_srj_build.c and a2a_srj_probe_inner_mt.c, the nested loop of
+nested_loop_join.c, and the range partitioning and sort-probe of
+mpsm_join_local_partition.c and mpsm_join_sort_probe.c must give what the
+oracle's restatement gives on the same inputs. The runners exist only where the reference tree was present when
 the oracle was built; elsewhere these tests are skipped."""
 import numpy as np
 import pytest
@@ -144,3 +145,115 @@ def test_reference_kernels_chained_join(oracle):
     got = dpu_ref.hash_join(rg, ro, sg, so)
     assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.dpu_phj(R, S)))
     assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
+
+
+def _range_bucket(keys, elem_range, interval):
+    return np.minimum(keys.astype(np.int64) // interval, dpu_ref.range_buckets(elem_range, interval) - 1)
+
+
+@pytest.mark.parametrize("n,elem_range,interval,gap", [(1, 64, 64, 0), (5000, 1 << 16, 64, 0),
+                                                       (100000, 1 << 16, 64, 13), (70000, 500000, 100, 0)])
+def test_range_partition_kernel(n, elem_range, interval, gap):
+    """mpsm_join_local_partition.c: the non-gap tuples grouped by key range
+    (bucket = min(key / interval, B - 1), so keys past elem_range land in the
+    last bucket), the B bucket starts it writes are the exclusive prefix sum of
+    the bucket sizes, the slots past the non-gap count are zeroed."""
+    rng = np.random.default_rng(n + elem_range)
+    keys = rng.integers(1, elem_range + 1, n)
+    keys[::101] = rng.integers(elem_range, 2**32, keys[::101].size)  # past the range
+    T = np.stack([keys, rng.integers(0, 2**32, n)], 1).astype(np.uint32)
+    if gap:
+        T[::gap, 0] = 0
+    got, starts, m = dpu_ref.range_partition(T, elem_range, interval)
+    nz = T[T[:, 0] != 0]
+    assert m == nz.shape[0]
+    B = dpu_ref.range_buckets(elem_range, interval)
+    sizes = np.bincount(_range_bucket(nz[:, 0], elem_range, interval), minlength=B)
+    assert np.array_equal(starts, np.cumsum(sizes) - sizes)
+    for b in np.flatnonzero(sizes):
+        grp = got[starts[b]:starts[b] + sizes[b]]
+        assert np.array_equal(oracle_sort(grp), oracle_sort(nz[_range_bucket(nz[:, 0], elem_range, interval) == b]))
+    assert not got[m:].any()
+
+
+def oracle_sort(t):
+    return t[np.lexsort((t[:, 1], t[:, 0]))]
+
+
+def test_sort_probe_bucket_walk():
+    """mpsm_join_sort_probe.c joins parts 0..510 of every full block of 512
+    bucket starts and parts 0..remains-2 of the last block: bucket 511 of each
+    full block and the last bucket are left unprobed."""
+    m = dpu_ref.probed_buckets(513 * 64 - 1, 64)  # B = 513
+    assert m.size == 513 and m.sum() == 511 and not m[511] and not m[512]
+    m = dpu_ref.probed_buckets(1023 * 64, 64)  # B = 1024, no partial block
+    assert m.sum() == 1022 and not m[511] and not m[1023]
+    m = dpu_ref.probed_buckets(524 * 64, 64)  # B = 525: 12 of the last block's 13
+    assert m.sum() == 511 + 12 and m[512:524].all() and not m[524]
+    assert dpu_ref.probed_buckets(10, 64).sum() == 0  # B = 1
+
+
+def _fk_inputs(rng, elem_range, interval, n_s, density=1.0, hot=0):
+    """R: a `density` share of the keys 1..elem_range, unique, random payloads;
+    S: n_s keys drawn from R (plus `hot` copies of one R key), payloads 0..;
+    bucket sizes stay within the kernels' 127-tuple buffers."""
+    keys = np.arange(1, elem_range + 1)
+    if density < 1.0:
+        keys = keys[rng.random(keys.size) < density]
+    keys = rng.permutation(keys)
+    R = np.stack([keys, rng.integers(0, 2**32, keys.size)], 1).astype(np.uint32)
+    sk = np.concatenate([keys[rng.integers(0, keys.size, n_s)], np.full(hot, keys[0])])
+    S = np.stack([rng.permutation(sk), np.arange(sk.size)], 1).astype(np.uint32)
+    return R, S
+
+
+@pytest.mark.parametrize("elem_range,interval,n_s,density,hot,gap",
+                         [(513 * 64 - 1, 64, 20000, 1.0, 0, 0),     # B = 513
+                          (1023 * 64, 64, 40000, 1.0, 40, 0),       # B = 1024, one key 40 more times
+                          (524 * 64, 64, 30000, 1.0, 0, 29),        # B = 525: the last block's loop
+                          (2047 * 128, 128, 100000, 0.5, 0, 0),     # B = 2048, half the keys in R
+                          (4095 * 32, 32, 60000, 1.0, 0, 0)])       # B = 4096
+def test_sort_merge_kernels_fk(oracle, elem_range, interval, n_s, density, hot, gap):
+    """mpsm_join_local_partition.c on R and on S, then mpsm_join_sort_probe.c:
+    on foreign-key inputs (the only ones the probe finishes on) the rows of the
+    buckets it probes equal the oracle's per-DPU sort-merge join of those S
+    tuples, keys in the same order (S sorted by key within a bucket, buckets by
+    range), and the S tuples it leaves unprobed are exactly those of the
+    unprobed buckets."""
+    rng = np.random.default_rng(elem_range + n_s)
+    R, S = _fk_inputs(rng, elem_range, interval, n_s, density, hot)
+    if gap:
+        R[::gap, 0] = 0  # gaps in both relations' packets; S keeps only keys R still holds
+        S = S[np.isin(S[:, 0], R[R[:, 0] != 0, 0])]
+        S[::gap, 0] = 0
+    rows, unprobed = dpu_ref.sort_merge(R, S, elem_range, interval)
+    nz = S[S[:, 0] != 0]
+    probed = dpu_ref.probed_buckets(elem_range, interval)[_range_bucket(nz[:, 0], elem_range, interval)]
+    want = oracle.dpu_smj(R[R[:, 0] != 0], nz[probed])
+    assert rows.shape[0] == want.shape[0] == int(probed.sum())
+    assert np.array_equal(rows[:, 0], want[:, 0])
+    assert np.array_equal(oracle.sort_pairs(rows), oracle.sort_pairs(want))
+    assert np.array_equal(oracle.sort_pairs(rows), oracle.sort_pairs(oracle.simple_join(R, nz[probed])))
+    assert np.array_equal(oracle.sort_pairs(unprobed), oracle.sort_pairs(nz[~probed]))
+
+
+def test_sort_merge_refuses_inputs_the_kernels_cannot_finish():
+    """The wrapper refuses, before any launch, the inputs on which the
+    reference's sort-probe would stop a tasklet early or overrun a buffer."""
+    rng = np.random.default_rng(3)
+    R, S = _fk_inputs(rng, 513 * 64 - 1, 64, 20000)
+    bad = S.copy()
+    bad[0, 0] = 513 * 64 + 5  # last bucket: unprobed, so allowed
+    dpu_ref.sort_merge(R, bad, 513 * 64 - 1, 64)
+    bad[0, 0] = 2 * 513 * 64  # still the last bucket (clamped)
+    dpu_ref.sort_merge(R, bad, 513 * 64 - 1, 64)
+    R2 = R[R[:, 0] != 100]
+    with pytest.raises(ValueError, match="not in R"):
+        dpu_ref.sort_merge(R2, np.array([[100, 0]], dtype=np.uint32), 513 * 64 - 1, 64)
+    with pytest.raises(ValueError, match="127"):
+        dpu_ref.sort_merge(R, np.array([[R[0, 0], i] for i in range(128)], dtype=np.uint32), 513 * 64 - 1, 64)
+    with pytest.raises(ValueError, match="exactly one"):
+        dpu_ref.sort_merge(R, S[:1000], 513 * 64 - 1, 64)  # sparse S: buckets of one S tuple
+    with pytest.raises(ValueError, match="last histogram block"):
+        R3, S3 = _fk_inputs(rng, 600 * 64, 64, 40000)
+        dpu_ref.sort_merge(R3, S3, 600 * 64, 64)  # B = 601: the last block's loop joins 88 buckets
