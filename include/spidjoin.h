@@ -37,7 +37,7 @@ enum spj_status {
     SPJ_E_OVERFLOW = -5,    /* a partition exceeded its shared-memory table */
     SPJ_E_TIMEOUT = -6,     /* a bounded device wait gave up */
     SPJ_E_NODEVICE = -7,    /* no CUDA device, or not an sm_100 device */
-    SPJ_E_UNSUPPORTED = -8  /* option not supported by this build */
+    SPJ_E_UNSUPPORTED = -8  /* option this library does not support */
 };
 
 /* join_alg values, include/idpHandler.hpp:135-138 */

@@ -19,6 +19,10 @@ int dpu_kernel_main(void);
 
 __thread unsigned dpu_host_tasklet;
 
+/* Room past the kernel's atomic-bit array (linked before this file, so it comes
+ * first in the section): the DPU's atomic register has 256 bits. */
+__attribute__((section("dpu_atomic"), used)) uint8_t dpu_host_atomic_tail[256];
+
 static uint8_t *g_mram;
 static uint64_t g_mram_bytes;
 static uint8_t *g_wram;

@@ -12,7 +12,8 @@
  *   - WRAM is a bump-allocated block mapped below 4 GiB, because the kernels
  *     round-trip WRAM pointers through uint32_t;
  *   - the runtime's mutexes are bytes taken with an atomic test-and-set, its
- *     barriers count arrivals per generation.
+ *     barriers count arrivals per generation; the kernels' atomic-bit arrays
+ *     share one section with room past their ends.
  * The DPU intrinsics and their meaning follow the UPMEM SDK documentation
  * (mram.h, alloc.h, barrier.h, mutex.h, defs.h, perfcounter.h). */
 #ifndef DPU_HOST_H
@@ -30,7 +31,11 @@
 #define __mram_ptr
 #define __mram
 #define __mram_noinit
-#define __atomic_bit
+/* The DPU keeps __atomic_bit arrays in its atomic register of 256 bits, so an
+ * index past an array's end still names an atomic bit (two kernels take bits 49
+ * and 50 of a 32-entry array). On the host they go to one section that ends
+ * with a 256-byte tail (dpu_host.c), so such an index stays inside it. */
+#define __atomic_bit __attribute__((section("dpu_atomic")))
 #define __dma_aligned __attribute__((aligned(8)))
 #define __noinline __attribute__((noinline))
 

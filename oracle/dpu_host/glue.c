@@ -2,8 +2,8 @@
  * argument struct set field by field from the runner's integer list (the struct
  * itself comes from the reference's include/argument.h), and its results read
  * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BUILD,
- * -DGLUE_PROBE, -DGLUE_NL, -DGLUE_LP, -DGLUE_SMP or -DGLUE_SMJ. Test
- * infrastructure of the oracle only. */
+ * -DGLUE_PROBE, -DGLUE_NL, -DGLUE_LP, -DGLUE_SMP, -DGLUE_SMJ, -DGLUE_NBUILD or
+ * -DGLUE_NPROBE. Test infrastructure of the oracle only. */
 #include <stdbool.h>
 #include <stdint.h>
 
@@ -189,6 +189,46 @@ int dpu_host_set_args(const int64_t *a, int n) {
 
 int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
 
+#elif defined(GLUE_NBUILD)
+/* src/dpu/src/join/packetwise_no_partitioned_hash_join_build.c */
+extern packetwise_nphj_build_arg param_packetwise_nphj_build;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 4) return -1;
+    packetwise_nphj_build_arg *p = &param_packetwise_nphj_build;
+    p->R_packet_start_byte = (int32_t)a[0];
+    p->num_input_bytes = (int32_t)a[1];
+    p->hash_table_start_byte = (int32_t)a[2];
+    p->hash_table_byte_size = (int32_t)a[3];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
+
+#elif defined(GLUE_NPROBE)
+/* src/dpu/src/join/packetwise_no_partitioned_hash_join_probe.c */
+extern packetwise_nphj_probe_arg param_packetwise_nphj_probe;
+extern packetwise_nphj_probe_return_arg param_packetwise_nphj_probe_return;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 5) return -1;
+    packetwise_nphj_probe_arg *p = &param_packetwise_nphj_probe;
+    p->S_packet_start_byte = (int32_t)a[0];
+    p->num_input_bytes = (int32_t)a[1];
+    p->hash_table_start_byte = (int32_t)a[2];
+    p->hash_table_byte_size = (int32_t)a[3];
+    p->result_start_byte = (int32_t)a[4];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) {
+    if (cap < 6) return 0;
+    errors_out(o);
+    o[4] = param_packetwise_nphj_probe_return.result_size;
+    o[5] = param_packetwise_nphj_probe_return.miss_count;
+    return 6;
+}
+
 #else
-#error "define GLUE_COUNT, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP or GLUE_SMJ"
+#error "define GLUE_COUNT, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP, GLUE_SMJ, GLUE_NBUILD or GLUE_NPROBE"
 #endif

@@ -3,10 +3,11 @@
 Test infrastructure only (tests/ imports it, nothing else): ``make -C oracle
 ref`` compiles glb_partition_count.c, a2a_packetwise_srj_local_partition.c,
 a2a_srj_build.c, a2a_srj_probe_inner_mt.c, nested_loop_join.c,
-mpsm_join_local_partition.c and mpsm_join_sort_probe.c (src/dpu/src/join/ of
+mpsm_join_local_partition.c, mpsm_join_sort_probe.c and
+packetwise_no_partitioned_hash_join_{build,probe}.c (src/dpu/src/join/ of
 yonsei-hpcp/spid-join) from the reference tree, each with the reference's
 hash.c and the host stand-in for the DPU runtime in oracle/dpu_host/, into
-oracle/_ref/dpu_{count,lp,build,probe,nl,smp,smj}.
+oracle/_ref/dpu_{count,lp,build,probe,nl,smp,smj,nbuild,nprobe}.
 One call of a runner is one DPU launch of 12 tasklets over one MRAM image; this
 module lays the image out, passes the kernel's arguments and reads its results
 back, so that the oracle's restatement of those kernels can be checked against
@@ -19,7 +20,8 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k) for k in ("count", "build", "probe", "nl", "lp", "smp", "smj")}
+RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k) for k in ("count", "build", "probe", "nl", "lp", "smp", "smj", "nbuild",
+                                                            "nprobe")}
 TASKLETS = 12              # NR_TASKLETS of every join kernel
 TABLE_BYTES = 32768        # one local partition's hash table (a2a_srj_build.c: 4096 x 8 B)
 JOIN_TYPE_EQUI = 1         # include/argument.h
@@ -257,3 +259,61 @@ def sort_merge(R, S, elem_range, hist_interval):
     out = img[res_at:res_at + 8 * n_s].view(np.uint32).reshape(n_s, 2)
     keep = probed[bucket(s_grp[:n_s, 0])]
     return out[keep].copy(), s_grp[:n_s][~keep].copy()
+
+
+def nphj_slots(n_r):
+    """The table the reference's host gives one DPU's non-partitioned hash
+    join: the power of two just above 16 slots per R tuple
+    (src/dpuArgumentJoin.cc:364-376, 389)."""
+    return 1 << (int(np.floor(np.log2(16 * max(int(n_r), 1)))) + 1)
+
+
+def nphj(R, S, slots=None):
+    """packetwise_no_partitioned_hash_join_build.c, then
+    packetwise_no_partitioned_hash_join_probe.c, on one DPU: one table of
+    `slots` 8-byte slots (default nphj_slots(|R|)) over the whole of R, first
+    slot join_hash2(key) & (slots - 1). After a collision the kernels step the
+    full hash value and reset it to 0 once it reaches `slots` (:143-149 of the
+    build), so a collision chain continues at slot 0 (the same sequence in
+    build and probe, so the join stays exact). Returns the pairs (R payload, S
+    payload) in the order the tasklets wrote them, and the probe's miss count."""
+    R = np.ascontiguousarray(R, dtype=np.uint32).reshape(-1, 2)
+    S = np.ascontiguousarray(S, dtype=np.uint32).reshape(-1, 2)
+    n_r, n_s = R.shape[0], S.shape[0]
+    slots = nphj_slots(n_r) if slots is None else int(slots)
+    if slots < 32 or slots & (slots - 1) or slots * 8 >= 1 << 31:
+        raise ValueError("slots: a power of two, 32 <= slots < 2^28")
+    if int((R[:, 0] != 0).sum()) >= slots:
+        # the build inserts without a bound: a full table would never finish
+        raise ValueError("no more R tuples than table slots - 1")
+    r_at = 0
+    ht = _align(n_r * 8) + 2048      # the kernels read whole 2 KiB blocks
+    s_at = ht + _align(slots * 8) + 2048
+    res_at = s_at + _align(n_s * 8) + 2048
+    mram = np.zeros(res_at + _align(n_s * 8) + 2048, dtype=np.uint8)
+    _put(mram, r_at, R)
+    _put(mram, s_at, S)
+    res, img = launch("nbuild", [r_at, 8 * n_r, ht, 8 * slots], mram)
+    if any(res[:4]):
+        raise RuntimeError(f"dpu_nbuild reported errors {res[:4]}")
+    res, img = launch("nprobe", [s_at, 8 * n_s, ht, 8 * slots, res_at], img)
+    if any(res[:4]):
+        raise RuntimeError(f"dpu_nprobe reported errors {res[:4]}")
+    m = int(res[4])
+    return img[res_at:res_at + 8 * m].view(np.uint32).reshape(m, 2).copy(), int(res[5])
+
+
+def nphj_table(R, slots):
+    """The table packetwise_no_partitioned_hash_join_build.c leaves after
+    inserting R: `slots` rows of (key, payload), key 0 where empty."""
+    R = np.ascontiguousarray(R, dtype=np.uint32).reshape(-1, 2)
+    n_r = R.shape[0]
+    if slots < 32 or slots & (slots - 1) or int((R[:, 0] != 0).sum()) >= slots:
+        raise ValueError("slots: a power of two >= 32, above the R tuples")
+    ht = _align(n_r * 8) + 2048
+    mram = np.zeros(ht + _align(slots * 8) + 2048, dtype=np.uint8)
+    _put(mram, 0, R)
+    res, img = launch("nbuild", [0, 8 * n_r, ht, 8 * slots], mram)
+    if any(res[:4]):
+        raise RuntimeError(f"dpu_nbuild reported errors {res[:4]}")
+    return img[ht:ht + 8 * slots].view(np.uint32).reshape(slots, 2).copy()

@@ -23,6 +23,10 @@
  *   sort-merge ............ src/dpu/src/join/mpsm_join_sort_probe.c:152-236
  *                           (range buckets: mpsm_join_local_partition.c:137,203-207)
  *   nested loop ........... src/dpu/src/join/nested_loop_join.c:184-231
+ *   non-partitioned hash .. src/dpu/src/join/packetwise_no_partitioned_hash_join_build.c:101-166,
+ *                           packetwise_no_partitioned_hash_join_probe.c:65-160 (one table over
+ *                           the DPU's R, first match per S tuple: the pairs of the hash join
+ *                           above, which the refpipe join runs for it)
  *
  * The CRC table is generated from the reflected CRC-32 polynomial 0xEDB88320; the
  * reference ships the same table literally (hash.c:15-59). The test suite pins

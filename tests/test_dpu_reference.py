@@ -4,9 +4,10 @@ oracle/dpu_host/): the global partition count of src/dpu/src/join/
 glb_partition_count.c, the local partitioning of
 a2a_packetwise_srj_local_partition.c, the hash build and probe of
 a2a_srj_build.c and a2a_srj_probe_inner_mt.c, the nested loop of
-nested_loop_join.c, and the range partitioning and sort-probe of
-mpsm_join_local_partition.c and mpsm_join_sort_probe.c must give what the
-oracle's restatement gives on the same inputs. The runners exist only where the reference tree was present when
+nested_loop_join.c, the range partitioning and sort-probe of
+mpsm_join_local_partition.c and mpsm_join_sort_probe.c, and the
+non-partitioned hash join of packetwise_no_partitioned_hash_join_{build,probe}.c
+must give what the oracle's restatement gives on the same inputs. The runners exist only where the reference tree was present when
 the oracle was built; elsewhere these tests are skipped."""
 import numpy as np
 import pytest
@@ -257,3 +258,76 @@ def test_sort_merge_refuses_inputs_the_kernels_cannot_finish():
     with pytest.raises(ValueError, match="last histogram block"):
         R3, S3 = _fk_inputs(rng, 600 * 64, 64, 40000)
         dpu_ref.sort_merge(R3, S3, 600 * 64, 64)  # B = 601: the last block's loop joins 88 buckets
+
+
+@pytest.mark.parametrize("n_r,n_s", [(1, 3), (1000, 5000), (1 << 16, 1 << 18)])
+def test_nphj_kernels_fk(oracle, n_r, n_s):
+    """packetwise_no_partitioned_hash_join_{build,probe}.c with the table the
+    reference's host sizes: unique R keys, S with misses and padding, one pair
+    per matching S tuple, equal to the oracle's per-DPU join and the
+    independent join."""
+    rng = np.random.default_rng(n_r * 7 + n_s)
+    keys = rng.permutation(np.arange(1, 4 * n_r + 2))[:n_r]
+    R = np.stack([keys, rng.integers(0, 2**32, n_r)], 1).astype(np.uint32)
+    hit = rng.random(n_s) < 0.7
+    S = np.stack([np.where(hit, keys[rng.integers(0, n_r, n_s)], rng.integers(4 * n_r + 2, 2**32, n_s)),
+                  np.arange(n_s)], 1).astype(np.uint32)
+    S[::41, 0] = 0
+    R[::97, 0] = 0
+    got, _ = dpu_ref.nphj(R, S)
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.dpu_phj(R, S)))
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
+
+
+def test_nphj_kernels_generated(oracle):
+    """One DPU's share of the benchmark relations (Zipf 1.0): every S tuple
+    joins, and the count and checksum are the generator's answer."""
+    R, S, expect = oracle.generate(1 << 16, 1 << 18, 1.0, seed=0x5EED)
+    got, _ = dpu_ref.nphj(R, S)
+    assert got.shape == (S.shape[0], 2) and oracle.checksum(got) == expect
+
+
+@pytest.mark.parametrize("slots", [1024, 2048])
+def test_nphj_kernels_full_table(oracle, slots):
+    """A table at load 1000/1024 and 1000/2048: the long collision chains still
+    give the exact join."""
+    rng = np.random.default_rng(slots)
+    keys = rng.permutation(np.arange(1, 1 << 20))[:1000]
+    R = np.stack([keys, np.arange(1000)], 1).astype(np.uint32)
+    S = np.stack([np.concatenate([keys, rng.integers(1 << 20, 2**32, 500)]), np.arange(1500)], 1).astype(np.uint32)
+    got, miss = dpu_ref.nphj(R, S, slots)
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
+    assert miss > 0
+
+
+def test_nphj_kernels_repeated_r_keys(oracle):
+    """Repeated R keys: the build inserts every copy, and the probe stops at
+    the first copy on the key's sequence. Each S tuple whose key R holds yields
+    one pair joining equal keys (which copy is first depends on the tasklets)."""
+    rng = np.random.default_rng(11)
+    R = np.stack([rng.integers(1, 3000, 12000), np.arange(12000)], 1).astype(np.uint32)
+    S = np.stack([rng.integers(1, 6000, 40000), np.arange(40000)], 1).astype(np.uint32)
+    got, _ = dpu_ref.nphj(R, S)
+    want = oracle.dpu_phj(R, S)
+    assert got.shape == want.shape
+    assert np.array_equal(np.sort(got[:, 1]), np.sort(want[:, 1]))
+    assert np.array_equal(R[got[:, 0], 0], S[got[:, 1], 0])
+
+
+def test_nphj_build_chains_restart_at_slot_zero(oracle):
+    """The build's collision step adds 1 to the full 32-bit hash and resets it
+    to 0 once it reaches the slot count, so a key whose home slot is taken goes
+    to the first free slot counting from 0: every slot below a displaced key's
+    slot is occupied. (The probe walks the same sequence, so the join is
+    exact.)"""
+    rng = np.random.default_rng(5)
+    slots = 256
+    keys = rng.permutation(np.arange(1, 1 << 20))[:200]
+    R = np.stack([keys, np.arange(200)], 1).astype(np.uint32)
+    table = dpu_ref.nphj_table(R, slots)
+    assert np.array_equal(np.sort(table[table[:, 0] != 0, 0]), np.sort(keys))
+    h2 = oracle.hashes(table[:, 0])[:, 3].astype(np.int64)
+    displaced = [i for i in range(slots) if table[i, 0] and h2[i] >= slots and h2[i] % slots != i]
+    assert displaced
+    for i in displaced:
+        assert (table[:i, 0] != 0).all()
