@@ -1,9 +1,9 @@
 /* glue.c -- the runner's view of one reference kernel's __host variables: its
  * argument struct set field by field from the runner's integer list (the struct
  * itself comes from the reference's include/argument.h), and its results read
- * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BUILD,
- * -DGLUE_PROBE, -DGLUE_NL, -DGLUE_LP, -DGLUE_SMP, -DGLUE_SMJ, -DGLUE_NBUILD or
- * -DGLUE_NPROBE. Test infrastructure of the oracle only. */
+ * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BGCOUNT,
+ * -DGLUE_BUILD, -DGLUE_PROBE, -DGLUE_NL, -DGLUE_LP, -DGLUE_SMP, -DGLUE_SMJ,
+ * -DGLUE_NBUILD or -DGLUE_NPROBE. Test infrastructure of the oracle only. */
 #include <stdbool.h>
 #include <stdint.h>
 
@@ -21,7 +21,7 @@ static int errors_out(int64_t *o) {
 }
 
 #if defined(GLUE_COUNT)
-/* src/dpu/src/join/glb_partition_count.c */
+/* src/dpu/src/join/glb_partition_count.c and glb_chipwise_partition_count.c */
 extern glb_partition_count_arg param_glb_partition_count;
 
 int dpu_host_set_args(const int64_t *a, int n) {
@@ -39,6 +39,26 @@ int dpu_host_set_args(const int64_t *a, int n) {
     p->num_rank_in_rankgroup = (int32_t)a[9];
     p->join_type = (int32_t)a[10];
     p->hist_interval = (int32_t)a[11];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
+
+#elif defined(GLUE_BGCOUNT)
+/* src/dpu/src/join/bg_broadcast_count.c */
+extern bg_broadcast_count_arg param_bg_broadcast_count;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 8) return -1;
+    bg_broadcast_count_arg *p = &param_bg_broadcast_count;
+    p->input_offset = (int32_t)a[0];
+    p->elem_num = (int32_t)a[1];
+    p->partition_info_start_byte = (int32_t)a[2];
+    p->histogram_start_byte = (int32_t)a[3];
+    p->partition_num = (int32_t)a[4];
+    p->bankgroup = (int32_t)a[5];
+    p->rankgroup = (int32_t)a[6];
+    p->padding = (int32_t)a[7];
     return 0;
 }
 
@@ -230,5 +250,5 @@ int dpu_host_get_results(int64_t *o, int cap) {
 }
 
 #else
-#error "define GLUE_COUNT, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP, GLUE_SMJ, GLUE_NBUILD or GLUE_NPROBE"
+#error "define GLUE_COUNT, GLUE_BGCOUNT, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP, GLUE_SMJ, GLUE_NBUILD or GLUE_NPROBE"
 #endif

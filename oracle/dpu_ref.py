@@ -1,13 +1,14 @@
 """The reference's own DPU join kernels, run on the host.
 
 Test infrastructure only (tests/ imports it, nothing else): ``make -C oracle
-ref`` compiles glb_partition_count.c, a2a_packetwise_srj_local_partition.c,
+ref`` compiles glb_partition_count.c, glb_chipwise_partition_count.c,
+bg_broadcast_count.c, a2a_packetwise_srj_local_partition.c,
 a2a_srj_build.c, a2a_srj_probe_inner_mt.c, nested_loop_join.c,
 mpsm_join_local_partition.c, mpsm_join_sort_probe.c and
 packetwise_no_partitioned_hash_join_{build,probe}.c (src/dpu/src/join/ of
 yonsei-hpcp/spid-join) from the reference tree, each with the reference's
 hash.c and the host stand-in for the DPU runtime in oracle/dpu_host/, into
-oracle/_ref/dpu_{count,lp,build,probe,nl,smp,smj,nbuild,nprobe}.
+oracle/_ref/dpu_{count,chipcount,bgcount,lp,build,probe,nl,smp,smj,nbuild,nprobe}.
 One call of a runner is one DPU launch of 12 tasklets over one MRAM image; this
 module lays the image out, passes the kernel's arguments and reads its results
 back, so that the oracle's restatement of those kernels can be checked against
@@ -20,8 +21,8 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k) for k in ("count", "build", "probe", "nl", "lp", "smp", "smj", "nbuild",
-                                                            "nprobe")}
+RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k)
+           for k in ("count", "chipcount", "bgcount", "build", "probe", "nl", "lp", "smp", "smj", "nbuild", "nprobe")}
 TASKLETS = 12              # NR_TASKLETS of every join kernel
 TABLE_BYTES = 32768        # one local partition's hash table (a2a_srj_build.c: 4096 x 8 B)
 JOIN_TYPE_EQUI = 1         # include/argument.h
@@ -78,6 +79,45 @@ def partition_count(tuples, P, type_=0, rank_sets=1, ranks_per_set=1):
     res, img = launch("count", args, mram)
     if any(res[:4]):
         raise RuntimeError(f"dpu_count reported errors {res[:4]}")
+    return (img[hist:hist + 4 * P].view(np.uint32).copy(), img[info:info + 4 * P].view(np.uint32).copy())
+
+
+def chipwise_partition_count(tuples, ranks, rank_sets, bank_set):
+    """glb_chipwise_partition_count.c on one DPU holding S block `tuples`, for
+    64 * ranks destinations, bank sets of `bank_set` (8 ... 64) and `rank_sets`
+    rank sets: (histogram, start offsets)."""
+    t = np.ascontiguousarray(tuples, dtype=np.uint32).reshape(-1, 2)
+    n, P = t.shape[0], 64 * ranks
+    if P > 2048 or bank_set not in (8, 16, 32, 64) or ranks % rank_sets or rank_sets > 256 or \
+            P // (bank_set * rank_sets) < 1:
+        # its histogram is 2048 words; a bank set of 1 takes the plain count kernel
+        raise ValueError("64 * ranks <= 2048, bank_set in 8..64, ranks / rank_sets * 64 >= bank_set")
+    info = _align(n * 8) + 2048
+    hist = info + _align(P * 4) + 2048
+    mram = np.zeros(hist + _align(P * 4) + 2048, dtype=np.uint8)
+    _put(mram, 0, t)
+    args = [0, 1, 0, n, info, hist, P, bank_set, rank_sets, ranks // rank_sets, JOIN_TYPE_EQUI, 0]
+    res, img = launch("chipcount", args, mram)
+    if any(res[:4]):
+        raise RuntimeError(f"dpu_chipcount reported errors {res[:4]}")
+    return (img[hist:hist + 4 * P].view(np.uint32).copy(), img[info:info + 4 * P].view(np.uint32).copy())
+
+
+def bg_broadcast_count(tuples, partitions, bank_set):
+    """bg_broadcast_count.c on one DPU holding R block `tuples`: (histogram,
+    start offsets) over `partitions` bank groups (the reference passes
+    ranks per set * 64 / bank_set), by glb_partition_hash."""
+    t = np.ascontiguousarray(tuples, dtype=np.uint32).reshape(-1, 2)
+    n, P = t.shape[0], int(partitions)
+    if P < 1 or P & (P - 1) or P > 2048:
+        raise ValueError("partitions: a power of two up to 2048")
+    info = _align(n * 8) + 2048
+    hist = info + _align(P * 4) + 2048
+    mram = np.zeros(hist + _align(P * 4) + 2048, dtype=np.uint8)
+    _put(mram, 0, t)
+    res, img = launch("bgcount", [0, n, info, hist, P, bank_set, 1, 0], mram)
+    if any(res[:4]):
+        raise RuntimeError(f"dpu_bgcount reported errors {res[:4]}")
     return (img[hist:hist + 4 * P].view(np.uint32).copy(), img[info:info + 4 * P].view(np.uint32).copy())
 
 

@@ -64,6 +64,8 @@ def lib():
         L.orc_local_partition.argtypes = [vp, i64, i64, vp, vp]
         L.orc_dpu_phj.restype = i64
         L.orc_dpu_phj.argtypes = [vp, i64, vp, i64, vp]
+        L.orc_chipwise_partition_count.restype = i32
+        L.orc_chipwise_partition_count.argtypes = [vp, i64, i32, i32, i32, vp]
         L.orc_dpu_smj.restype = i64
         L.orc_dpu_smj.argtypes = [vp, i64, vp, i64, vp]
         L.orc_refpipe_dpu_sizes.restype = i32
@@ -151,6 +153,18 @@ def partition_count(tuples, P, type_=0, rank_sets=1, ranks_per_set=1):
     t = _tuples(tuples)
     hist = np.zeros(P, dtype=np.uint32)
     lib().orc_glb_partition_count(_ptr(t), t.shape[0], type_, P, rank_sets, ranks_per_set, _ptr(hist))
+    return hist
+
+
+def chipwise_partition_count(tuples, ranks, rank_sets, bank_set):
+    """Histogram of one DPU's S block over the 64 * ranks destinations with
+    bank sets (8 ... 64): bank group by hash, DPU in the group by the tuple's
+    index, rank set by the index's slot (the chip-wise split)."""
+    t = _tuples(tuples)
+    hist = np.zeros(64 * ranks, dtype=np.uint32)
+    rc = lib().orc_chipwise_partition_count(_ptr(t), t.shape[0], ranks, rank_sets, bank_set, _ptr(hist))
+    if rc:
+        raise RuntimeError(ERRORS.get(rc, rc))
     return hist
 
 

@@ -346,6 +346,25 @@ static inline int s_dest(const refpipe_t *rp, orc_tuple t, int64_t j)
            (((i / slot) & (rp->G - 1)) << ilog2i(64 * rp->rps));
 }
 
+/* The chip-wise count kernel's histogram for one DPU's S block (the source
+ * block's D = 64 * ranks destinations; glb_chipwise_partition_count.c:158-255):
+ * s_dest of every non-padding tuple. bank_set is 8 ... 64 (the kernel only
+ * runs with bank sets). Returns 0 or ORC_E_ARG. */
+int orc_chipwise_partition_count(const orc_tuple *t, int64_t n, int ranks, int rank_sets, int bank_set,
+                                 uint32_t *hist)
+{
+    if (ranks <= 0 || rank_sets <= 0 || ranks % rank_sets || rank_sets > 256) return ORC_E_ARG;
+    if (!(bank_set == 8 || bank_set == 16 || bank_set == 32 || bank_set == 64)) return ORC_E_ARG;
+    refpipe_t rp;
+    memset(&rp, 0, sizeof(rp));
+    rp.ranks = ranks; rp.G = rank_sets; rp.rps = ranks / rank_sets; rp.B = bank_set;
+    if (rp.rps * 64 < bank_set) return ORC_E_ARG;
+    memset(hist, 0, (size_t)ranks * 64 * sizeof(uint32_t));
+    for (int64_t j = 0; j < n; j++)
+        if (t[j].key) hist[s_dest(&rp, t[j], j)]++;
+    return ORC_OK;
+}
+
 static void count_task(void *ctx, int64_t blk)
 {
     refpipe_t *rp = (refpipe_t *)ctx;

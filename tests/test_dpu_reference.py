@@ -1,7 +1,8 @@
 """The oracle against the reference's own DPU join kernels, compiled from the
 reference tree as plain C and run on the host (oracle/dpu_ref.py,
-oracle/dpu_host/): the global partition count of src/dpu/src/join/
-glb_partition_count.c, the local partitioning of
+oracle/dpu_host/): the global partition counts of src/dpu/src/join/
+glb_partition_count.c, glb_chipwise_partition_count.c and
+bg_broadcast_count.c, the local partitioning of
 a2a_packetwise_srj_local_partition.c, the hash build and probe of
 a2a_srj_build.c and a2a_srj_probe_inner_mt.c, the nested loop of
 nested_loop_join.c, the range partitioning and sort-probe of
@@ -34,6 +35,39 @@ def test_partition_count_kernel(oracle, n, P, type_, rank_sets, ranks_per_set):
     assert np.array_equal(hist, want)
     assert np.array_equal(start, (np.cumsum(want) - want).astype(np.uint32))
     assert int(hist.sum()) == int((T[:, 0] != 0).sum())
+
+
+@pytest.mark.parametrize("n", [1, 256, 50001])
+@pytest.mark.parametrize("ranks,rank_sets,bank_set", [(1, 1, 8), (1, 1, 64), (4, 2, 16), (8, 1, 64), (32, 4, 32),
+                                                      (16, 16, 8), (32, 1, 8)])
+def test_chipwise_partition_count_kernel(oracle, n, ranks, rank_sets, bank_set):
+    """glb_chipwise_partition_count.c (S with bank sets): bank group by hash,
+    DPU inside the group by the tuple's index in its 2 KiB block, rank set by
+    the index's slot. Its histogram and start offsets equal the oracle's
+    chip-wise split."""
+    rng = np.random.default_rng(n + ranks * 7 + bank_set)
+    T = _tuples(rng, n)
+    T[::37, 0] = 0
+    hist, start = dpu_ref.chipwise_partition_count(T, ranks, rank_sets, bank_set)
+    want = oracle.chipwise_partition_count(T, ranks, rank_sets, bank_set)
+    assert np.array_equal(hist, want)
+    assert np.array_equal(start, (np.cumsum(want) - want).astype(np.uint32))
+    assert int(hist.sum()) == int((T[:, 0] != 0).sum())
+
+
+@pytest.mark.parametrize("ranks,rank_sets,bank_set", [(1, 1, 64), (4, 2, 16), (32, 4, 8), (64, 2, 8)])
+def test_bg_broadcast_count_kernel(oracle, ranks, rank_sets, bank_set):
+    """bg_broadcast_count.c (R with bank sets) over the ranks per set * 64 /
+    bank_set bank groups the reference passes it: the oracle's hash
+    histogram."""
+    rng = np.random.default_rng(ranks + bank_set)
+    T = _tuples(rng, 30001)
+    T[::29, 0] = 0
+    P = ranks // rank_sets * 64 // bank_set
+    hist, start = dpu_ref.bg_broadcast_count(T, P, bank_set)
+    want = oracle.partition_count(T, P, 0)
+    assert np.array_equal(hist, want)
+    assert np.array_equal(start, (np.cumsum(want) - want).astype(np.uint32))
 
 
 def _join_both(oracle, R, S):
