@@ -3,7 +3,8 @@
  * itself comes from the reference's include/argument.h), and its results read
  * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BGCOUNT,
  * -DGLUE_BUILD, -DGLUE_PROBE, -DGLUE_NL, -DGLUE_LP, -DGLUE_SMP, -DGLUE_SMJ,
- * -DGLUE_NBUILD or -DGLUE_NPROBE. Test infrastructure of the oracle only. */
+ * -DGLUE_NBUILD, -DGLUE_NPROBE or -DGLUE_FINISH. Test infrastructure of the
+ * oracle only. */
 #include <stdbool.h>
 #include <stdint.h>
 
@@ -249,6 +250,22 @@ int dpu_host_get_results(int64_t *o, int cap) {
     return 6;
 }
 
+#elif defined(GLUE_FINISH)
+/* src/dpu/src/join/finish_join.c */
+extern finish_join_arg param_finish_join;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 4) return -1;
+    finish_join_arg *p = &param_finish_join;
+    p->join_result_start_byte = (int32_t)a[0];
+    p->max_bytes = (int32_t)a[1];
+    p->effective_bytes = (int32_t)a[2];
+    p->dummy = (int32_t)a[3];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
+
 #else
-#error "define GLUE_COUNT, GLUE_BGCOUNT, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP, GLUE_SMJ, GLUE_NBUILD or GLUE_NPROBE"
+#error "define GLUE_COUNT, GLUE_BGCOUNT, GLUE_FINISH, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP, GLUE_SMJ, GLUE_NBUILD or GLUE_NPROBE"
 #endif

@@ -4,11 +4,11 @@ Test infrastructure only (tests/ imports it, nothing else): ``make -C oracle
 ref`` compiles glb_partition_count.c, glb_chipwise_partition_count.c,
 bg_broadcast_count.c, a2a_packetwise_srj_local_partition.c,
 a2a_srj_build.c, a2a_srj_probe_inner_mt.c, nested_loop_join.c,
-mpsm_join_local_partition.c, mpsm_join_sort_probe.c and
-packetwise_no_partitioned_hash_join_{build,probe}.c (src/dpu/src/join/ of
+mpsm_join_local_partition.c, mpsm_join_sort_probe.c,
+packetwise_no_partitioned_hash_join_{build,probe}.c and finish_join.c (src/dpu/src/join/ of
 yonsei-hpcp/spid-join) from the reference tree, each with the reference's
 hash.c and the host stand-in for the DPU runtime in oracle/dpu_host/, into
-oracle/_ref/dpu_{count,chipcount,bgcount,lp,build,probe,nl,smp,smj,nbuild,nprobe}.
+oracle/_ref/dpu_{count,chipcount,bgcount,lp,build,probe,nl,smp,smj,nbuild,nprobe,finish}.
 One call of a runner is one DPU launch of 12 tasklets over one MRAM image; this
 module lays the image out, passes the kernel's arguments and reads its results
 back, so that the oracle's restatement of those kernels can be checked against
@@ -22,7 +22,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k)
-           for k in ("count", "chipcount", "bgcount", "build", "probe", "nl", "lp", "smp", "smj", "nbuild", "nprobe")}
+           for k in ("count", "chipcount", "bgcount", "build", "probe", "nl", "lp", "smp", "smj", "nbuild", "nprobe",
+                     "finish")}
 TASKLETS = 12              # NR_TASKLETS of every join kernel
 TABLE_BYTES = 32768        # one local partition's hash table (a2a_srj_build.c: 4096 x 8 B)
 JOIN_TYPE_EQUI = 1         # include/argument.h
@@ -357,3 +358,22 @@ def nphj_table(R, slots):
     if any(res[:4]):
         raise RuntimeError(f"dpu_nbuild reported errors {res[:4]}")
     return img[ht:ht + 8 * slots].view(np.uint32).reshape(slots, 2).copy()
+
+
+def finish_join(block, effective):
+    """finish_join.c on one DPU whose result block is `block` (m pairs, the
+    block's max_bytes = 8 m): the first `effective` pairs are kept and the
+    rest of the block becomes (0, 0), so every DPU's block has the common size
+    the host transfers."""
+    b = np.ascontiguousarray(block, dtype=np.uint32).reshape(-1, 2)
+    m = b.shape[0]
+    if not 0 <= effective <= m:
+        raise ValueError("0 <= effective <= block size")
+    at = 2048
+    mram = np.full(at + _align(m * 8) + 2048, 0xAB, dtype=np.uint8)
+    _put(mram, at, b)
+    res, img = launch("finish", [at, 8 * m, 8 * int(effective), 0], mram)
+    if any(res[:4]):
+        raise RuntimeError(f"dpu_finish reported errors {res[:4]}")
+    assert (img[:at] == 0xAB).all() and (img[at + 8 * m:] == 0xAB).all(), "wrote outside its block"
+    return img[at:at + 8 * m].view(np.uint32).reshape(m, 2).copy()

@@ -365,3 +365,35 @@ def test_nphj_build_chains_restart_at_slot_zero(oracle):
     assert displaced
     for i in displaced:
         assert (table[:i, 0] != 0).all()
+
+
+@pytest.mark.parametrize("m,effective", [(1000, 300), (1000, 0), (1000, 1000), (512, 256), (257, 1), (2048, 2047)])
+def test_finish_join_kernel(m, effective):
+    """finish_join.c keeps a DPU block's first `effective` pairs and turns the
+    rest of the block into (0, 0), writing nothing outside it."""
+    rng = np.random.default_rng(m + effective)
+    block = rng.integers(1, 2**32, (m, 2), dtype=np.uint32)
+    out = dpu_ref.finish_join(block, effective)
+    assert np.array_equal(out[:effective], block[:effective])
+    assert not out[effective:].any()
+
+
+@pytest.mark.parametrize("n", [0, 1, 63, 64, 65, 5000])
+def test_padded_result_layout_matches_finish_join(spj, n):
+    """The facades' padded result layout (FinishJoin with dpu_blocks) is what
+    the reference's finish kernel leaves in each of a rank's 64 DPU blocks of
+    the common size: the block's pairs, then (0, 0) to the block's end."""
+    rng = np.random.default_rng(n)
+    pairs = rng.integers(1, 2**32, (n, 2), dtype=np.uint32)
+    layout = spj._dpu_blocks(pairs)
+    per = layout.shape[0] // 64
+    base, extra = divmod(n, 64)
+    lo = 0
+    for b in range(64):
+        cnt = base + (1 if b < extra else 0)
+        block = rng.integers(1, 2**32, (per, 2), dtype=np.uint32)  # stale bytes past the pairs
+        block[:cnt] = pairs[lo:lo + cnt]
+        if per:
+            assert np.array_equal(dpu_ref.finish_join(block, cnt), layout[b * per:(b + 1) * per])
+        lo += cnt
+    assert lo == n
