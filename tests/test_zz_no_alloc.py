@@ -127,3 +127,35 @@ def test_noalloc_call_leaves_free_device_memory_unchanged(spj):
     torch.cuda.synchronize()
     assert torch.cuda.mem_get_info()[0] == free0
     assert int(n.item()) == S.shape[0]
+
+
+def test_noalloc_captured_in_a_cuda_graph(spj, oracle):
+    """After one call (the per-device set-up), spj_join_noalloc is captured
+    into a CUDA graph on a side stream in global capture mode, which fails any
+    allocation or synchronisation inside the call. Two replays, each on new
+    inputs copied into the same buffers, give those inputs' exact joins."""
+    import torch
+    n_r, n_s = 1 << 18, 1 << 20
+    R0, S0, _ = spj.generate_host(n_r, n_s, 1.0, seed=41)
+    dR, dS = _device(R0), _device(S0)
+    cap = n_s + (1 << 21)
+    out = torch.empty((cap, 2), dtype=torch.int32, device="cuda")
+    n = torch.zeros(1, dtype=torch.int64, device="cuda")
+    args = (dR.data_ptr(), n_r, dS.data_ptr(), n_s, out.data_ptr(), cap, n.data_ptr())
+    spj.check(spj.lib().spj_join_noalloc(*args, None))
+    torch.cuda.synchronize()
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side, capture_error_mode="global"):
+        spj.check(spj.lib().spj_join_noalloc(*args, side.cuda_stream))
+    for seed, zipf in ((42, 1.5), (43, 0.0)):
+        R, S, expect = spj.generate_host(n_r, n_s, zipf, seed=seed)
+        dR.copy_(_device(R))
+        dS.copy_(_device(S))
+        graph.replay()
+        torch.cuda.synchronize()
+        k = int(n.item())
+        got = out[:k].cpu().numpy().view(np.uint32)
+        assert k == n_s and oracle.checksum(got) == expect
+        assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
+    del graph
