@@ -1,10 +1,10 @@
 /* glue.c -- the runner's view of one reference kernel's __host variables: its
  * argument struct set field by field from the runner's integer list (the struct
  * itself comes from the reference's include/argument.h), and its results read
- * back as integers. Built once per kernel with -DGLUE_COUNT, -DGLUE_BGCOUNT,
- * -DGLUE_BUILD, -DGLUE_PROBE, -DGLUE_NL, -DGLUE_LP, -DGLUE_SMP, -DGLUE_SMJ,
- * -DGLUE_NBUILD, -DGLUE_NPROBE or -DGLUE_FINISH. Test infrastructure of the
- * oracle only. */
+ * back as integers. Built once per kernel with one of -DGLUE_COUNT,
+ * -DGLUE_PACKET, -DGLUE_BGCOUNT, -DGLUE_BUILD, -DGLUE_PROBE, -DGLUE_NL,
+ * -DGLUE_LP, -DGLUE_SMP, -DGLUE_SMJ, -DGLUE_NBUILD, -DGLUE_NPROBE or
+ * -DGLUE_FINISH. Test infrastructure of the oracle only. */
 #include <stdbool.h>
 #include <stdint.h>
 
@@ -40,6 +40,36 @@ int dpu_host_set_args(const int64_t *a, int n) {
     p->num_rank_in_rankgroup = (int32_t)a[9];
     p->join_type = (int32_t)a[10];
     p->hist_interval = (int32_t)a[11];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
+
+#elif defined(GLUE_PACKET)
+/* src/dpu/src/join/glb_partition_packet.c */
+extern glb_partition_packet_arg param_glb_partition_packet;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 18) return -1;
+    glb_partition_packet_arg *p = &param_glb_partition_packet;
+    p->dpu_id = (int32_t)a[0];
+    p->rank_id = (int32_t)a[1];
+    p->input_type = (int32_t)a[2];
+    p->partition_type = (int32_t)a[3];
+    p->input_offset1 = (int32_t)a[4];
+    p->input_offset2 = (int32_t)a[5];
+    p->elem_num = (int32_t)a[6];
+    p->histogram_start_byte = (int32_t)a[7];
+    p->packet_histogram_start_byte = (int32_t)a[8];
+    p->partition_num = (int32_t)a[9];
+    p->result_offset = (int32_t)a[10];
+    p->packet_size = (int32_t)a[11];
+    p->partition_start = (int32_t)a[12];
+    p->bankgroup = (int32_t)a[13];
+    p->num_rankgroup = (int32_t)a[14];
+    p->num_rank_in_rankgroup = (int32_t)a[15];
+    p->join_type = (int32_t)a[16];
+    p->hist_interval = (int32_t)a[17];
     return 0;
 }
 
@@ -267,5 +297,5 @@ int dpu_host_set_args(const int64_t *a, int n) {
 int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
 
 #else
-#error "define GLUE_COUNT, GLUE_BGCOUNT, GLUE_FINISH, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP, GLUE_SMJ, GLUE_NBUILD or GLUE_NPROBE"
+#error "define GLUE_COUNT, GLUE_PACKET, GLUE_BGCOUNT, GLUE_FINISH, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP, GLUE_SMJ, GLUE_NBUILD or GLUE_NPROBE"
 #endif

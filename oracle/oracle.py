@@ -64,6 +64,8 @@ def lib():
         L.orc_local_partition.argtypes = [vp, i64, i64, vp, vp]
         L.orc_dpu_phj.restype = i64
         L.orc_dpu_phj.argtypes = [vp, i64, vp, i64, vp]
+        L.orc_glb_partition_dest.restype = None
+        L.orc_glb_partition_dest.argtypes = [vp, i64, i32, i32, i32, i32, vp]
         L.orc_chipwise_partition_count.restype = i32
         L.orc_chipwise_partition_count.argtypes = [vp, i64, i32, i32, i32, vp]
         L.orc_dpu_smj.restype = i64
@@ -154,6 +156,15 @@ def partition_count(tuples, P, type_=0, rank_sets=1, ranks_per_set=1):
     hist = np.zeros(P, dtype=np.uint32)
     lib().orc_glb_partition_count(_ptr(t), t.shape[0], type_, P, rank_sets, ranks_per_set, _ptr(hist))
     return hist
+
+
+def partition_dest(tuples, P, type_=0, rank_sets=1, ranks_per_set=1):
+    """Each tuple's global partition as partition_count assigns it (-1 for
+    padding, key 0)."""
+    t = _tuples(tuples)
+    dest = np.empty(t.shape[0], dtype=np.int32)
+    lib().orc_glb_partition_dest(_ptr(t), t.shape[0], type_, P, rank_sets, ranks_per_set, _ptr(dest))
+    return dest
 
 
 def chipwise_partition_count(tuples, ranks, rank_sets, bank_set):

@@ -203,23 +203,30 @@ static void parallel_for(int nthreads, int64_t n, task_fn fn, void *ctx)
  *             where i is the tuple's index inside its 2048-byte read block
  *             (ELEM_PER_BLOCK2 = 256 tuples, :317-318).
  * hist must hold P counters; key-0 tuples are skipped (:190-192). */
+static inline uint32_t glb_dest(uint32_t key, int64_t j, int type, int P, int rank_sets, int ranks_per_set)
+{
+    uint32_t h = orc_glb_partition_hash(key);
+    if (type == 0) return h & (uint32_t)(P - 1);
+    uint32_t i = (uint32_t)(j & 255);
+    return (h & (uint32_t)(P / rank_sets - 1)) + (i & (uint32_t)(rank_sets - 1)) * (uint32_t)(ranks_per_set * 64);
+}
+
 void orc_glb_partition_count(const orc_tuple *t, int64_t n, int type, int P, int rank_sets,
                              int ranks_per_set, uint32_t *hist)
 {
     memset(hist, 0, (size_t)P * sizeof(uint32_t));
-    for (int64_t j = 0; j < n; j++) {
-        if (t[j].key == 0) continue;
-        uint32_t h = orc_glb_partition_hash(t[j].key);
-        uint32_t id;
-        if (type == 0) {
-            id = h & (uint32_t)(P - 1);
-        } else {
-            uint32_t i = (uint32_t)(j & 255);
-            id = (h & (uint32_t)(P / rank_sets - 1)) +
-                 (i & (uint32_t)(rank_sets - 1)) * (uint32_t)(ranks_per_set * 64);
-        }
-        hist[id]++;
-    }
+    for (int64_t j = 0; j < n; j++)
+        if (t[j].key) hist[glb_dest(t[j].key, j, type, P, rank_sets, ranks_per_set)]++;
+}
+
+/* The destination the count above gives each tuple of one DPU's block (-1 for
+ * padding): the partition the packet scatter writes it to
+ * (glb_partition_packet.c:418-431, 531-544). */
+void orc_glb_partition_dest(const orc_tuple *t, int64_t n, int type, int P, int rank_sets, int ranks_per_set,
+                            int32_t *dest)
+{
+    for (int64_t j = 0; j < n; j++)
+        dest[j] = t[j].key ? (int32_t)glb_dest(t[j].key, j, type, P, rank_sets, ranks_per_set) : -1;
 }
 
 /* ---------------------------------------------------------- simple join -- */

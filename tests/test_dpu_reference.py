@@ -1,15 +1,20 @@
 """The oracle against the reference's own DPU join kernels, compiled from the
 reference tree as plain C and run on the host (oracle/dpu_ref.py,
-oracle/dpu_host/): the global partition counts of src/dpu/src/join/
-glb_partition_count.c, glb_chipwise_partition_count.c and
-bg_broadcast_count.c, the local partitioning of
-a2a_packetwise_srj_local_partition.c, the hash build and probe of
-a2a_srj_build.c and a2a_srj_probe_inner_mt.c, the nested loop of
-nested_loop_join.c, the range partitioning and sort-probe of
-mpsm_join_local_partition.c and mpsm_join_sort_probe.c, and the
-non-partitioned hash join of packetwise_no_partitioned_hash_join_{build,probe}.c
-must give what the oracle's restatement gives on the same inputs. The runners exist only where the reference tree was present when
-the oracle was built; elsewhere these tests are skipped."""
+oracle/dpu_host/). The kernels, all under src/dpu/src/join/, are these:
+  - the global partition counts of glb_partition_count.c,
+    glb_chipwise_partition_count.c and bg_broadcast_count.c;
+  - the packet scatter of glb_partition_packet.c;
+  - the local partitioning of a2a_packetwise_srj_local_partition.c;
+  - the hash build and probe of a2a_srj_build.c and a2a_srj_probe_inner_mt.c;
+  - the nested loop of nested_loop_join.c;
+  - the range partitioning and sort-probe of mpsm_join_local_partition.c and
+    mpsm_join_sort_probe.c;
+  - the non-partitioned hash join of
+    packetwise_no_partitioned_hash_join_{build,probe}.c;
+  - the finish kernel of finish_join.c.
+Each must give what the oracle's restatement gives on the same inputs. The
+runners exist only where the reference tree was present when the oracle was
+built; elsewhere these tests are skipped."""
 import numpy as np
 import pytest
 
@@ -35,6 +40,35 @@ def test_partition_count_kernel(oracle, n, P, type_, rank_sets, ranks_per_set):
     assert np.array_equal(hist, want)
     assert np.array_equal(start, (np.cumsum(want) - want).astype(np.uint32))
     assert int(hist.sum()) == int((T[:, 0] != 0).sum())
+
+
+@pytest.mark.parametrize("n", [1, 256, 20001])
+@pytest.mark.parametrize("ranks,rank_sets,dpu_id,packet_size", [(1, 1, 0, 8), (4, 1, 8, 8), (4, 2, 19, 16),
+                                                                (8, 4, 63, 64), (32, 1, 40, 128), (16, 16, 7, 8)])
+def test_packet_scatter_kernel(oracle, n, ranks, rank_sets, dpu_id, packet_size):
+    """glb_partition_count.c, then glb_partition_packet.c with the packet
+    counts the host derives from the histogram. The scatter's own check (its
+    per-destination counts equal the count kernel's) passes, and every
+    destination DPU's packets, read through the rotated layout, hold exactly
+    the tuples the oracle sends there, then (0, 0)."""
+    rng = np.random.default_rng(n + ranks + dpu_id)
+    T = _tuples(rng, n)
+    T[::53, 0] = 0
+    groups = dpu_ref.packet_scatter(T, ranks, rank_sets, dpu_id, packet_size)
+    dest = oracle.partition_dest(T, 64 * ranks, 0 if rank_sets == 1 else 1, rank_sets, ranks // rank_sets)
+    assert len(groups) == 64 * ranks
+    for d, g in enumerate(groups):
+        assert np.array_equal(oracle.sort_pairs(g), oracle.sort_pairs(T[dest == d]))
+    assert sum(g.shape[0] for g in groups) == int((T[:, 0] != 0).sum())
+
+
+def test_packet_rounds_follow_the_fullest_destination():
+    """The host sizes a destination rank's packets by its fullest DPU, in
+    packets of packet_size / 8 tuples, and gives an empty rank one packet."""
+    hist = np.zeros(3 * 64, dtype=np.int64)
+    hist[5], hist[64 + 63], hist[64 + 1] = 9, 17, 3
+    assert list(dpu_ref.packet_rounds(hist, 3, 8)) == [9, 17, 1]
+    assert list(dpu_ref.packet_rounds(hist, 3, 32)) == [3, 5, 1]
 
 
 @pytest.mark.parametrize("n", [1, 256, 50001])
