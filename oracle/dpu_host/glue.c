@@ -46,7 +46,7 @@ int dpu_host_set_args(const int64_t *a, int n) {
 int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
 
 #elif defined(GLUE_PACKET)
-/* src/dpu/src/join/glb_partition_packet.c */
+/* src/dpu/src/join/glb_partition_packet.c and glb_chipwise_partition_packet.c */
 extern glb_partition_packet_arg param_glb_partition_packet;
 
 int dpu_host_set_args(const int64_t *a, int n) {

@@ -1,15 +1,23 @@
 """The reference's own DPU join kernels, run on the host.
 
-Test infrastructure only (tests/ imports it, nothing else): ``make -C oracle
-ref`` compiles glb_partition_count.c, glb_partition_packet.c,
-glb_chipwise_partition_count.c,
-bg_broadcast_count.c, a2a_packetwise_srj_local_partition.c,
-a2a_srj_build.c, a2a_srj_probe_inner_mt.c, nested_loop_join.c,
-mpsm_join_local_partition.c, mpsm_join_sort_probe.c,
-packetwise_no_partitioned_hash_join_{build,probe}.c and finish_join.c (src/dpu/src/join/ of
-yonsei-hpcp/spid-join) from the reference tree, each with the reference's
-hash.c and the host stand-in for the DPU runtime in oracle/dpu_host/, into
-oracle/_ref/dpu_{count,packet,chipcount,bgcount,lp,build,probe,nl,smp,smj,nbuild,nprobe,finish}.
+Test infrastructure only (tests/ imports it, nothing else). ``make -C oracle
+ref`` compiles these kernels of yonsei-hpcp/spid-join (src/dpu/src/join/) from
+the reference tree, each with the reference's hash.c and the host stand-in for
+the DPU runtime in oracle/dpu_host/, into oracle/_ref/dpu_<name>:
+  count       glb_partition_count.c
+  packet      glb_partition_packet.c
+  chipcount   glb_chipwise_partition_count.c
+  chippacket  glb_chipwise_partition_packet.c
+  bgcount     bg_broadcast_count.c
+  lp          a2a_packetwise_srj_local_partition.c
+  build       a2a_srj_build.c
+  probe       a2a_srj_probe_inner_mt.c
+  nl          nested_loop_join.c
+  smp         mpsm_join_local_partition.c
+  smj         mpsm_join_sort_probe.c
+  nbuild      packetwise_no_partitioned_hash_join_build.c
+  nprobe      packetwise_no_partitioned_hash_join_probe.c
+  finish      finish_join.c
 One call of a runner is one DPU launch of 12 tasklets over one MRAM image; this
 module lays the image out, passes the kernel's arguments and reads its results
 back, so that the oracle's restatement of those kernels can be checked against
@@ -23,7 +31,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k)
-           for k in ("count", "packet", "chipcount", "bgcount", "build", "probe", "nl", "lp", "smp", "smj", "nbuild", "nprobe",
+           for k in ("count", "packet", "chipcount", "chippacket", "bgcount", "build", "probe", "nl", "lp", "smp", "smj", "nbuild", "nprobe",
                      "finish")}
 TASKLETS = 12              # NR_TASKLETS of every join kernel
 TABLE_BYTES = 32768        # one local partition's hash table (a2a_srj_build.c: 4096 x 8 B)
@@ -94,21 +102,29 @@ def packet_rounds(hist, ranks, packet_size):
     return np.maximum(1, -(-top // per))
 
 
-def packet_scatter(tuples, ranks, rank_sets=1, dpu_id=0, packet_size=8):
-    """glb_partition_count.c, then glb_partition_packet.c, on one DPU (number
-    dpu_id of its rank) holding `tuples`, for 64 * ranks destinations (with
-    rank_sets > 1 the index-based rank-set split of S). The scatter writes each
-    destination DPU's tuples into its packets: for destination rank r a region
-    of packet_rounds[r] rounds of 64 packets, the packet of DPU m at slot
-    ((m / 8 - dpu_id / 8) mod 8) + 8 (m mod 8) of each round (the rotation that
-    staggers the source DPUs of a bank group). Returns, per destination, its
-    packets' slots in order (padding beyond its count is checked to be (0, 0))."""
+def packet_scatter(tuples, ranks, rank_sets=1, dpu_id=0, packet_size=8, bank_set=1, errors=None):
+    """The count kernel, then the packet scatter, on one DPU (number dpu_id of
+    its rank) holding `tuples`, for 64 * ranks destinations: with bank_set 1
+    glb_partition_count.c and glb_partition_packet.c (rank_sets > 1: the
+    index-based rank-set split of S), with bank_set 8 ... 64 the chip-wise
+    glb_chipwise_partition_count.c and glb_chipwise_partition_packet.c. The
+    scatter writes each destination DPU's tuples into its packets: for
+    destination rank r a region of packet_rounds[r] rounds of 64 packets, the
+    packet of DPU m at slot ((m / 8 - dpu_id / 8) mod 8) + 8 (m mod 8) of each
+    round (the rotation that staggers the source DPUs of a bank group).
+    Returns, per destination, its packets' slots in order (padding beyond its
+    count is checked to be (0, 0)). The kernel's error fields go to `errors`
+    (a list) if given; otherwise any nonzero one raises."""
     t = np.ascontiguousarray(tuples, dtype=np.uint32).reshape(-1, 2)
     n, P = t.shape[0], 64 * ranks
     if P > 2048 or ranks % rank_sets or packet_size not in (8, 16, 32, 64, 128) or not 0 <= dpu_id < 64:
         raise ValueError("64 * ranks <= 2048, rank_sets dividing ranks, packet_size 8..128, dpu_id < 64")
-    type_ = 0 if rank_sets == 1 else 1
-    hist, _ = partition_count(t, P, type_, rank_sets, ranks // rank_sets)
+    if bank_set == 1:
+        type_, kernel = (0 if rank_sets == 1 else 1), "packet"
+        hist, _ = partition_count(t, P, type_, rank_sets, ranks // rank_sets)
+    else:
+        type_, kernel = 1, "chippacket"
+        hist, _ = chipwise_partition_count(t, ranks, rank_sets, bank_set)
     rounds = packet_rounds(hist, ranks, packet_size)
     acc = np.concatenate([[0], np.cumsum(rounds)])
     hist_at = _align(n * 8) + 2048
@@ -119,11 +135,13 @@ def packet_scatter(tuples, ranks, rank_sets=1, dpu_id=0, packet_size=8):
     _put(mram, 0, t)
     _put(mram, hist_at, hist.astype(np.uint32))
     _put(mram, ph_at, rounds.astype(np.int64))
-    args = [dpu_id, 0, 0, type_, 0, 0, n, hist_at, ph_at, P, res_at, packet_size, 0, 1, rank_sets,
+    args = [dpu_id, 0, 0, type_, 0, 0, n, hist_at, ph_at, P, res_at, packet_size, 0, bank_set, rank_sets,
             ranks // rank_sets, JOIN_TYPE_EQUI, 0]
-    res, img = launch("packet", args, mram)
-    if any(res[:4]):
-        raise RuntimeError(f"dpu_packet reported errors {res[:4]}")  # its counts differ from the count kernel's
+    res, img = launch(kernel, args, mram)
+    if errors is not None:
+        errors[:] = res[:4]
+    elif any(res[:4]):
+        raise RuntimeError(f"dpu_{kernel} reported errors {res[:4]}")  # e.g. its counts differ from the count kernel's
     region = img[res_at:res_at + res_bytes].view(np.uint32).reshape(-1, 2)
     per = packet_size // 8
     out = []

@@ -66,6 +66,8 @@ def lib():
         L.orc_dpu_phj.argtypes = [vp, i64, vp, i64, vp]
         L.orc_glb_partition_dest.restype = None
         L.orc_glb_partition_dest.argtypes = [vp, i64, i32, i32, i32, i32, vp]
+        L.orc_chipwise_partition_dest.restype = i32
+        L.orc_chipwise_partition_dest.argtypes = [vp, i64, i32, i32, i32, vp]
         L.orc_chipwise_partition_count.restype = i32
         L.orc_chipwise_partition_count.argtypes = [vp, i64, i32, i32, i32, vp]
         L.orc_dpu_smj.restype = i64
@@ -177,6 +179,16 @@ def chipwise_partition_count(tuples, ranks, rank_sets, bank_set):
     if rc:
         raise RuntimeError(ERRORS.get(rc, rc))
     return hist
+
+
+def chipwise_partition_dest(tuples, ranks, rank_sets, bank_set):
+    """Each tuple's destination under the chip-wise split (-1 for padding)."""
+    t = _tuples(tuples)
+    dest = np.empty(t.shape[0], dtype=np.int32)
+    rc = lib().orc_chipwise_partition_dest(_ptr(t), t.shape[0], ranks, rank_sets, bank_set, _ptr(dest))
+    if rc:
+        raise RuntimeError(ERRORS.get(rc, rc))
+    return dest
 
 
 def simple_join(R, S, keep_unmatched=False):

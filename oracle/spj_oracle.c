@@ -221,7 +221,7 @@ void orc_glb_partition_count(const orc_tuple *t, int64_t n, int type, int P, int
 
 /* The destination the count above gives each tuple of one DPU's block (-1 for
  * padding): the partition the packet scatter writes it to
- * (glb_partition_packet.c:418-431, 531-544). */
+ * (glb_partition_packet.c:430-431, 543-544). */
 void orc_glb_partition_dest(const orc_tuple *t, int64_t n, int type, int P, int rank_sets, int ranks_per_set,
                             int32_t *dest)
 {
@@ -357,18 +357,36 @@ static inline int s_dest(const refpipe_t *rp, orc_tuple t, int64_t j)
  * block's D = 64 * ranks destinations; glb_chipwise_partition_count.c:158-255):
  * s_dest of every non-padding tuple. bank_set is 8 ... 64 (the kernel only
  * runs with bank sets). Returns 0 or ORC_E_ARG. */
-int orc_chipwise_partition_count(const orc_tuple *t, int64_t n, int ranks, int rank_sets, int bank_set,
-                                 uint32_t *hist)
+static int chipwise_setup(refpipe_t *rp, int ranks, int rank_sets, int bank_set)
 {
     if (ranks <= 0 || rank_sets <= 0 || ranks % rank_sets || rank_sets > 256) return ORC_E_ARG;
     if (!(bank_set == 8 || bank_set == 16 || bank_set == 32 || bank_set == 64)) return ORC_E_ARG;
+    memset(rp, 0, sizeof(*rp));
+    rp->ranks = ranks; rp->G = rank_sets; rp->rps = ranks / rank_sets; rp->B = bank_set;
+    return rp->rps * 64 < bank_set ? ORC_E_ARG : ORC_OK;
+}
+
+int orc_chipwise_partition_count(const orc_tuple *t, int64_t n, int ranks, int rank_sets, int bank_set,
+                                 uint32_t *hist)
+{
     refpipe_t rp;
-    memset(&rp, 0, sizeof(rp));
-    rp.ranks = ranks; rp.G = rank_sets; rp.rps = ranks / rank_sets; rp.B = bank_set;
-    if (rp.rps * 64 < bank_set) return ORC_E_ARG;
+    const int e = chipwise_setup(&rp, ranks, rank_sets, bank_set);
+    if (e) return e;
     memset(hist, 0, (size_t)ranks * 64 * sizeof(uint32_t));
     for (int64_t j = 0; j < n; j++)
         if (t[j].key) hist[s_dest(&rp, t[j], j)]++;
+    return ORC_OK;
+}
+
+/* Each tuple's destination under the chip-wise split (-1 for padding): where
+ * glb_chipwise_partition_packet.c:468-472 scatters it. */
+int orc_chipwise_partition_dest(const orc_tuple *t, int64_t n, int ranks, int rank_sets, int bank_set,
+                                int32_t *dest)
+{
+    refpipe_t rp;
+    const int e = chipwise_setup(&rp, ranks, rank_sets, bank_set);
+    if (e) return e;
+    for (int64_t j = 0; j < n; j++) dest[j] = t[j].key ? s_dest(&rp, t[j], j) : -1;
     return ORC_OK;
 }
 

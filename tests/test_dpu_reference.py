@@ -3,7 +3,8 @@ reference tree as plain C and run on the host (oracle/dpu_ref.py,
 oracle/dpu_host/). The kernels, all under src/dpu/src/join/, are these:
   - the global partition counts of glb_partition_count.c,
     glb_chipwise_partition_count.c and bg_broadcast_count.c;
-  - the packet scatter of glb_partition_packet.c;
+  - the packet scatters of glb_partition_packet.c and
+    glb_chipwise_partition_packet.c;
   - the local partitioning of a2a_packetwise_srj_local_partition.c;
   - the hash build and probe of a2a_srj_build.c and a2a_srj_probe_inner_mt.c;
   - the nested loop of nested_loop_join.c;
@@ -431,3 +432,37 @@ def test_padded_result_layout_matches_finish_join(spj, n):
             assert np.array_equal(dpu_ref.finish_join(block, cnt), layout[b * per:(b + 1) * per])
         lo += cnt
     assert lo == n
+
+
+@pytest.mark.parametrize("n", [1, 256, 20001])
+@pytest.mark.parametrize("ranks,rank_sets,bank_set,dpu_id,packet_size", [(1, 1, 8, 0, 8), (4, 2, 16, 8, 16),
+                                                                         (8, 1, 64, 63, 64), (32, 4, 32, 21, 8),
+                                                                         (16, 16, 8, 35, 128)])
+def test_chipwise_packet_scatter_kernel(oracle, n, ranks, rank_sets, bank_set, dpu_id, packet_size):
+    """glb_chipwise_partition_count.c, then glb_chipwise_partition_packet.c
+    (S with bank sets) with the host's packet counts: every destination DPU's
+    packets hold exactly the tuples the oracle's chip-wise split sends there,
+    then (0, 0), and the kernel reports no error."""
+    rng = np.random.default_rng(n + ranks + bank_set + dpu_id)
+    T = _tuples(rng, n, key_hi=2**31)
+    T[::53, 0] = 0
+    groups = dpu_ref.packet_scatter(T, ranks, rank_sets, dpu_id, packet_size, bank_set=bank_set)
+    dest = oracle.chipwise_partition_dest(T, ranks, rank_sets, bank_set)
+    for d, g in enumerate(groups):
+        assert np.array_equal(oracle.sort_pairs(g), oracle.sort_pairs(T[dest == d]))
+    assert sum(g.shape[0] for g in groups) == int((T[:, 0] != 0).sum())
+
+
+def test_chipwise_packet_scatter_flags_high_keys(oracle):
+    """The chip-wise scatter sets ERROR_TYPE_3 = 1 for a key of 2^31 or above
+    (it tests the key as a signed integer) and scatters the tuple all the
+    same, to the oracle's destination."""
+    rng = np.random.default_rng(77)
+    T = _tuples(rng, 5000, key_hi=2**31)
+    T[17, 0] = 0x80000001
+    errors = []
+    groups = dpu_ref.packet_scatter(T, 4, 1, 0, 8, bank_set=16, errors=errors)
+    assert errors == [0, 0, 0, 1]
+    dest = oracle.chipwise_partition_dest(T, 4, 1, 16)
+    for d, g in enumerate(groups):
+        assert np.array_equal(oracle.sort_pairs(g), oracle.sort_pairs(T[dest == d]))
