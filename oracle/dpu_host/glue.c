@@ -2,7 +2,7 @@
  * argument struct set field by field from the runner's integer list (the struct
  * itself comes from the reference's include/argument.h), and its results read
  * back as integers. Built once per kernel with one of -DGLUE_COUNT,
- * -DGLUE_PACKET, -DGLUE_BGCOUNT, -DGLUE_BUILD, -DGLUE_PROBE, -DGLUE_NL,
+ * -DGLUE_PACKET, -DGLUE_BGCOUNT, -DGLUE_BGALIGN, -DGLUE_BUILD, -DGLUE_PROBE, -DGLUE_NL,
  * -DGLUE_LP, -DGLUE_SMP, -DGLUE_SMJ, -DGLUE_NBUILD, -DGLUE_NPROBE or
  * -DGLUE_FINISH. Test infrastructure of the oracle only. */
 #include <stdbool.h>
@@ -90,6 +90,28 @@ int dpu_host_set_args(const int64_t *a, int n) {
     p->bankgroup = (int32_t)a[5];
     p->rankgroup = (int32_t)a[6];
     p->padding = (int32_t)a[7];
+    return 0;
+}
+
+int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
+
+#elif defined(GLUE_BGALIGN)
+/* src/dpu/src/join/bg_broadcast_align.c */
+extern bg_broadcast_align_arg param_bg_broadcast_align;
+
+int dpu_host_set_args(const int64_t *a, int n) {
+    if (n != 10) return -1;
+    bg_broadcast_align_arg *p = &param_bg_broadcast_align;
+    p->elem_num = (uint32_t)a[0];
+    p->partition_num = (uint32_t)a[1];
+    p->tid_offset = (uint32_t)a[2];
+    p->payload_offset = (uint32_t)a[3];
+    p->result_offset = (uint32_t)a[4];
+    p->global_histogram_start_byte = (uint32_t)a[5];
+    p->aggr_histogram_start_byte = (uint32_t)a[6];
+    p->bankgroup = (int32_t)a[7];
+    p->rankgroup = (int32_t)a[8];
+    p->padding = (int32_t)a[9];
     return 0;
 }
 
@@ -297,5 +319,5 @@ int dpu_host_set_args(const int64_t *a, int n) {
 int dpu_host_get_results(int64_t *o, int cap) { return cap < 4 ? 0 : errors_out(o); }
 
 #else
-#error "define GLUE_COUNT, GLUE_PACKET, GLUE_BGCOUNT, GLUE_FINISH, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP, GLUE_SMJ, GLUE_NBUILD or GLUE_NPROBE"
+#error "define GLUE_COUNT, GLUE_PACKET, GLUE_BGCOUNT, GLUE_BGALIGN, GLUE_FINISH, GLUE_BUILD, GLUE_PROBE, GLUE_NL, GLUE_LP, GLUE_SMP, GLUE_SMJ, GLUE_NBUILD or GLUE_NPROBE"
 #endif

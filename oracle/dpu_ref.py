@@ -9,6 +9,7 @@ the DPU runtime in oracle/dpu_host/, into oracle/_ref/dpu_<name>:
   chipcount   glb_chipwise_partition_count.c
   chippacket  glb_chipwise_partition_packet.c
   bgcount     bg_broadcast_count.c
+  bgalign     bg_broadcast_align.c
   lp          a2a_packetwise_srj_local_partition.c
   build       a2a_srj_build.c
   probe       a2a_srj_probe_inner_mt.c
@@ -31,7 +32,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 RUNNERS = {k: os.path.join(HERE, "_ref", "dpu_" + k)
-           for k in ("count", "packet", "chipcount", "chippacket", "bgcount", "build", "probe", "nl", "lp", "smp", "smj", "nbuild", "nprobe",
+           for k in ("count", "packet", "chipcount", "chippacket", "bgcount", "bgalign", "build", "probe", "nl", "lp", "smp", "smj", "nbuild", "nprobe",
                      "finish")}
 TASKLETS = 12              # NR_TASKLETS of every join kernel
 TABLE_BYTES = 32768        # one local partition's hash table (a2a_srj_build.c: 4096 x 8 B)
@@ -194,6 +195,48 @@ def bg_broadcast_count(tuples, partitions, bank_set):
     if any(res[:4]):
         raise RuntimeError(f"dpu_bgcount reported errors {res[:4]}")
     return (img[hist:hist + 4 * P].view(np.uint32).copy(), img[info:info + 4 * P].view(np.uint32).copy())
+
+
+def bg_broadcast_align(tuples, ranks_per_set, bank_set, errors=None):
+    """bg_broadcast_count.c, then bg_broadcast_align.c, on one DPU holding R
+    block `tuples` with bank sets of `bank_set`: the tuples grouped by their
+    ranks_per_set * 64 / bank_set bank groups. Each bank group of rank r gets a
+    slot of the size the host gives that rank (its fullest bank group,
+    src/queryHostFunc.cc:1731-1770), the slots laid out rank after rank.
+    Returns, per bank group, its slot's first `count` tuples (the rest of the
+    slot is checked to be (0, 0)). The kernel's error fields go to `errors` (a
+    list) if given; otherwise any nonzero one raises."""
+    t = np.ascontiguousarray(tuples, dtype=np.uint32).reshape(-1, 2)
+    n = t.shape[0]
+    per_rank = 64 // bank_set
+    P = ranks_per_set * per_rank
+    if bank_set not in (8, 16, 32, 64) or P > 2048:
+        raise ValueError("bank_set in 8..64 and ranks_per_set * 64 / bank_set <= 2048")
+    hist, _ = bg_broadcast_count(t, P, bank_set)
+    slot = hist.astype(np.int64).reshape(ranks_per_set, per_rank).max(axis=1)
+    start = np.concatenate([[0], np.cumsum(slot * per_rank)])
+    addr = np.array([start[i // per_rank] + (i % per_rank) * slot[i // per_rank] for i in range(P)], dtype=np.int64)
+    gh_at = _align(n * 8) + 2048
+    ah_at = gh_at + _align(P * 4) + 2048
+    res_at = ah_at + _align(ranks_per_set * 4) + 2048
+    res_n = int(start[-1])
+    mram = np.zeros(res_at + _align(res_n * 8) + 2048, dtype=np.uint8)
+    _put(mram, 0, t)
+    _put(mram, gh_at, hist.astype(np.uint32))
+    _put(mram, ah_at, slot.astype(np.uint32))
+    res, img = launch("bgalign", [n, P, 0, 0, res_at, gh_at, ah_at, bank_set, 1, 0], mram)
+    if errors is not None:
+        errors[:] = res[:4]
+    elif any(res[:4]):
+        raise RuntimeError(f"dpu_bgalign reported errors {res[:4]}")  # e.g. its counts differ from the count kernel's
+    region = img[res_at:res_at + 8 * res_n].view(np.uint32).reshape(res_n, 2)
+    out = []
+    for i in range(P):
+        a, c, w = int(addr[i]), int(hist[i]), int(slot[i // per_rank])
+        if region[a + c:a + w].any():
+            raise RuntimeError(f"bank group {i}: tuples past its count")
+        out.append(region[a:a + c].copy())
+    return out
 
 
 def hash_join(r_grouped, r_off, s_grouped, s_off):

@@ -4,7 +4,8 @@ oracle/dpu_host/). The kernels, all under src/dpu/src/join/, are these:
   - the global partition counts of glb_partition_count.c,
     glb_chipwise_partition_count.c and bg_broadcast_count.c;
   - the packet scatters of glb_partition_packet.c and
-    glb_chipwise_partition_packet.c;
+    glb_chipwise_partition_packet.c, and the bank-group R layout of
+    bg_broadcast_align.c;
   - the local partitioning of a2a_packetwise_srj_local_partition.c;
   - the hash build and probe of a2a_srj_build.c and a2a_srj_probe_inner_mt.c;
   - the nested loop of nested_loop_join.c;
@@ -103,6 +104,36 @@ def test_bg_broadcast_count_kernel(oracle, ranks, rank_sets, bank_set):
     want = oracle.partition_count(T, P, 0)
     assert np.array_equal(hist, want)
     assert np.array_equal(start, (np.cumsum(want) - want).astype(np.uint32))
+
+
+@pytest.mark.parametrize("ranks_per_set,bank_set", [(1, 64), (1, 8), (4, 16), (32, 8), (8, 32)])
+def test_bg_broadcast_align_kernel(oracle, ranks_per_set, bank_set):
+    """bg_broadcast_count.c, then bg_broadcast_align.c (R with bank sets) with
+    the slot sizes the host derives: each bank group's slot holds exactly the R
+    tuples the oracle sends to that bank group, then (0, 0), and the kernel's
+    own check (its counts equal the count kernel's) passes."""
+    rng = np.random.default_rng(ranks_per_set * 3 + bank_set)
+    T = _tuples(rng, 30001, key_hi=2**31)
+    T[::29, 0] = 0
+    groups = dpu_ref.bg_broadcast_align(T, ranks_per_set, bank_set)
+    dest = oracle.partition_dest(T, ranks_per_set * 64 // bank_set, 0)
+    for i, g in enumerate(groups):
+        assert np.array_equal(oracle.sort_pairs(g), oracle.sort_pairs(T[dest == i]))
+    assert sum(g.shape[0] for g in groups) == int((T[:, 0] != 0).sum())
+
+
+def test_bg_broadcast_align_flags_high_keys(oracle):
+    """Like the chip-wise scatter, the align kernel sets ERROR_TYPE_3 = 1 for a
+    key of 2^31 or above and still places the tuple in its bank group."""
+    rng = np.random.default_rng(78)
+    T = _tuples(rng, 4000, key_hi=2**31)
+    T[5, 0] = 0xFFFFFFF0
+    errors = []
+    groups = dpu_ref.bg_broadcast_align(T, 2, 16, errors=errors)
+    assert errors == [0, 0, 0, 1]
+    dest = oracle.partition_dest(T, 2 * 64 // 16, 0)
+    for i, g in enumerate(groups):
+        assert np.array_equal(oracle.sort_pairs(g), oracle.sort_pairs(T[dest == i]))
 
 
 def _join_both(oracle, R, S):
