@@ -497,3 +497,77 @@ def test_chipwise_packet_scatter_flags_high_keys(oracle):
     dest = oracle.chipwise_partition_dest(T, 4, 1, 16)
     for d, g in enumerate(groups):
         assert np.array_equal(oracle.sort_pairs(g), oracle.sort_pairs(T[dest == d]))
+
+
+def _split_blocks(T, D):
+    """LoadColumn's split of a column over D DPUs (src/query.cc:230-300): padded
+    with key-0 tuples to a multiple of D * 8 bytes (a whole extra row when it is
+    aligned already) and cut into D equal blocks."""
+    per = (T.shape[0] * 8 + (D * 8 - T.shape[0] * 8 % (D * 8))) // 8 // D
+    padded = np.zeros((per * D, 2), dtype=np.uint32)
+    padded[:T.shape[0]] = T
+    return [padded[b * per:(b + 1) * per] for b in range(D)]
+
+
+def test_reference_kernels_over_one_rank(oracle):
+    """The reference's join on one rank of 64 DPUs, every DPU step by its own
+    kernels run on the host. Each source DPU's block goes through the count
+    kernel and the packet scatter. The exchange hands each destination DPU the
+    packets addressed to it (the host's rotate-and-stream only moves them).
+    Each destination DPU then runs local partitioning of R, of S with R's
+    partition count, the build and the probe. The per-DPU R and S sizes equal
+    the oracle's pipeline restatement, and the pairs equal its join and the
+    independent join."""
+    R, S, expect = oracle.generate(1 << 15, 1 << 17, 1.0, seed=0x5EED0001)
+    D = 64
+    to_r = [dpu_ref.packet_scatter(blk, 1, 1, b) for b, blk in enumerate(_split_blocks(R, D))]
+    to_s = [dpu_ref.packet_scatter(blk, 1, 1, b) for b, blk in enumerate(_split_blocks(S, D))]
+    r_in = [np.concatenate([to_r[b][d] for b in range(D)]) for d in range(D)]
+    s_in = [np.concatenate([to_s[b][d] for b in range(D)]) for d in range(D)]
+    want_r, want_s = oracle.refpipe_dpu_sizes(R, S, ranks=1)
+    assert [x.shape[0] for x in r_in] == list(want_r)
+    assert [x.shape[0] for x in s_in] == list(want_s)
+    pairs = []
+    for d in range(D):
+        rg, ro, L = dpu_ref.local_partition(r_in[d])
+        sg, so, _ = dpu_ref.local_partition(s_in[d], partitions=L)
+        pairs.append(dpu_ref.hash_join(rg, ro, sg, so))
+    got = np.concatenate(pairs)
+    assert got.shape[0] == S.shape[0] and oracle.checksum(got) == expect
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.refpipe_join(R, S, ranks=1)))
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S)))
+
+
+def test_reference_kernels_over_two_rank_sets(oracle):
+    """The same chain on two ranks in two rank sets (-r 2 -R 2): R is
+    partitioned over one rank's 64 DPUs and every rank set receives a copy
+    (the host's rank-group copy, src/queryHostFunc.cc:654-776); S is split
+    over both rank sets by each tuple's index in its block. The per-DPU sizes
+    and the pairs equal the oracle's pipeline restatement."""
+    R, S, expect = oracle.generate(1 << 14, 1 << 16, 1.5, seed=0x5EED0002)
+    ranks, rank_sets = 2, 2
+    D, PR = 64 * ranks, 64 * ranks // rank_sets
+    r_in = [[] for _ in range(D)]
+    s_in = [[] for _ in range(D)]
+    for b, blk in enumerate(_split_blocks(R, D)):
+        groups = dpu_ref.packet_scatter(blk, ranks // rank_sets, 1, b % 64)
+        for g in range(rank_sets):
+            for p in range(PR):
+                r_in[g * PR + p].append(groups[p])
+    for b, blk in enumerate(_split_blocks(S, D)):
+        for d, grp in enumerate(dpu_ref.packet_scatter(blk, ranks, rank_sets, b % 64)):
+            s_in[d].append(grp)
+    r_in = [np.concatenate(x) for x in r_in]
+    s_in = [np.concatenate(x) for x in s_in]
+    want_r, want_s = oracle.refpipe_dpu_sizes(R, S, ranks=ranks, rank_sets=rank_sets)
+    assert [x.shape[0] for x in r_in] == list(want_r)
+    assert [x.shape[0] for x in s_in] == list(want_s)
+    pairs = []
+    for d in range(D):
+        rg, ro, L = dpu_ref.local_partition(r_in[d])
+        sg, so, _ = dpu_ref.local_partition(s_in[d], partitions=L)
+        pairs.append(dpu_ref.hash_join(rg, ro, sg, so))
+    got = np.concatenate(pairs)
+    assert got.shape[0] == S.shape[0] and oracle.checksum(got) == expect
+    want = oracle.refpipe_join(R, S, ranks=ranks, rank_sets=rank_sets)
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(want))
