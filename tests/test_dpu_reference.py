@@ -571,3 +571,52 @@ def test_reference_kernels_over_two_rank_sets(oracle):
     assert got.shape[0] == S.shape[0] and oracle.checksum(got) == expect
     want = oracle.refpipe_join(R, S, ranks=ranks, rank_sets=rank_sets)
     assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(want))
+
+
+def test_reference_nested_loop_over_one_rank(oracle):
+    """The nested-loop form of the join on one rank of 64 DPUs by the
+    reference's kernels: count and packet scatter per source DPU, then
+    nested_loop_join.c per destination DPU, which rewrites every S tuple in
+    place. The rows (matched ones (R payload, S payload), the others unchanged)
+    equal the oracle's nested-loop pipeline. R payloads lie above every key, so
+    the kernel's second rewrite of a payload that equals a key cannot occur."""
+    rng = np.random.default_rng(0x5EED0003)
+    n_r, n_s = 1 << 13, 1 << 15
+    keys = rng.permutation(np.arange(1, 4 * n_r))[:n_r]
+    R = np.stack([keys, rng.integers(1 << 31, 2**32, n_r)], 1).astype(np.uint32)
+    hit = rng.random(n_s) < 0.75
+    S = np.stack([np.where(hit, keys[rng.integers(0, n_r, n_s)], rng.integers(4 * n_r, 1 << 30, n_s)),
+                  np.arange(n_s)], 1).astype(np.uint32)
+    D = 64
+    to_r = [dpu_ref.packet_scatter(blk, 1, 1, b) for b, blk in enumerate(_split_blocks(R, D))]
+    to_s = [dpu_ref.packet_scatter(blk, 1, 1, b) for b, blk in enumerate(_split_blocks(S, D))]
+    rows = []
+    for d in range(D):
+        r_d = np.concatenate([to_r[b][d] for b in range(D)])
+        s_d = np.concatenate([to_s[b][d] for b in range(D)])
+        rows.append(dpu_ref.nested_loop(r_d, s_d))
+    got = np.concatenate(rows)
+    want = oracle.refpipe_join(R, S, ranks=1, alg=oracle.ALG_NL)
+    assert got.shape == want.shape == (n_s, 2)
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(want))
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(oracle.simple_join(R, S, keep_unmatched=True)))
+
+
+def test_reference_nphj_over_one_rank(oracle):
+    """The non-partitioned form on one rank of 64 DPUs by the reference's
+    kernels: count and packet scatter per source DPU, then the
+    non-partitioned build and probe per destination DPU with the table the
+    host sizes. The pairs equal the oracle's pipeline for that algorithm."""
+    R, S, expect = oracle.generate(1 << 15, 1 << 17, 1.5, seed=0x5EED0004)
+    D = 64
+    to_r = [dpu_ref.packet_scatter(blk, 1, 1, b) for b, blk in enumerate(_split_blocks(R, D))]
+    to_s = [dpu_ref.packet_scatter(blk, 1, 1, b) for b, blk in enumerate(_split_blocks(S, D))]
+    pairs = []
+    for d in range(D):
+        r_d = np.concatenate([to_r[b][d] for b in range(D)])
+        s_d = np.concatenate([to_s[b][d] for b in range(D)])
+        pairs.append(dpu_ref.nphj(r_d, s_d)[0])
+    got = np.concatenate(pairs)
+    assert got.shape[0] == S.shape[0] and oracle.checksum(got) == expect
+    want = oracle.refpipe_join(R, S, ranks=1, alg=oracle.ALG_NPHJ)
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(want))
