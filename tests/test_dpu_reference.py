@@ -620,3 +620,34 @@ def test_reference_nphj_over_one_rank(oracle):
     assert got.shape[0] == S.shape[0] and oracle.checksum(got) == expect
     want = oracle.refpipe_join(R, S, ranks=1, alg=oracle.ALG_NPHJ)
     assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(want))
+
+
+def test_reference_sort_merge_over_one_rank(oracle):
+    """The sort-merge form on one rank of 64 DPUs by the reference's kernels:
+    count and packet scatter per source DPU, then per destination DPU the
+    range partitioning and the sort-probe with the arguments the reference's
+    host passes (elem_range = |R| keys 1..|R|, hist_interval = 64 DPUs * 64,
+    src/queryDpuFunc.cc:538-555, src/dpuArgumentJoin.cc:517, 566-567). |R| = 12 *
+    4096 gives 13 buckets, of which the sort-probe joins the first 12 (the
+    last, key 49152 alone, it leaves unprobed). The probed rows equal the
+    oracle's sort-merge pipeline's rows for those S tuples."""
+    rng = np.random.default_rng(0x5EED0005)
+    n_r = n_s = 12 * 4096
+    R = np.stack([rng.permutation(np.arange(1, n_r + 1)), rng.integers(0, 2**32, n_r)], 1).astype(np.uint32)
+    S = np.stack([rng.integers(1, n_r + 1, n_s), np.arange(n_s)], 1).astype(np.uint32)
+    D = 64
+    to_r = [dpu_ref.packet_scatter(blk, 1, 1, b) for b, blk in enumerate(_split_blocks(R, D))]
+    to_s = [dpu_ref.packet_scatter(blk, 1, 1, b) for b, blk in enumerate(_split_blocks(S, D))]
+    rows, unprobed = [], []
+    for d in range(D):
+        r_d = np.concatenate([to_r[b][d] for b in range(D)])
+        s_d = np.concatenate([to_s[b][d] for b in range(D)])
+        got, skipped = dpu_ref.sort_merge(r_d, s_d, n_r, 64 * 64)
+        rows.append(got)
+        unprobed.append(skipped)
+    rows, unprobed = np.concatenate(rows), np.concatenate(unprobed)
+    assert np.array_equal(np.sort(unprobed[:, 1]), np.sort(S[S[:, 0] == n_r, 1]))
+    want = oracle.refpipe_join(R, S, ranks=1, alg=oracle.ALG_SMJ)
+    probed = ~np.isin(want[:, 1], unprobed[:, 1])
+    assert rows.shape[0] == int(probed.sum()) == n_s - unprobed.shape[0]
+    assert np.array_equal(oracle.sort_pairs(rows), oracle.sort_pairs(want[probed]))
