@@ -66,6 +66,8 @@ def lib():
         L.orc_dpu_phj.argtypes = [vp, i64, vp, i64, vp]
         L.orc_glb_partition_dest.restype = None
         L.orc_glb_partition_dest.argtypes = [vp, i64, i32, i32, i32, i32, vp]
+        L.orc_r_dests.restype = i32
+        L.orc_r_dests.argtypes = [ctypes.c_uint32, i32, i32, i32, vp]
         L.orc_chipwise_partition_dest.restype = i32
         L.orc_chipwise_partition_dest.argtypes = [vp, i64, i32, i32, i32, vp]
         L.orc_chipwise_partition_count.restype = i32
@@ -179,6 +181,16 @@ def chipwise_partition_count(tuples, ranks, rank_sets, bank_set):
     if rc:
         raise RuntimeError(ERRORS.get(rc, rc))
     return hist
+
+
+def r_dests(key, ranks, rank_sets=1, bank_set=1):
+    """The DPUs the reference pipeline sends an R tuple of `key` to (its
+    replicas over rank sets and bank-set members included)."""
+    out = np.zeros(64 * ranks, dtype=np.int32)
+    m = lib().orc_r_dests(int(key), ranks, rank_sets, bank_set, _ptr(out))
+    if m < 0:
+        raise RuntimeError(ERRORS.get(m, m))
+    return out[:m]
 
 
 def chipwise_partition_dest(tuples, ranks, rank_sets, bank_set):

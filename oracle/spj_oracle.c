@@ -378,6 +378,24 @@ int orc_chipwise_partition_count(const orc_tuple *t, int64_t n, int ranks, int r
     return ORC_OK;
 }
 
+/* The DPUs that receive an R tuple of `key` (replicas included; at most
+ * 64 * ranks): FOR_R_DESTS. Returns their number or ORC_E_ARG. */
+int orc_r_dests(uint32_t key, int ranks, int rank_sets, int bank_set, int32_t *dests)
+{
+    refpipe_t rp;
+    int e = bank_set == 1 ? ORC_OK : chipwise_setup(&rp, ranks, rank_sets, bank_set);
+    if (e) return e;
+    if (bank_set == 1) {
+        if (ranks <= 0 || rank_sets <= 0 || ranks % rank_sets) return ORC_E_ARG;
+        memset(&rp, 0, sizeof(rp));
+        rp.ranks = ranks; rp.G = rank_sets; rp.rps = ranks / rank_sets; rp.B = 1;
+    }
+    orc_tuple t = {key, 0};
+    int m = 0;
+    FOR_R_DESTS(&rp, t, dests[m++] = dest);
+    return m;
+}
+
 /* Each tuple's destination under the chip-wise split (-1 for padding): where
  * glb_chipwise_partition_packet.c:468-472 scatters it. */
 int orc_chipwise_partition_dest(const orc_tuple *t, int64_t n, int ranks, int rank_sets, int bank_set,

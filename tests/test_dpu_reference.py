@@ -651,3 +651,41 @@ def test_reference_sort_merge_over_one_rank(oracle):
     probed = ~np.isin(want[:, 1], unprobed[:, 1])
     assert rows.shape[0] == int(probed.sum()) == n_s - unprobed.shape[0]
     assert np.array_equal(oracle.sort_pairs(rows), oracle.sort_pairs(want[probed]))
+
+
+@pytest.mark.parametrize("ranks,rank_sets,bank_set", [(1, 1, 8), (2, 2, 16)])
+def test_reference_kernels_with_bank_sets(oracle, ranks, rank_sets, bank_set):
+    """The join with bank sets (-B) by the reference's kernels, except the
+    host's chip-wise broadcast of R. R: bank-group count and align per source
+    DPU; each bank group's tuples go to the DPUs the oracle's pipeline sends
+    them to (the broadcast itself runs in the host's transfer code). S: the
+    chip-wise count and packet scatter. Then local partitioning, build and
+    probe per DPU. Every S tuple finds its R tuple on the DPU the reference's
+    own S routing chose, so the per-DPU sizes and the pairs equal the oracle's
+    pipeline, and the count and checksum its generator's answer."""
+    R, S, expect = oracle.generate(1 << 14, 1 << 16, 1.0, seed=0x5EED0006 + bank_set)
+    D, rps = 64 * ranks, ranks // rank_sets
+    r_in = [[] for _ in range(D)]
+    s_in = [[] for _ in range(D)]
+    for blk in _split_blocks(R, D):
+        for grp in dpu_ref.bg_broadcast_align(blk, rps, bank_set):
+            if grp.shape[0]:
+                for d in oracle.r_dests(grp[0, 0], ranks, rank_sets, bank_set):
+                    r_in[d].append(grp)
+    for b, blk in enumerate(_split_blocks(S, D)):
+        for d, grp in enumerate(dpu_ref.packet_scatter(blk, ranks, rank_sets, b % 64, bank_set=bank_set)):
+            s_in[d].append(grp)
+    r_in = [np.concatenate(x) if x else np.zeros((0, 2), np.uint32) for x in r_in]
+    s_in = [np.concatenate(x) for x in s_in]
+    want_r, want_s = oracle.refpipe_dpu_sizes(R, S, ranks=ranks, rank_sets=rank_sets, bank_set=bank_set)
+    assert [x.shape[0] for x in r_in] == list(want_r)
+    assert [x.shape[0] for x in s_in] == list(want_s)
+    pairs = []
+    for d in range(D):
+        rg, ro, L = dpu_ref.local_partition(r_in[d])
+        sg, so, _ = dpu_ref.local_partition(s_in[d], partitions=L)
+        pairs.append(dpu_ref.hash_join(rg, ro, sg, so))
+    got = np.concatenate(pairs)
+    assert got.shape[0] == S.shape[0] and oracle.checksum(got) == expect
+    want = oracle.refpipe_join(R, S, ranks=ranks, rank_sets=rank_sets, bank_set=bank_set)
+    assert np.array_equal(oracle.sort_pairs(got), oracle.sort_pairs(want))
