@@ -188,6 +188,28 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
 /* Output capacity (pairs) that `out` must provide for this plan. */
 int64_t spj_plan_output_capacity(const spj_plan_t *plan);
 
+/* The planner's choice for one join: what spj_plan_create (batch_tuples = 0)
+ * or spj_batch_create (batch_tuples = the batch's total |R| + |S|, its size
+ * class's tuning applied) would run, computed from the device limits given
+ * here instead of queried. It needs no device, so a caller can inspect a plan
+ * anywhere (the EXPLAIN of this path). num_sms: 148 on B200;
+ * max_smem_per_block: the opt-in shared memory per block, 232448 bytes on
+ * B200. */
+typedef struct {
+    int32_t join_alg;           /* spj_join_alg the join runs (NPHJ replaces a hash join alone with |R| <= 2^22) */
+    int32_t radix_bits;         /* partitions = 2^radix_bits (0: the non-partitioned join) */
+    int32_t scatter_passes;     /* passes of the partitioning scatter: 1 or 2 (0: non-partitioned) */
+    int32_t table_slots;        /* shared-memory table slots of a work unit (partitioned joins) */
+    int64_t global_table_slots; /* the non-partitioned join's table in HBM (else 0) */
+    int32_t heavy_sample;       /* S keys sampled for heavy keys joined on the fly (0: none) */
+    int32_t unit_tuples;        /* S tuples per work unit */
+    int32_t out_chunk;          /* output pairs a warp reserves at a time */
+    int32_t chunk_tuples;       /* tuples per first-pass chunk */
+} spj_plan_shape_t;
+
+int spj_plan_describe(int64_t n_r, int64_t n_s, const spj_design_t *design, int num_sms, int max_smem_per_block,
+                      int64_t batch_tuples, spj_plan_shape_t *out);
+
 /* r, s, out: device pointers. n_out: device int64 that receives the pair count.
  * stream: a cudaStream_t (NULL = legacy default stream). */
 int spj_plan_execute(spj_plan_t *plan, const spj_kv_pair_t *r, const spj_kv_pair_t *s, spj_kv_pair_t *out,

@@ -632,6 +632,33 @@ int spj_plan_create(int64_t n_r, int64_t n_s, const spj_design_t *design, spj_pl
     return create_plan(1, &n_r, &n_s, design, out);
 }
 
+// The same plan_shape call as create_plan, with the device limits as arguments.
+int spj_plan_describe(int64_t n_r, int64_t n_s, const spj_design_t *design, int num_sms, int max_smem_per_block,
+                      int64_t batch_tuples, spj_plan_shape_t *out) {
+    if (!out) return set_error(SPJ_E_ARG, "out is NULL");
+    int rc = validate_design(design);
+    if (rc) return rc;
+    if (n_r < 0 || n_s < 0 || n_r >= kMaxTuples || n_s >= kMaxTuples)
+        return set_error(SPJ_E_ARG, "relation sizes must be in [0, 2^32 - 2^24 - 1)");
+    if (num_sms < 1 || max_smem_per_block < 48 * 1024 || batch_tuples < 0)
+        return set_error(SPJ_E_ARG, "num_sms >= 1, max_smem_per_block >= 48 KiB, batch_tuples >= 0");
+    const bool alone = batch_tuples == 0;
+    spj_tuning_t tn;
+    const JoinShape sh = plan_shape(n_r, n_s, *design, num_sms, max_table_slots_for(max_smem_per_block), alone,
+                                    batch_tuples, alone ? nullptr : find_tuning(n_r, n_s, &tn));
+    const bool nphj = sh.alg == SPJ_ALG_NPHJ;
+    out->join_alg = sh.alg;
+    out->radix_bits = nphj ? 0 : sh.bits;
+    out->scatter_passes = nphj ? 0 : (sh.fine_bits ? 2 : 1);
+    out->table_slots = nphj ? 0 : sh.table_slots;
+    out->global_table_slots = nphj ? (int64_t)sh.gtable_slots : 0;
+    out->heavy_sample = (int32_t)sh.heavy_sample;
+    out->unit_tuples = (int32_t)sh.unit_tuples;
+    out->out_chunk = (int32_t)sh.out_chunk;
+    out->chunk_tuples = (int32_t)sh.chunk[0];
+    return SPJ_OK;
+}
+
 int64_t spj_plan_output_capacity(const spj_plan_t *plan) {
     return plan ? (int64_t)plan->joins[0].dev.out_cap : 0;
 }

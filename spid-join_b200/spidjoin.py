@@ -36,7 +36,7 @@ EXPORTS = (
     "spj_server_reset_stats", "spj_server_destroy", "spj_server_hold", "spj_exchange_split",
     "spj_tuning_set", "spj_tuning_get", "spj_exchange_count", "spj_exchange_scatter", "spj_select",
     "spj_dist_unique_id", "spj_dist_create", "spj_dist_set_heavy", "spj_dist_join", "spj_dist_heavy_keys",
-    "spj_dist_destroy", "spj_dist_abort",
+    "spj_dist_destroy", "spj_dist_abort", "spj_plan_describe",
 )
 
 
@@ -106,6 +106,16 @@ class ServerStats(ctypes.Structure):
         return {f[0]: getattr(self, f[0]) for f in self._fields_ if f[0] != "reserved0"}
 
 
+class PlanShape(ctypes.Structure):
+    _fields_ = [("join_alg", ctypes.c_int32), ("radix_bits", ctypes.c_int32), ("scatter_passes", ctypes.c_int32),
+                ("table_slots", ctypes.c_int32), ("global_table_slots", ctypes.c_int64),
+                ("heavy_sample", ctypes.c_int32), ("unit_tuples", ctypes.c_int32), ("out_chunk", ctypes.c_int32),
+                ("chunk_tuples", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
 class KernelTimes(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
                 ("hist_ms", "scan_ms", "scatter_ms", "units_ms", "join_ms", "fixup_ms", "total_ms")]
@@ -138,6 +148,7 @@ def lib():
         L.spj_destroy.argtypes = [vp]
         L.spj_destroy.restype = None
         L.spj_plan_create.argtypes = [i64, i64, ctypes.POINTER(Design), ctypes.POINTER(vp)]
+        L.spj_plan_describe.argtypes = [i64, i64, ctypes.POINTER(Design), i32, i32, i64, ctypes.POINTER(PlanShape)]
         L.spj_plan_output_capacity.argtypes = [vp]
         L.spj_plan_output_capacity.restype = i64
         L.spj_plan_execute.argtypes = [vp, vp, vp, vp, vp, vp]
@@ -203,6 +214,22 @@ def make_design(**kw):
             raise KeyError(k)
         setattr(d, k, v if isinstance(v, Predicate) else int(v))
     return d
+
+
+B200_SMS, B200_SMEM_PER_BLOCK = 148, 232448
+
+
+def describe(n_r, n_s, design=None, num_sms=B200_SMS, max_smem_per_block=B200_SMEM_PER_BLOCK, batch_tuples=0):
+    """The planner's choice for one join (spj_plan_describe): a dict with the
+    local-join algorithm ("phj", "nphj", "smj", "nl"), fan-out, passes, table
+    sizes, heavy-key sample, unit, output chunk and chunk size. Needs no GPU."""
+    d = design if design is not None else make_design()
+    sh = PlanShape()
+    check(lib().spj_plan_describe(n_r, n_s, ctypes.byref(d), num_sms, max_smem_per_block, batch_tuples,
+                                  ctypes.byref(sh)))
+    out = sh.as_dict()
+    out["join_alg"] = {v: k for k, v in ALG.items()}[out["join_alg"]]
+    return out
 
 
 def _host_tuples(a):
