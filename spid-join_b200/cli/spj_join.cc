@@ -3,9 +3,10 @@
 //   -s input_size (|R|)  -r rank_num  -z zipf_factor (Zipf exponent x 100)
 //   -t rs_ratio (|S|/|R|)  -R rank_set  -B bank_set
 // plus -a algorithm (phj|nphj|smj|nl), -n repetitions, -S seed, -o (result
-// buffers owned by the caller) and -P (the reference's padded per-rank layout of
-// 64 DPU blocks; implies -o). -h, -p and -f take an argument and are ignored, as
-// in the reference.
+// buffers owned by the caller), -P (the reference's padded per-rank layout of
+// 64 DPU blocks; implies -o) and -E (print the plan the join would run, from
+// spj_plan_describe with the B200's limits, and exit without touching a GPU).
+// -h, -p and -f take an argument and are ignored, as in the reference.
 //
 // With -z 0 the relations are the reference driver's (test/join/main.cc:33-43):
 // R[i] = (i+1, i+3) and S[i] = (i/ratio + 1, i/ratio + 3). With -z > 0 the
@@ -54,14 +55,15 @@ int main(int argc, char **argv) {
     int reps = 1;
     bool owned = false;  // -o: result buffers owned by the caller, as the reference hands them out
     bool padded = false; // -P: the reference's transfer layout, 64 zero-padded DPU blocks per rank
+    bool explain = false; // -E: the plan only
     uint64_t seed = 0x5EED5EEDull;
     if (argc < 2) {
         fprintf(stderr, "usage: %s -s |R| [-r ranks] [-z zipf*100] [-t |S|/|R|] [-R rank_set] [-B bank_set] "
-                        "[-a phj|nphj|smj|nl] [-n reps] [-S seed] [-o] [-P]\n", argv[0]);
+                        "[-a phj|nphj|smj|nl] [-n reps] [-S seed] [-o] [-P] [-E]\n", argv[0]);
         return 0;
     }
     int opt;
-    while ((opt = getopt(argc, argv, "s:r:z:t:R:B:h:p:f:a:n:S:oP")) != -1) {
+    while ((opt = getopt(argc, argv, "s:r:z:t:R:B:h:p:f:a:n:S:oPE")) != -1) {
         switch (opt) {
             case 's': d.input_size = atoll(optarg); break;
             case 'r': d.rank_num = atoi(optarg); break;
@@ -74,6 +76,7 @@ int main(int argc, char **argv) {
             case 'S': seed = strtoull(optarg, nullptr, 0); break;
             case 'o': owned = true; break;
             case 'P': padded = owned = true; break;
+            case 'E': explain = true; break;
             default: break;
         }
     }
@@ -89,6 +92,20 @@ int main(int argc, char **argv) {
     if (n_r <= 0 || d.rs_ratio <= 0 || d.rank_num <= 0 || d.rank_set <= 0 || d.rank_num % d.rank_set) {
         fprintf(stderr, "bad sizes or rank layout\n");
         return 2;
+    }
+    if (explain) {
+        const spj_design_t c = d.to_c();
+        spj_plan_shape_t sh;
+        if (spj_plan_describe(n_r, n_s, &c, 148, 232448, 0, &sh) != SPJ_OK) {
+            fprintf(stderr, "%s\n", spj_last_error());
+            return 2;
+        }
+        static const char *const names[] = {"phj", "nphj", "smj", "nl"};
+        printf("plan: |R|=%lld |S|=%lld alg=%s radix_bits=%d passes=%d table_slots=%d global_table_slots=%lld "
+               "heavy_sample=%d unit_tuples=%d out_chunk=%d chunk_tuples=%d\n",
+               (long long)n_r, (long long)n_s, names[sh.join_alg], sh.radix_bits, sh.scatter_passes, sh.table_slots,
+               (long long)sh.global_table_slots, sh.heavy_sample, sh.unit_tuples, sh.out_chunk, sh.chunk_tuples);
+        return 0;
     }
     std::vector<kv_pair_t> R(n_r), S(n_s);
     uint64_t expect = 0;

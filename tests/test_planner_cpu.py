@@ -123,3 +123,32 @@ def test_describe_rejects_bad_arguments(spj):
         spj.describe(10, 10, max_smem_per_block=1024)
     with pytest.raises(spj.SpjError):
         spj.describe(10, 10, _d(spj, rank_num=3, rank_set=2))
+
+
+def _cli():
+    import os
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "spid-join_b200", "spj_join")
+    if not os.path.exists(path):
+        pytest.skip("spj_join is not built")
+    return path
+
+
+@pytest.mark.parametrize("args,want", [
+    (["-s", "1048576", "-t", "2"], "alg=nphj radix_bits=0 passes=0"),                  # the reference driver's case
+    (["-s", "134217728", "-t", "4", "-r", "4", "-R", "4", "-z", "100"],
+     "alg=phj radix_bits=15 passes=2 table_slots=12288"),                            # config 2
+    (["-s", "67108864", "-t", "8", "-a", "smj"], "alg=smj radix_bits=15 passes=2 table_slots=8192"),
+])
+def test_cli_explains_without_a_gpu(spj, args, want):
+    """spj_join -E prints the plan the reference driver's options give (the
+    same planner as the library) and exits 0 without touching a GPU."""
+    import subprocess
+    out = subprocess.run([_cli(), *args, "-E"], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, out.stderr
+    assert want in out.stdout
+
+
+def test_cli_explain_rejects_a_bad_design():
+    import subprocess
+    out = subprocess.run([_cli(), "-s", "100", "-t", "2", "-B", "3", "-E"], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 2 and "bank_set" in out.stderr
