@@ -788,3 +788,25 @@ def test_local_partition_kernel_rejects_high_keys():
         dpu_ref.local_partition(T)
     got, starts, L = dpu_ref.local_partition(T[[0, 2]])
     assert L == 1 and starts.tolist() == [0, 2]
+
+
+@hyp.settings(max_examples=15, deadline=None)
+@hyp.given(seed=st.integers(0, 2**32 - 1), n=st.integers(0, 5000), log_ranks=st.integers(0, 3),
+           log_g=st.integers(0, 3), dpu_id=st.integers(0, 63), log_packet=st.integers(3, 7),
+           bank_set=st.sampled_from([1, 8, 16, 32, 64]), zero_every=st.sampled_from([0, 2, 97]))
+def test_property_packet_scatters(oracle, seed, n, log_ranks, log_g, dpu_id, log_packet, bank_set, zero_every):
+    """The plain and chip-wise packet scatters against the oracle's
+    destinations for random blocks, rank counts, rank sets, source DPUs,
+    packet sizes and bank sets."""
+    ranks = 1 << log_ranks
+    G = 1 << min(log_g, log_ranks)
+    if bank_set > 1 and ranks // G * 64 < bank_set:
+        return
+    T, _ = _random_relations(seed, n, 0, 2**31 - 1, zero_every)
+    groups = dpu_ref.packet_scatter(T, ranks, G, dpu_id, 1 << log_packet, bank_set=bank_set)
+    if bank_set > 1:
+        dest = oracle.chipwise_partition_dest(T, ranks, G, bank_set)
+    else:
+        dest = oracle.partition_dest(T, 64 * ranks, 0 if G == 1 else 1, G, ranks // G)
+    for d, g in enumerate(groups):
+        assert np.array_equal(oracle.sort_pairs(g), oracle.sort_pairs(T[dest == d]))
