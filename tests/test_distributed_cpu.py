@@ -135,3 +135,67 @@ def test_exchange_layout_tiles_every_receive_buffer():
                 assert a == pos
                 pos = b
             assert pos == layouts[d][0] <= need == layouts[0][2]
+
+
+def _rank_fail_main(rank, world, port, out_q, mode="raise"):
+    """Rank 1 fails on the host before its first exchange: its split raises and
+    it leaves (mode "raise"), or it stalls there without leaving (mode
+    "stall"). Rank 0 runs normally and must end with an error, not wait for
+    good: at once when its peer's connection drops, within the process group's
+    5 s timeout when the peer stalls."""
+    import datetime
+    import time
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(ROOT, "spid-join_b200"))
+    import spidjoin
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    R, S = _dataset(11, 2000, 8000)
+
+    def split(T, heavy, mode):
+        if rank == 1:
+            if mode == "stall":
+                time.sleep(20)  # never reaches the exchange while rank 0 waits
+            raise RuntimeError("injected failure on rank 1")
+        a = T.numpy().view(np.uint32).reshape(-1, 2)
+        a = a[a[:, 0] != 0]
+        d = _dest(a[:, 0], world)
+        order = np.argsort(d, kind="stable")
+        return torch.from_numpy(a[order].view(np.int32).copy()), torch.from_numpy(np.bincount(d, minlength=world))
+
+    dj = spidjoin.DistributedJoin(split=split, join=lambda r, s: (r, torch.tensor([0])), heavy=False)
+    t0 = time.monotonic()
+    try:
+        dj.run(torch.from_numpy(R.view(np.int32).copy()), torch.from_numpy(S.view(np.int32).copy()))
+        out_q.put((rank, "finished", "", time.monotonic() - t0))
+    except Exception as e:  # noqa: BLE001 -- the outcome is what the test checks
+        out_q.put((rank, type(e).__name__, str(e)[:200], time.monotonic() - t0))
+    # the group is broken: leave without another collective, once the result is sent
+    out_q.close()
+    out_q.join_thread()
+    os._exit(0)
+
+
+@pytest.mark.parametrize("mode", ["raise", "stall"])
+def test_a_failing_rank_ends_its_peers_with_an_error(mode):
+    """Failure detection on the host: when one rank raises before its exchange
+    and leaves, or stalls there, the other rank's pending collective ends with
+    an error (within the process group's timeout) instead of waiting for
+    good."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_fail_main, args=(r, 2, port, q, mode)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = {r: (kind, msg, secs) for r, kind, msg, secs in (q.get(timeout=120) for _ in range(2))}
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0, "a rank did not exit"
+    assert res[1][0] == "RuntimeError" and "injected failure" in res[1][1]
+    assert res[0][0] != "finished", "rank 0 finished a join its peer never joined"
+    assert res[0][2] < (2 if mode == "raise" else 15)
