@@ -152,3 +152,38 @@ def test_cli_explain_rejects_a_bad_design():
     import subprocess
     out = subprocess.run([_cli(), "-s", "100", "-t", "2", "-B", "3", "-E"], capture_output=True, text=True, timeout=60)
     assert out.returncode == 2 and "bank_set" in out.stderr
+
+
+def test_committed_tuning_table_shapes_batch_members(spj):
+    """The tuning table the autotuner wrote for the B200 (tuning_b200.json, which
+    bench.py installs for batches) loads, and each entry shapes the plan of a
+    batch member of its size class: its fan-out offset against the untuned
+    planner, its table, its algorithm. A join alone keeps the planner's own
+    shape."""
+    import os
+    path = os.path.join(os.path.dirname(spj.__file__), "tuning_b200.json")
+    saved = spj.get_tuning()
+    try:
+        spj.set_tuning([])
+        table = spj.load_tuning(path)
+        assert table["entries"] and spj.get_tuning()
+        for e in table["entries"]:
+            n_r = 1 << e["log2_r"]
+            n_s = n_r << e["log2_ratio"]
+            tuned = spj.describe(n_r, n_s, batch_tuples=1 << 26)
+            alone_tuned = spj.describe(n_r, n_s)
+            spj.set_tuning([])
+            plain = spj.describe(n_r, n_s, batch_tuples=1 << 26)
+            assert spj.describe(n_r, n_s) == alone_tuned  # a join alone: untouched by the table
+            spj.load_tuning(path)
+            if e["join_alg"] > 0:
+                assert spj.ALG[tuned["join_alg"]] == e["join_alg"] - 1
+            if tuned["join_alg"] != "nphj":
+                want_bits = min(max(plain["radix_bits"] + e["radix_bits_delta"], 1), 15)
+                assert tuned["radix_bits"] == want_bits
+                if e["table_slots"] > 0:
+                    assert tuned["table_slots"] == min(e["table_slots"], 12288) & ~1
+            if e["unit_tuples"] > 0:
+                assert tuned["unit_tuples"] == e["unit_tuples"]
+    finally:
+        spj.set_tuning(saved)
