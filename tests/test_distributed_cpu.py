@@ -137,9 +137,9 @@ def test_exchange_layout_tiles_every_receive_buffer():
             assert pos == layouts[d][0] <= need == layouts[0][2]
 
 
-def _rank_fail_main(rank, world, port, out_q, mode="raise"):
+def _rank_fail_main(rank, world, port, out_q, failure="raise"):
     """Rank 1 fails on the host before its first exchange: its split raises and
-    it leaves (mode "raise"), or it stalls there without leaving (mode
+    it leaves (failure "raise"), or it stalls there without leaving (failure
     "stall"). Rank 0 runs normally and must end with an error, not wait for
     good: at once when its peer's connection drops, within the process group's
     5 s timeout when the peer stalls."""
@@ -157,8 +157,8 @@ def _rank_fail_main(rank, world, port, out_q, mode="raise"):
 
     def split(T, heavy, mode):
         if rank == 1:
-            if mode == "stall":
-                time.sleep(20)  # never reaches the exchange while rank 0 waits
+            if failure == "stall":
+                time.sleep(12)  # does not reach the exchange before rank 0's timeout
             raise RuntimeError("injected failure on rank 1")
         a = T.numpy().view(np.uint32).reshape(-1, 2)
         a = a[a[:, 0] != 0]
@@ -179,8 +179,8 @@ def _rank_fail_main(rank, world, port, out_q, mode="raise"):
     os._exit(0)
 
 
-@pytest.mark.parametrize("mode", ["raise", "stall"])
-def test_a_failing_rank_ends_its_peers_with_an_error(mode):
+@pytest.mark.parametrize("failure", ["raise", "stall"])
+def test_a_failing_rank_ends_its_peers_with_an_error(failure):
     """Failure detection on the host: when one rank raises before its exchange
     and leaves, or stalls there, the other rank's pending collective ends with
     an error (within the process group's timeout) instead of waiting for
@@ -189,7 +189,7 @@ def test_a_failing_rank_ends_its_peers_with_an_error(mode):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_fail_main, args=(r, 2, port, q, mode)) for r in range(2)]
+    procs = [ctx.Process(target=_rank_fail_main, args=(r, 2, port, q, failure)) for r in range(2)]
     for p in procs:
         p.start()
     res = {r: (kind, msg, secs) for r, kind, msg, secs in (q.get(timeout=120) for _ in range(2))}
@@ -198,4 +198,6 @@ def test_a_failing_rank_ends_its_peers_with_an_error(mode):
         assert p.exitcode == 0, "a rank did not exit"
     assert res[1][0] == "RuntimeError" and "injected failure" in res[1][1]
     assert res[0][0] != "finished", "rank 0 finished a join its peer never joined"
-    assert res[0][2] < (2 if mode == "raise" else 15)
+    assert res[0][2] < (2 if failure == "raise" else 11)
+    if failure == "stall":
+        assert res[0][2] >= 4, "rank 0 ended before its process group's timeout"
