@@ -147,3 +147,46 @@ def test_dpu_block_layout(spj, n):
     assert np.array_equal(np.concatenate([blocks[b, :filled[b]] for b in range(64)]), pairs)  # order kept
     for b in range(64):
         assert not blocks[b, filled[b]:].any()  # padding is (0, 0)
+
+
+C_CALLER = r"""
+#include <stdio.h>
+#include "spidjoin.h"
+
+int main(void) {
+    spj_design_t d;
+    spj_design_default(&d);
+    d.rank_num = 4;
+    d.rank_set = 4;
+    spj_plan_shape_t sh;
+    int rc = spj_plan_describe((int64_t)1 << 27, (int64_t)1 << 29, &d, 148, 232448, 0, &sh);
+    printf("describe %d %d %d %d %d\n", rc, sh.join_alg, sh.radix_bits, sh.scatter_passes, sh.table_slots);
+    spj_plan_t *plan = NULL;
+    rc = spj_plan_create(1000, 2000, &d, &plan);
+    printf("create %d %s\n", rc, spj_last_error());
+    return 0;
+}
+"""
+
+
+def test_header_compiles_as_c_and_links(tmp_path):
+    """The boundary is a C ABI: a strict C11 program (-pedantic -Werror)
+    includes include/spidjoin.h, links libspidjoin.so and calls it. The
+    planner's description works without a device; a join entry point returns
+    SPJ_E_NODEVICE (with no GPU) instead of running anywhere else."""
+    import shutil
+    import subprocess
+    import torch
+    cc = shutil.which("gcc") or shutil.which("cc")
+    lib_dir = os.path.join(ROOT, "spid-join_b200")
+    if not cc or not os.path.exists(os.path.join(lib_dir, "libspidjoin.so")):
+        pytest.skip("no C compiler or library")
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    subprocess.run([cc, "-std=c11", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-L", lib_dir, "-lspidjoin", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60, check=True).stdout.split("\n")
+    assert out[0] == "describe 0 0 15 2 12288"
+    if not torch.cuda.is_available():
+        assert out[1].startswith("create -7 no CUDA device")
