@@ -190,3 +190,28 @@ def test_header_compiles_as_c_and_links(tmp_path):
     assert out[0] == "describe 0 0 15 2 12288"
     if not torch.cuda.is_available():
         assert out[1].startswith("create -7 no CUDA device")
+
+
+def test_reference_driver_compiles_unchanged_against_the_facade(tmp_path):
+    """The drop-in claim for C++ callers: the reference's own driver
+    (test/join/main.cc of the reference, unmodified) compiles against
+    include/pidjoin.hpp and links libspidjoin.so. Run without a GPU it stops
+    with pidjoin::Error instead of computing anywhere else. Skipped where the
+    reference tree is absent."""
+    import shutil
+    import subprocess
+    import torch
+    ref = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref-dir"], capture_output=True,
+                         text=True).stdout.strip()
+    main_cc = os.path.join(ref, "test", "join", "main.cc")
+    cxx = shutil.which("g++")
+    lib_dir = os.path.join(ROOT, "spid-join_b200")
+    if not (ref and os.path.exists(main_cc) and cxx and os.path.exists(os.path.join(lib_dir, "libspidjoin.so"))):
+        pytest.skip("no reference driver, C++ compiler or library here")
+    exe = tmp_path / "ref_main"
+    subprocess.run([cxx, "-std=c++17", "-I", os.path.join(ROOT, "include"), main_cc, "-L", lib_dir, "-lspidjoin",
+                    f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    if not torch.cuda.is_available():
+        p = subprocess.run([str(exe), "-s", "1024", "-t", "2", "-z", "0", "-r", "1", "-R", "1", "-B", "1"],
+                           capture_output=True, text=True, timeout=60)
+        assert p.returncode != 0 and "no CUDA device" in p.stderr
