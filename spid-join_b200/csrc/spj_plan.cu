@@ -118,8 +118,8 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     // size class among the algorithms with the same output (the hash joins drop
     // unmatched S tuples, sort-merge and nested loop keep them)
     int alg = d.join_alg;
-    // A hash join planned alone whose R's global table (2 slots of 8 bytes per R
-    // tuple, rounded to a power of two) fits in half of the 126 MB L2 runs as the
+    // A hash join planned alone whose R's global table (2 to 4 slots of 8 bytes
+    // per R tuple, a power of two: at most 64 MiB) fits in half of the 126 MB L2 runs as the
     // non-partitioned hash join: same output, no partitioning passes, and its
     // probes hit L2 (|R| <= 2^22 here; measured on B200 it beats the partitioned
     // join there by 1.2-1.6x, and loses from 2^23 on). Adaptive skew mode only:
