@@ -119,9 +119,9 @@ JoinShape plan_shape(int64_t n_r, int64_t n_s, const spj_design_t &d, int sms, i
     // unmatched S tuples, sort-merge and nested loop keep them)
     int alg = d.join_alg;
     // A hash join planned alone whose R's global table (2 to 4 slots of 8 bytes
-    // per R tuple, a power of two: at most 64 MiB) fits in half of the 126 MB L2 runs as the
-    // non-partitioned hash join: same output, no partitioning passes, and its
-    // probes hit L2 (|R| <= 2^22 here; measured on B200 it beats the partitioned
+    // per R tuple, a power of two: at most 64 MiB) fits in half of the 126 MB L2
+    // runs as the non-partitioned hash join: same output, no partitioning passes,
+    // and its probes hit L2 (|R| <= 2^22 here; measured on B200 it beats the partitioned
     // join there by 1.2-1.6x, and loses from 2^23 on). Adaptive skew mode only:
     // the rank-set and bank-set replication knobs of the fixed mode shape
     // partitions.
