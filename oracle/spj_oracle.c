@@ -549,7 +549,12 @@ static int cmp_key_stable(const void *a, const void *b)
  * merge; each S tuple takes the first R tuple with its key, else stays unchanged.
  * The reference stops probing a bucket at the first S key below the current R
  * key (:226-229), which leaves later S tuples unmatched only when S holds keys
- * that R lacks; this restatement keeps merging (intended semantics). */
+ * that R lacks; this restatement keeps merging (intended semantics). It also
+ * joins every S tuple, where the reference's sort-probe leaves bucket 511 of
+ * each block of 512 range buckets and the last bucket unprobed (:297, :395) and
+ * reads a stale buffer for a bucket of one tuple (its merge sort, :153-208). On
+ * the buckets it does join, the two agree (the reference's kernels run on the
+ * host in the tests). */
 static int dpu_smj(const orc_tuple *r, int64_t nr, const orc_tuple *s, int64_t ns, orc_tuple *out,
                    int64_t *nout)
 {
