@@ -594,7 +594,9 @@ int64_t orc_dpu_smj(const orc_tuple *r, int64_t nr, const orc_tuple *s, int64_t 
  * stay unchanged. Restated with a first-occurrence map, which yields the same
  * rows. (The reference keeps comparing the rewritten value against later R
  * blocks, :156-231, so a payload that equals a later R key is rewritten again;
- * this restatement keeps the single rewrite the kernel intends.) */
+ * this restatement keeps the single rewrite the kernel intends. It also compares
+ * key 0, so its (0, 0) padding "joins" R's padding and stays (0, 0); padding
+ * gives no row here.) */
 static int dpu_nl(const orc_tuple *r, int64_t nr, const orc_tuple *s, int64_t ns, orc_tuple *out,
                   int64_t *nout)
 {
