@@ -169,7 +169,15 @@ int main(void) {
 """
 
 
-def test_header_compiles_as_c_and_links(tmp_path):
+def _build_dir(name):
+    """A scratch directory for a test's build products inside the repository's
+    git-ignored _build/."""
+    d = os.path.join(ROOT, "_build", "tests", name)
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def test_header_compiles_as_c_and_links():
     """The boundary is a C ABI: a strict C11 program (-pedantic -Werror)
     includes include/spidjoin.h, links libspidjoin.so and calls it. The
     planner's description works without a device; a join entry point returns
@@ -181,9 +189,10 @@ def test_header_compiles_as_c_and_links(tmp_path):
     lib_dir = os.path.join(ROOT, "spid-join_b200")
     if not cc or not os.path.exists(os.path.join(lib_dir, "libspidjoin.so")):
         pytest.skip("no C compiler or library")
-    src = tmp_path / "caller.c"
-    src.write_text(C_CALLER)
-    exe = tmp_path / "caller"
+    d = _build_dir("c_caller")
+    src, exe = os.path.join(d, "caller.c"), os.path.join(d, "caller")
+    with open(src, "w") as f:
+        f.write(C_CALLER)
     subprocess.run([cc, "-std=c11", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"),
                     str(src), "-L", lib_dir, "-lspidjoin", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60, check=True).stdout.split("\n")
@@ -192,7 +201,7 @@ def test_header_compiles_as_c_and_links(tmp_path):
         assert out[1].startswith("create -7 no CUDA device")
 
 
-def test_reference_driver_compiles_unchanged_against_the_facade(tmp_path):
+def test_reference_driver_compiles_unchanged_against_the_facade():
     """The drop-in claim for C++ callers: the reference's own driver
     (test/join/main.cc of the reference, unmodified) compiles against
     include/pidjoin.hpp and links libspidjoin.so. Run without a GPU it stops
@@ -208,7 +217,7 @@ def test_reference_driver_compiles_unchanged_against_the_facade(tmp_path):
     lib_dir = os.path.join(ROOT, "spid-join_b200")
     if not (ref and os.path.exists(main_cc) and cxx and os.path.exists(os.path.join(lib_dir, "libspidjoin.so"))):
         pytest.skip("no reference driver, C++ compiler or library here")
-    exe = tmp_path / "ref_main"
+    exe = os.path.join(_build_dir("reference_driver"), "ref_main")
     subprocess.run([cxx, "-std=c++17", "-I", os.path.join(ROOT, "include"), main_cc, "-L", lib_dir, "-lspidjoin",
                     f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
     if not torch.cuda.is_available():
